@@ -1,0 +1,166 @@
+/*
+ * semtex_b200.h -- C ABI of the B200 per-Fourier-mode Helmholtz solver.
+ *
+ * Drop-in boundary for semtex's elliptic solve.  Each entry point names the
+ * reference interface it replaces (file:line in the semtex tree).  All calls
+ * return an int status (SX_OK == 0); nothing calls exit(), unlike
+ * message(..., ERROR) in the reference (veclib/util.c:24-46).
+ *
+ * Data layout (same as the reference's AuxField planes, src/auxfield.cpp:31-54):
+ *   a plane holds nel elements, each np*np values row-major
+ *   (src/element.h:23-24); planes are `plane_stride` doubles apart
+ *   (Geometry::planeSize, src/geometry.cpp:103-109); plane 0 is mode 0,
+ *   plane 1 the Nyquist datum (skipped, as at src/field.cpp:566),
+ *   planes 2k / 2k+1 the real / imaginary parts of mode k
+ *   (femlib/fourier.c:63-69).
+ *
+ * Boundary-condition lines: for each plane, nbound*np values, boundary b's
+ * np values at its side nodes in CCW order (the reference's Field::_line,
+ * src/field.cpp:51-73).
+ *
+ * Threading: an sx_mesh / sx_modal may be used from one host thread at a
+ * time.  Calls on different handles may run concurrently on different
+ * streams.
+ */
+#ifndef SEMTEX_B200_H
+#define SEMTEX_B200_H
+
+#if defined(__GNUC__)
+#define SX_API __attribute__((visibility("default")))
+#else
+#define SX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  SX_OK = 0,
+  SX_ERR_ARG = 1,           /* invalid argument                                   */
+  SX_ERR_CUDA = 2,          /* CUDA runtime error                                 */
+  SX_ERR_NOMEM = 3,         /* device or host allocation failed                   */
+  SX_ERR_JACOBIAN = 4,      /* nonpositive Jacobian (src/element.cpp:1349-1352)   */
+  SX_ERR_SINGULAR_HII = 5,  /* singular interior block (src/element.cpp:212-216)  */
+  SX_ERR_NOT_SPD = 6,       /* band factor failed (src/matrix.cpp:259-261)        */
+  SX_ERR_BAND = 7,          /* btog couples nodes further apart than nband        */
+  SX_WARN_STEP_LIMIT = 8,   /* PCG step limit reached (a warning in the
+                               reference, src/field.cpp:706); solution returned  */
+  SX_ERR_UNSUPPORTED = 9,   /* e.g. np outside [3, 12], cylindrical geometry       */
+  SX_ERR_TIMEOUT = 10,      /* a bounded device-side wait ran out                 */
+  SX_ERR_CAPACITY = 11,     /* serving: request larger than the memory budget     */
+  SX_ERR_NOT_FOUND = 12     /* serving: unknown request id                        */
+};
+
+/* Solver kinds: femlib/cfemdef.h:43-47 (SolverKind). */
+enum { SX_DIRECT = 0, SX_JACPCG = 1, SX_MIXED = 2 };
+
+/* Boundary-condition kinds (src/condition.h: Essential, Natural, Mixed). */
+enum { SX_BC_ESSENTIAL = 0, SX_BC_NATURAL = 1, SX_BC_MIXED = 2 };
+
+/* Precision of the batched form. */
+enum { SX_FP64 = 0, SX_MIXED_FP32 = 1 };
+
+typedef struct sx_mesh_s *sx_mesh;
+typedef struct sx_modal_s *sx_modal;
+
+/* Mesh description: what semtex's vector<Element*> + BoundarySys/NumberSys
+ * carry into MatrixSys and Field::solve.  All arrays are host memory and are
+ * copied; the caller keeps ownership. */
+typedef struct {
+  int np;               /* knots per element side, Geometry::nP()              */
+  int nel;              /* elements, Geometry::nElmt()                          */
+  const double *x;      /* nel*np*np node x, Element::_xmesh                    */
+  const double *y;      /* nel*np*np node y, Element::_ymesh                    */
+  const int *btog;      /* nel*4*(np-1), NumberSys::btog() (src/numbersys.h:59) */
+  const int *bmask;     /* nel*4*(np-1), NumberSys::bmask()                     */
+  int nglobal;          /* NumberSys::nGlobal()                                 */
+  int nsolve;           /* NumberSys::nSolve()                                  */
+  int nband;            /* NumberSys::nBand(), band incl. diagonal              */
+  int nbound;           /* boundary edges (BoundarySys::nSurf())                */
+  const int *b_elmt;    /* nbound: element of each boundary edge                */
+  const int *b_side;    /* nbound: side 0..3 (CCW, side 0 at s = -1)            */
+  const int *b_kind;    /* nbound: SX_BC_*                                      */
+  const double *b_K;    /* nbound or NULL: Mixed K  (src/condition.cpp:247-262) */
+  const double *b_C;    /* nbound or NULL: Mixed C                              */
+} sx_mesh_desc;
+
+/* Solve statistics. */
+typedef struct {
+  int planes_solved;    /* planes actually solved (Nyquist excluded)            */
+  int iterations_max;   /* PCG: max iterations over planes (0 for DIRECT)       */
+  int iterations_total; /* PCG: sum over planes                                 */
+  int refinements;      /* mixed precision: outer refinement steps taken        */
+  double final_rel_residual; /* mixed precision / PCG: max ||r||/||b||          */
+} sx_solve_stats;
+
+/* ---- library ------------------------------------------------------------ */
+SX_API const char *sx_version(void);
+SX_API const char *sx_status_string(int status);
+/* Human-readable detail of the last failing call on this host thread. */
+SX_API const char *sx_last_error(void);
+/* Device used by subsequent calls from this host thread (cudaSetDevice). */
+SX_API int sx_set_device(int device);
+
+/* ---- mesh: replaces Element construction + BCmgr numbering ---------------
+ * Element::Element / Element::mapping (src/element.cpp:30-100, 1281-1436),
+ * BCmgr::buildnum emask (src/bcmgr.cpp:797-803), Edge::Edge area factors
+ * (src/edge.cpp:35-80).  Geometry factors are computed on the host in FP64
+ * and kept resident on the device. */
+SX_API int sx_mesh_create(const sx_mesh_desc *desc, sx_mesh *out);
+SX_API int sx_mesh_destroy(sx_mesh mesh);
+/* Read back element e's geometric factors Q1,Q2,Q3,Q4,Q8 (np*np each). */
+SX_API int sx_mesh_geometry(sx_mesh mesh, int e, double *q1, double *q2, double *q3, double *q4,
+                     double *q8);
+
+/* ---- modal system: replaces ModalMatrixSys::ModalMatrixSys ---------------
+ * src/matrix.cpp:33-110, MatrixSys::MatrixSys src/matrix.cpp:139-317.
+ * For each mode k in [base_mode, base_mode+num_modes): betak2 = (beta k)^2
+ * (src/field.cpp:1121-1139).  DIRECT builds per-element hbi*hii^-1, hii^-1
+ * and the banded Cholesky factor on the GPU (FP64); JACPCG builds the
+ * inverse diagonal; MIXED is DIRECT for mode 0 and JACPCG otherwise
+ * (src/matrix.cpp:93-96).  Systems with equal (lambda2, betak2) are shared,
+ * as the reference's MS cache shares them (src/matrix.cpp:85-102). */
+SX_API int sx_modal_create(sx_mesh mesh, double lambda2, double beta, int base_mode, int num_modes,
+                    int method, sx_modal *out);
+/* Same, with an explicit (lambda2, betak2) per local mode. */
+SX_API int sx_modal_create_ex(sx_mesh mesh, int base_mode, int num_modes, const double *lambda2,
+                       const double *betak2, int method, sx_modal *out);
+/* ModalMatrixSys::~ModalMatrixSys, src/matrix.cpp:113-130. */
+SX_API int sx_modal_destroy(sx_modal modal);
+/* Band factor of local mode m, in LAPACK "U" band storage
+ * (ldab = nband, veclib/lapack.h:107-108): nsolve*nband doubles. */
+/* Device memory held by the modal system (factors, element matrices). */
+SX_API unsigned long long sx_modal_device_bytes(sx_modal modal);
+SX_API int sx_modal_band(sx_modal modal, int m, double *ab, int *nsolve, int *singular);
+
+/* ---- solve: replaces Field::solve (src/field.cpp:509-725) ----------------
+ * Plain form: FP64, mode by mode, same semantics as the reference:
+ *   u   nz planes: in = initial guess (used by JACPCG), out = solution
+ *   f   nz planes: forcing, overwritten (as src/field.cpp:525-526)
+ *   bc  nz * nbound * np boundary-line values (NULL = all zero)
+ * tol_rel / step_max: TOL_REL / STEP_MAX for JACPCG (femlib/defaults.h:29,89).
+ * Host pointers; the copies are part of the call. */
+SX_API int sx_field_solve(sx_modal modal, double *u, double *f, const double *bc, int nz,
+                   int plane_stride, double tol_rel, int step_max, sx_solve_stats *stats);
+/* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream). */
+SX_API int sx_field_solve_device(sx_modal modal, double *d_u, double *d_f, const double *d_bc, int nz,
+                          int plane_stride, double tol_rel, int step_max, void *stream,
+                          sx_solve_stats *stats);
+
+/* ---- batched form (no reference counterpart: extends Field::solve) --------
+ * All modes of the system in one captured CUDA graph, every mode's planes
+ * processed together.  precision = SX_FP64 (same answer as the plain form
+ * to rounding) or SX_MIXED_FP32 (FP32 operator / interior / inner PCG,
+ * FP64 band Cholesky, residual and refinement update; stops when the FP64
+ * relative residual is <= tol_rel). */
+SX_API int sx_field_solve_batched(sx_modal modal, double *d_u, double *d_f, const double *d_bc, int nz,
+                           int plane_stride, int precision, double tol_rel, int max_refine,
+                           void *stream, sx_solve_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEMTEX_B200_H */

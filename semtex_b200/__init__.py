@@ -1,0 +1,231 @@
+"""semtex_b200: B200-native per-Fourier-mode Helmholtz solves for semtex.
+
+Python front-end over the C ABI in include/semtex_b200.h.  The classes mirror
+the reference's solve interface:
+
+* ``Mesh``            Elements + BoundarySys/NumberSys (src/element.h,
+                      src/bsys.h, src/numbersys.h) resident on the GPU;
+* ``ModalMatrixSys``  ModalMatrixSys (src/matrix.h:56-71): one MatrixSys per
+                      Fourier mode, factored on the GPU;
+* ``ModalMatrixSys.solve``  Field::solve (src/field.cpp:509-725): forcing is
+                      overwritten, the solution returned.
+
+The compute path is the compiled CUDA library; there is no CPU fallback.
+If ``libsemtex_b200.so`` is missing or cannot be loaded, import fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .mesh import (ESSENTIAL, MIXED, NATURAL, Boundary, QuadMesh, gll_points,  # noqa: F401
+                   rect_mesh)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsemtex_b200.so")
+
+DIRECT, JACPCG, MIXED_SOLVER = 0, 1, 2
+FP64, MIXED_FP32 = 0, 1
+OK, WARN_STEP_LIMIT = 0, 8
+
+
+class SolverError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status}): {last_error()}")
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("np", C.c_int), ("nel", C.c_int),
+                ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)),
+                ("btog", C.POINTER(C.c_int)), ("bmask", C.POINTER(C.c_int)),
+                ("nglobal", C.c_int), ("nsolve", C.c_int), ("nband", C.c_int),
+                ("nbound", C.c_int),
+                ("b_elmt", C.POINTER(C.c_int)), ("b_side", C.POINTER(C.c_int)),
+                ("b_kind", C.POINTER(C.c_int)),
+                ("b_K", C.POINTER(C.c_double)), ("b_C", C.POINTER(C.c_double))]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("planes_solved", C.c_int), ("iterations_max", C.c_int),
+                ("iterations_total", C.c_int), ("refinements", C.c_int),
+                ("final_rel_residual", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m semtex_b200.build` "
+                          "(no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+    P = C.POINTER
+    L.sx_version.restype = C.c_char_p
+    L.sx_status_string.restype = C.c_char_p
+    L.sx_status_string.argtypes = [ip]
+    L.sx_last_error.restype = C.c_char_p
+    L.sx_set_device.argtypes = [ip]
+    L.sx_mesh_create.argtypes = [P(MeshDesc), P(vp)]
+    L.sx_mesh_destroy.argtypes = [vp]
+    L.sx_mesh_geometry.argtypes = [vp, ip] + [P(dp)] * 5
+    L.sx_modal_create.argtypes = [vp, dp, dp, ip, ip, ip, P(vp)]
+    L.sx_modal_create_ex.argtypes = [vp, ip, ip, P(dp), P(dp), ip, P(vp)]
+    L.sx_modal_destroy.argtypes = [vp]
+    L.sx_modal_device_bytes.argtypes = [vp]
+    L.sx_modal_device_bytes.restype = C.c_ulonglong
+    L.sx_modal_band.argtypes = [vp, ip, P(dp), P(ip), P(ip)]
+    L.sx_field_solve.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, dp, ip, P(SolveStats)]
+    L.sx_field_solve_device.argtypes = [vp, vp, vp, vp, ip, ip, dp, ip, vp, P(SolveStats)]
+    if hasattr(L, "sx_field_solve_batched"):
+        L.sx_field_solve_batched.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(SolveStats)]
+    return L
+
+
+lib = _load()
+
+
+def status_string(s):
+    return lib.sx_status_string(s).decode()
+
+
+def last_error():
+    return lib.sx_last_error().decode()
+
+
+def version():
+    return lib.sx_version().decode()
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _check(st, what, allow=(OK,)):
+    if st not in allow:
+        raise SolverError(st, what)
+    return st
+
+
+class Mesh:
+    """A QuadMesh uploaded to the GPU (geometry factors + numbering)."""
+
+    def __init__(self, qm: QuadMesh):
+        self.qm = qm
+        nb, be, bs, bk, bK, bC = qm.bc_arrays()
+        self._keep = dict(
+            x=np.ascontiguousarray(qm.x, dtype=np.float64).reshape(-1),
+            y=np.ascontiguousarray(qm.y, dtype=np.float64).reshape(-1),
+            btog=np.ascontiguousarray(qm.btog, dtype=np.int32).reshape(-1),
+            bmask=np.ascontiguousarray(qm.bmask, dtype=np.int32).reshape(-1),
+            be=be.astype(np.int32), bs=bs.astype(np.int32), bk=bk.astype(np.int32),
+            bK=bK.astype(np.float64), bC=bC.astype(np.float64))
+        k = self._keep
+        d = MeshDesc(qm.np, qm.nel, _dptr(k["x"]), _dptr(k["y"]), _iptr(k["btog"]),
+                     _iptr(k["bmask"]), qm.nglobal, qm.nsolve, qm.nband, nb,
+                     _iptr(k["be"]), _iptr(k["bs"]), _iptr(k["bk"]), _dptr(k["bK"]), _dptr(k["bC"]))
+        h = C.c_void_p()
+        _check(lib.sx_mesh_create(C.byref(d), C.byref(h)), "sx_mesh_create")
+        self.h = h
+
+    def geometry(self, e):
+        out = [np.zeros(self.qm.npnp) for _ in range(5)]
+        _check(lib.sx_mesh_geometry(self.h, e, *[_dptr(a) for a in out]), "sx_mesh_geometry")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.sx_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class ModalMatrixSys:
+    """One Helmholtz system per Fourier mode (ModalMatrixSys, src/matrix.cpp:33-110).
+
+    Either ``lambda2`` (scalar) with ``beta`` (betak2 = (beta k)^2), or
+    per-mode arrays ``lambda2_modes`` / ``betak2_modes``.
+    """
+
+    def __init__(self, mesh: Mesh, lambda2=0.0, beta=0.0, base_mode=0, num_modes=1,
+                 method=DIRECT, lambda2_modes=None, betak2_modes=None):
+        self.mesh = mesh
+        self.base_mode, self.num_modes, self.method = base_mode, num_modes, method
+        h = C.c_void_p()
+        if lambda2_modes is None:
+            _check(lib.sx_modal_create(mesh.h, float(lambda2), float(beta), base_mode, num_modes,
+                                       method, C.byref(h)), "sx_modal_create")
+        else:
+            lam = np.ascontiguousarray(lambda2_modes, dtype=np.float64)
+            bk2 = (np.zeros(num_modes) if betak2_modes is None
+                   else np.ascontiguousarray(betak2_modes, dtype=np.float64))
+            _check(lib.sx_modal_create_ex(mesh.h, base_mode, num_modes, _dptr(lam), _dptr(bk2),
+                                          method, C.byref(h)), "sx_modal_create_ex")
+        self.h = h
+
+    @property
+    def device_bytes(self):
+        return int(lib.sx_modal_device_bytes(self.h))
+
+    def band(self, m=0):
+        """Factored band of local mode m in LAPACK "U" storage (nsolve, nband)."""
+        ns, sg = C.c_int(), C.c_int()
+        _check(lib.sx_modal_band(self.h, m, None, C.byref(ns), C.byref(sg)), "sx_modal_band")
+        ab = np.zeros(ns.value * self.mesh.qm.nband)
+        _check(lib.sx_modal_band(self.h, m, _dptr(ab), C.byref(ns), C.byref(sg)), "sx_modal_band")
+        return ab.reshape(ns.value, self.mesh.qm.nband), bool(sg.value)
+
+    def _bc_array(self, bc, nz):
+        qm = self.mesh.qm
+        nb = max(len(qm.boundaries), 1)
+        if bc is None:
+            return None
+        return np.ascontiguousarray(np.broadcast_to(bc, (nz, nb, qm.np)), dtype=np.float64).copy()
+
+    def solve(self, forcing, bc=None, u0=None, tol_rel=1e-8, step_max=500, return_stats=False):
+        """Field::solve on host arrays.  forcing: (nz, nplane); returns u."""
+        qm = self.mesh.qm
+        f = np.ascontiguousarray(forcing, dtype=np.float64).reshape(-1, qm.nplane).copy()
+        nz = f.shape[0]
+        u = (np.zeros_like(f) if u0 is None
+             else np.ascontiguousarray(u0, dtype=np.float64).reshape(nz, qm.nplane).copy())
+        b = self._bc_array(bc, nz)
+        st = SolveStats()
+        rc = lib.sx_field_solve(self.h, _dptr(u), _dptr(f), _dptr(b) if b is not None else None,
+                                nz, qm.nplane, tol_rel, step_max, C.byref(st))
+        _check(rc, "sx_field_solve", allow=(OK, WARN_STEP_LIMIT))
+        return (u, st.as_dict()) if return_stats else u
+
+    def solve_device(self, d_u, d_f, d_bc, nz, stride, tol_rel=1e-8, step_max=500, stream=0):
+        """Field::solve on device pointers (ints), enqueued on `stream`."""
+        st = SolveStats()
+        rc = lib.sx_field_solve_device(self.h, d_u, d_f, d_bc, nz, stride, tol_rel, step_max,
+                                       stream, C.byref(st))
+        _check(rc, "sx_field_solve_device", allow=(OK, WARN_STEP_LIMIT))
+        return st.as_dict()
+
+    def solve_batched(self, d_u, d_f, d_bc, nz, stride, precision=FP64, tol_rel=1e-12,
+                      max_refine=8, stream=0):
+        """All modes in one captured graph (device pointers)."""
+        st = SolveStats()
+        rc = lib.sx_field_solve_batched(self.h, d_u, d_f, d_bc, nz, stride, precision, tol_rel,
+                                        max_refine, stream, C.byref(st))
+        _check(rc, "sx_field_solve_batched", allow=(OK, WARN_STEP_LIMIT))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.sx_modal_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

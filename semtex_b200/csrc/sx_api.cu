@@ -1,0 +1,372 @@
+// sx_api.cu -- C ABI: ModalMatrixSys and Field::solve replacements.
+#include <cmath>
+#include <cstring>
+
+#include "sx_internal.h"
+#include "sx_kernels.cuh"
+#include "sx_pcg.cuh"
+#include "sx_solve.cuh"
+
+namespace sx {
+const char *last_error();
+}
+
+using namespace sx;
+
+struct sx_modal_s {
+  sx_mesh_s *mesh = nullptr;
+  int base_mode = 0, num_modes = 0, method = SX_DIRECT;
+  std::vector<std::shared_ptr<System>> sys;   // per local mode
+  std::vector<std::shared_ptr<System>> uniq;  // distinct systems
+  // solve workspace, sized for all planes at once
+  int ws_planes = 0;
+  DBuf<double> rhs, Fb, gess;
+  PcgWork pcg;
+  DBuf<Job> djobs;
+  // host-pointer entry: device staging
+  DBuf<double> hu, hf, hbc;
+  size_t npad_max = 0;
+  // batched form: captured graph and the arguments it was captured for
+  cudaStream_t own = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  const void *gkey[3] = {nullptr, nullptr, nullptr};
+  int gnz = 0, gstride = 0, gprec = -1;
+  DBuf<Job> bjobs;
+  ~sx_modal_s() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
+extern "C" const char *sx_version(void) { return "semtex_b200 0.1 (sm_100a)"; }
+
+extern "C" const char *sx_status_string(int s) {
+  switch (s) {
+    case SX_OK: return "ok";
+    case SX_ERR_ARG: return "invalid argument";
+    case SX_ERR_CUDA: return "CUDA error";
+    case SX_ERR_NOMEM: return "out of memory";
+    case SX_ERR_JACOBIAN: return "nonpositive element Jacobian";
+    case SX_ERR_SINGULAR_HII: return "singular interior matrix hii";
+    case SX_ERR_NOT_SPD: return "failed to factor Helmholtz matrix";
+    case SX_ERR_BAND: return "numbering exceeds declared band";
+    case SX_WARN_STEP_LIMIT: return "PCG step limit exceeded";
+    case SX_ERR_UNSUPPORTED: return "unsupported configuration";
+    case SX_ERR_TIMEOUT: return "device wait timed out";
+    case SX_ERR_CAPACITY: return "request exceeds memory budget";
+    case SX_ERR_NOT_FOUND: return "unknown request";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char *sx_last_error(void) { return last_error(); }
+
+extern "C" int sx_set_device(int device) {
+  SX_CUDA(cudaSetDevice(device));
+  return SX_OK;
+}
+
+static bool same_constants(const System &S, double lambda2, double betak2, int method) {
+  // MatrixSys::match, src/matrix.cpp:326-347 (same mesh numbering implied).
+  return std::fabs(S.lambda2 - lambda2) < EPSDP && std::fabs(S.betak2 - betak2) < EPSDP &&
+         S.method == method;
+}
+
+static int modal_build(sx_mesh m, int base_mode, int num_modes, const double *lam, const double *bk2,
+                       int method, sx_modal *out) {
+  if (!m || !out || num_modes <= 0 || base_mode < 0 || method < SX_DIRECT || method > SX_MIXED)
+    return SX_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<sx_modal_s> M(new sx_modal_s());
+  M->mesh = m;
+  M->base_mode = base_mode;
+  M->num_modes = num_modes;
+  M->method = method;
+  cudaStream_t st = 0;
+  std::vector<System *> to_factor;
+  for (int l = 0; l < num_modes; l++) {
+    const int mode = base_mode + l;
+    int kind = method;
+    if (method == SX_MIXED) kind = (mode == 0) ? SX_DIRECT : SX_JACPCG;  // src/matrix.cpp:93-96
+    std::shared_ptr<System> found;
+    for (auto &s : M->uniq)
+      if (same_constants(*s, lam[l], bk2[l], kind)) {
+        found = s;
+        break;
+      }
+    if (!found) {
+      found = std::make_shared<System>();
+      found->mesh = m;
+      found->lambda2 = lam[l];
+      found->betak2 = bk2[l];
+      found->method = kind;
+      if (kind == SX_DIRECT) {
+        SX_TRY(system_build_direct(*found, st));
+        if (found->nsolve > 0) to_factor.push_back(found.get());
+      } else {
+        SX_TRY(system_build_jacobi(*found, st));
+      }
+      M->uniq.push_back(found);
+    }
+    M->sys.push_back(found);
+  }
+  SX_TRY(factor_batch(to_factor, st));
+  for (System *S : to_factor) {
+    int h = 0;
+    SX_CUDA(cudaMemcpy(&h, S->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h & (1 << SX_ERR_NOT_SPD)) {
+      set_error("failed to factor Helmholtz matrix (lambda2=%g, betak2=%g)", S->lambda2, S->betak2);
+      return SX_ERR_NOT_SPD;
+    }
+  }
+  *out = M.release();
+  return SX_OK;
+}
+
+extern "C" int sx_modal_create(sx_mesh m, double lambda2, double beta, int base_mode, int num_modes,
+                               int method, sx_modal *out) {
+  if (num_modes <= 0) return SX_ERR_ARG;
+  std::vector<double> lam(num_modes, lambda2), bk2(num_modes);
+  for (int l = 0; l < num_modes; l++) {
+    const double bk = beta * (base_mode + l);  // Field::modeConstant, Cartesian
+    bk2[l] = bk * bk;
+  }
+  return modal_build(m, base_mode, num_modes, lam.data(), bk2.data(), method, out);
+}
+
+extern "C" int sx_modal_create_ex(sx_mesh m, int base_mode, int num_modes, const double *lambda2,
+                                  const double *betak2, int method, sx_modal *out) {
+  if (!lambda2 || !betak2) return SX_ERR_ARG;
+  return modal_build(m, base_mode, num_modes, lambda2, betak2, method, out);
+}
+
+extern "C" int sx_modal_destroy(sx_modal s) {
+  delete s;
+  return SX_OK;
+}
+
+extern "C" int sx_modal_band(sx_modal s, int m, double *ab, int *nsolve, int *singular) {
+  if (!s || m < 0 || m >= s->num_modes) return SX_ERR_ARG;
+  const System &S = *s->sys[m];
+  if (nsolve) *nsolve = S.nsolve;
+  if (singular) *singular = S.singular ? 1 : 0;
+  if (S.method != SX_DIRECT) return SX_ERR_ARG;
+  if (ab) SX_TRY(system_band_export(S, ab));
+  return SX_OK;
+}
+
+extern "C" unsigned long long sx_modal_device_bytes(sx_modal s) {
+  if (!s) return 0;
+  size_t b = 0;
+  for (auto &u : s->uniq) b += u->bytes();
+  return b;
+}
+
+// Plane groups of a solve: local mode l owns planes 2l, 2l+1; plane 1 is the
+// Nyquist datum when the base mode is 0 (src/field.cpp:564-573).
+struct Group {
+  int mode;    // local mode
+  int plane0;  // first plane
+  int P;       // planes
+};
+
+static int plane_groups(const sx_modal_s &M, int nz, std::vector<Group> &g) {
+  g.clear();
+  if (nz <= 0) return SX_ERR_ARG;
+  if (nz == 1) {
+    g.push_back({0, 0, 1});
+    return SX_OK;
+  }
+  if (nz % 2) return SX_ERR_ARG;
+  if (nz / 2 > M.num_modes) return SX_ERR_ARG;
+  for (int l = 0; l < nz / 2; l++) {
+    if (l == 0 && M.base_mode == 0)
+      g.push_back({0, 0, 1});
+    else
+      g.push_back({l, 2 * l, 2});
+  }
+  return SX_OK;
+}
+
+static int reserve_ws(sx_modal_s &M, int planes) {
+  const sx_mesh_s &Mh = *M.mesh;
+  size_t npad = 1;
+  for (auto &s : M.uniq) npad = std::max(npad, (size_t)std::max(s->nblk, 1) * NB);
+  if (planes <= M.ws_planes && npad <= M.npad_max) return SX_OK;
+  SX_TRY(M.rhs.alloc((size_t)planes * npad));
+  SX_TRY(M.Fb.alloc((size_t)planes * Mh.nel * Mh.next));
+  SX_TRY(M.gess.alloc((size_t)planes * Mh.nglobal));
+  M.ws_planes = planes;
+  M.npad_max = npad;
+  return SX_OK;
+}
+
+static Job make_job(sx_modal_s &M, const Group &g, int slot, double *u, double *f, const double *bc,
+                    long long stride, long long bcstride) {
+  const sx_mesh_s &Mh = *M.mesh;
+  const System &S = *M.sys[g.mode];
+  Job j;
+  std::memset(&j, 0, sizeof(j));
+  j.u = u + (long long)g.plane0 * stride;
+  j.f = f + (long long)g.plane0 * stride;
+  j.bc = bc ? bc + (long long)g.plane0 * bcstride : nullptr;
+  j.ustride = j.fstride = stride;
+  j.bcstride = bcstride;
+  j.P = g.P;
+  j.hCon = S.betak2 + S.lambda2;
+  j.nsolve = S.nsolve;
+  j.hbi = S.hbi.p;
+  j.hii = S.hii.p;
+  j.tiles = S.tiles.p;
+  j.dinv = S.dinv.p;
+  j.nblk = S.nblk;
+  j.J = S.J;
+  j.npad = std::max(S.nblk, 1) * NB;
+  j.rhs_stride = (long long)M.npad_max;
+  j.rhs = M.rhs.p + (size_t)slot * M.npad_max;
+  j.Fb = M.Fb.p + (size_t)slot * Mh.nel * Mh.next;
+  j.gess = M.gess.p + (size_t)slot * Mh.nglobal;
+  j.pc = S.pc.p;
+  return j;
+}
+
+extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
+                                     int plane_stride, double tol_rel, int step_max, void *stream,
+                                     sx_solve_stats *stats) {
+  if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<Group> groups;
+  SX_TRY(plane_groups(*s, nz, groups));
+  int planes = 0;
+  for (auto &g : groups) planes += g.P;
+  SX_TRY(reserve_ws(*s, planes));
+  const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
+  std::vector<Job> jobs;
+  int slot = 0;
+  for (auto &g : groups) {
+    jobs.push_back(make_job(*s, g, slot, d_u, d_f, d_bc, plane_stride, bcstride));
+    slot += g.P;
+  }
+  if (s->djobs.n < jobs.size()) SX_TRY(s->djobs.alloc(jobs.size()));
+  SX_CUDA(cudaMemcpyAsync(s->djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
+  const MeshView M = s->mesh->view();
+  SX_TRY(prepare_direct_kernels(M));
+  sx_solve_stats loc{};
+  int rc = SX_OK;
+  // Mode by mode, as Field::solve's plane loop.
+  for (size_t i = 0; i < groups.size(); i++) {
+    const System &S = *s->sys[groups[i].mode];
+    std::vector<Job> one(1, jobs[i]);
+    if (S.method == SX_DIRECT) {
+      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st));
+    } else {
+      int iters = 0;
+      double rr = 0.0;
+      const int r = pcg_solve_job(M, S, s->pcg, jobs[i], tol_rel, step_max, st, &iters, &rr);
+      if (r != SX_OK && r != SX_WARN_STEP_LIMIT) return r;
+      if (r == SX_WARN_STEP_LIMIT) rc = SX_WARN_STEP_LIMIT;
+      loc.iterations_max = std::max(loc.iterations_max, iters);
+      loc.iterations_total += iters * groups[i].P;
+      loc.final_rel_residual = std::max(loc.final_rel_residual, rr);
+    }
+    loc.planes_solved += groups[i].P;
+  }
+  SX_CUDA(cudaGetLastError());
+  if (stats) *stats = loc;
+  return rc;
+}
+
+extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc, int nz, int plane_stride,
+                              double tol_rel, int step_max, sx_solve_stats *stats) {
+  if (!s || !u || !f || nz <= 0) return SX_ERR_ARG;
+  const size_t n = (size_t)nz * plane_stride;
+  const size_t nbc = (size_t)nz * std::max(s->mesh->nbound, 1) * s->mesh->np;
+  if (s->hu.n < n) SX_TRY(s->hu.alloc(n));
+  if (s->hf.n < n) SX_TRY(s->hf.alloc(n));
+  if (bc && s->hbc.n < nbc) SX_TRY(s->hbc.alloc(nbc));
+  SX_CUDA(cudaMemcpy(s->hu.p, u, n * 8, cudaMemcpyHostToDevice));
+  SX_CUDA(cudaMemcpy(s->hf.p, f, n * 8, cudaMemcpyHostToDevice));
+  if (bc) SX_CUDA(cudaMemcpy(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice));
+  const int rc = sx_field_solve_device(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride,
+                                       tol_rel, step_max, nullptr, stats);
+  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  SX_CUDA(cudaMemcpy(u, s->hu.p, n * 8, cudaMemcpyDeviceToHost));
+  return rc;
+}
+
+static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
+                               int plane_stride, double tol_rel, int max_refine, void *stream,
+                               sx_solve_stats *stats) {
+  (void)s; (void)d_u; (void)d_f; (void)d_bc; (void)nz; (void)plane_stride; (void)tol_rel;
+  (void)max_refine; (void)stream; (void)stats;
+  set_error("mixed-precision batched form not built yet");
+  return SX_ERR_UNSUPPORTED;
+}
+
+// Batched form: every mode's planes in each launch (one job per mode), the
+// whole sequence captured once into a CUDA graph and replayed.
+extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
+                                      int plane_stride, int precision, double tol_rel, int max_refine,
+                                      void *stream, sx_solve_stats *stats) {
+  if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+  if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+  if (precision == SX_MIXED_FP32)
+    return mixed_solve_batched(s, d_u, d_f, d_bc, nz, plane_stride, tol_rel, max_refine, stream, stats);
+  std::vector<Group> groups;
+  SX_TRY(plane_groups(*s, nz, groups));
+  for (auto &g : groups)
+    if (s->sys[g.mode]->method != SX_DIRECT) {
+      set_error("batched FP64 form needs DIRECT systems");
+      return SX_ERR_UNSUPPORTED;
+    }
+  int planes = 0;
+  for (auto &g : groups) planes += g.P;
+  SX_TRY(reserve_ws(*s, planes));
+  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
+  const bool same = s->gexec && s->gkey[0] == d_u && s->gkey[1] == d_f && s->gkey[2] == d_bc &&
+                    s->gnz == nz && s->gstride == plane_stride && s->gprec == precision;
+  if (!same) {
+    if (s->gexec) {
+      cudaGraphExecDestroy(s->gexec);
+      s->gexec = nullptr;
+    }
+    const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
+    std::vector<Job> jobs;
+    int slot = 0;
+    for (auto &g : groups) {
+      jobs.push_back(make_job(*s, g, slot, d_u, d_f, d_bc, plane_stride, bcstride));
+      slot += g.P;
+    }
+    if (s->bjobs.n < jobs.size()) SX_TRY(s->bjobs.alloc(jobs.size()));
+    SX_CUDA(cudaMemcpy(s->bjobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice));
+    const MeshView M = s->mesh->view();
+    // warm the kernel attributes outside capture
+    SX_TRY(prepare_direct_kernels(M));
+    cudaGraph_t g = nullptr;
+    SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st);
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (rc != SX_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    SX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
+    cudaGraphDestroy(g);
+    SX_CUDA(ie);
+    s->gkey[0] = d_u;
+    s->gkey[1] = d_f;
+    s->gkey[2] = d_bc;
+    s->gnz = nz;
+    s->gstride = plane_stride;
+    s->gprec = precision;
+  }
+  SX_CUDA(cudaGraphLaunch(s->gexec, st));
+  if (!stream) SX_CUDA(cudaStreamSynchronize(st));
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->planes_solved = planes;
+  }
+  return SX_OK;
+}

@@ -1,0 +1,499 @@
+// sx_factor.cu -- GPU set-up of a DIRECT or JACPCG system (MatrixSys).
+//
+// DIRECT (src/matrix.cpp:175-274):
+//   1. k_elem_condense: one CTA per element builds the elemental Helmholtz
+//      matrix in edge-major order (Element::HelmholtzRow,
+//      src/element.cpp:1439-1509), inverts the interior block (the reference
+//      uses getrf+getri, src/element.cpp:212-216; hii is SPD here so
+//      Gauss-Jordan without pivoting is used) and condenses
+//      hbb -= hbi hii^-1 hib, hbi <- hbi hii^-1 (src/element.cpp:218-220).
+//   2. k_band_add: direct-stiffness assembly of hbb into the banded matrix,
+//      one element colour per launch so no two CTAs touch the same entry
+//      (deterministic; src/matrix.cpp:236-241).  Mixed-BC diagonal terms
+//      follow in boundary order (Mixed::augmentSC, src/condition.cpp:347-381).
+//   3. Tiled right-looking banded Cholesky, A = U^T U (LAPACK dpbtrf "U",
+//      src/matrix.cpp:259): per block column k, k_potrf factors the diagonal
+//      tile and forms its inverse, k_trsm forms the off-diagonal tiles of
+//      block row k, k_update applies the trailing rank-nb update inside the
+//      band.  All systems of a batch share each launch.
+// JACPCG (src/matrix.cpp:276-317): k_elem_diag + k_diag_dss.
+#include <cmath>
+#include <cstring>
+
+#include "sx_internal.h"
+#include "sx_kernels.cuh"
+
+namespace sx {
+
+// ---------------------------------------------------------------------------
+// Element matrix + static condensation
+// ---------------------------------------------------------------------------
+
+// smem (doubles): D nn | Q1..Q4 4nn | hbb next^2 | hbi next*nint | hii nint^2 |
+// t next*nint | colk nint ; ints: emap nn
+static size_t condense_smem(const MeshView &M) {
+  const size_t nn = M.npnp, ne = M.next, ni = M.nint;
+  return sizeof(double) * (5 * nn + ne * ne + 2 * ne * ni + ni * ni + ni) + sizeof(int) * nn + 16;
+}
+
+__global__ void k_elem_condense(MeshView M, double hCon, double *__restrict__ hbi_out,
+                                double *__restrict__ hii_out, double *__restrict__ hbb_out,
+                                int *status) {
+  extern __shared__ double sm[];
+  const int np = M.np, nn = M.npnp, next = M.next, nint = M.nint;
+  const int e = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  double *D = sm, *Q1 = D + nn, *Q2 = Q1 + nn, *Q3 = Q2 + nn, *Q4 = Q3 + nn;
+  double *hbb = Q4 + nn, *hbi = hbb + next * next, *hii = hbi + next * nint;
+  double *t = hii + nint * nint, *colk = t + next * nint;
+  int *emap = (int *)(colk + nint);
+  __shared__ int bad;
+  if (tid == 0) bad = 0;
+  const size_t eo = (size_t)e * nn;
+  for (int i = tid; i < nn; i += nt) {
+    D[i] = M.D[i];
+    Q1[i] = M.Q1[eo + i];
+    Q2[i] = M.Q2[eo + i];
+    Q3[i] = M.Q3[eo + i];
+    Q4[i] = M.Q4[eo + i];
+    emap[i] = M.emap[i];
+  }
+  __syncthreads();
+  const bool q3 = M.hasQ3[e];
+  // Entry H[(i,j),(m,n)] of the elemental matrix, accumulated in the order
+  // of HelmholtzRow: Q1 term, Q2 term, the two Q3 terms, then Q4*hCon.
+  for (int idx = tid; idx < nn * nn; idx += nt) {
+    const int a = idx / nn, b = idx - a * nn;
+    if (a >= next && b < next) continue;
+    const int r = emap[a], c = emap[b];
+    const int i = r / np, j = r - i * np, m = c / np, n = c - m * np;
+    double h = 0.0;
+    if (m == i) {
+      double s = 0.0;
+      for (int q = 0; q < np; q++) s += Q1[i * np + q] * (D[q * np + j] * D[q * np + n]);
+      h = s;
+    }
+    if (n == j) {
+      double s = 0.0;
+      for (int p = 0; p < np; p++) s += Q2[p * np + j] * (D[p * np + i] * D[p * np + m]);
+      h += s;
+    }
+    if (q3) {
+      h += Q3[i * np + n] * D[n * np + j] * D[i * np + m];
+      h += Q3[m * np + j] * D[j * np + n] * D[m * np + i];
+    }
+    if (m == i && n == j) h += Q4[i * np + j] * hCon;
+    if (a < next) {
+      if (b < next)
+        hbb[a * next + b] = h;
+      else
+        hbi[a * nint + (b - next)] = h;
+    } else {
+      hii[(a - next) * nint + (b - next)] = h;
+    }
+  }
+  __syncthreads();
+  // In-place Gauss-Jordan inverse of the SPD interior block.
+  for (int k = 0; k < nint; k++) {
+    const double p = hii[k * nint + k];
+    for (int i = tid; i < nint; i += nt) colk[i] = hii[i * nint + k];
+    if (tid == 0 && !(p > 0.0)) bad = 1;
+    __syncthreads();
+    const double rp = (p > 0.0) ? 1.0 / p : 1.0;
+    for (int j = tid; j < nint; j += nt) hii[k * nint + j] = ((j == k) ? 1.0 : hii[k * nint + j]) * rp;
+    __syncthreads();
+    for (int idx = tid; idx < nint * nint; idx += nt) {
+      const int i = idx / nint, j = idx - i * nint;
+      if (i == k) continue;
+      const double v = (j == k) ? 0.0 : hii[idx];
+      hii[idx] = v - colk[i] * hii[k * nint + j];
+    }
+    __syncthreads();
+  }
+  // t = hbi * hii^-1 ; hbb -= t * hbi^T
+  for (int idx = tid; idx < next * nint; idx += nt) {
+    const int b = idx / nint, c = idx - b * nint;
+    double s = 0.0;
+    for (int q = 0; q < nint; q++) s += hbi[b * nint + q] * hii[q * nint + c];
+    t[idx] = s;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < next * next; idx += nt) {
+    const int b = idx / next, b2 = idx - b * next;
+    double s = 0.0;
+    for (int q = 0; q < nint; q++) s += t[b * nint + q] * hbi[b2 * nint + q];
+    hbb[idx] -= s;
+  }
+  __syncthreads();
+  double *ob = hbi_out + (size_t)e * next * nint;
+  for (int i = tid; i < next * nint; i += nt) ob[i] = t[i];
+  double *oi = hii_out + (size_t)e * nint * nint;
+  for (int i = tid; i < nint * nint; i += nt) oi[i] = hii[i];
+  double *oh = hbb_out + (size_t)e * next * next;
+  for (int i = tid; i < next * next; i += nt) oh[i] = hbb[i];
+  if (tid == 0 && bad) atomicOr(status, 1 << SX_ERR_SINGULAR_HII);
+}
+
+// ---------------------------------------------------------------------------
+// Band assembly into tiles
+// ---------------------------------------------------------------------------
+
+__global__ void k_band_identity_pad(double *tiles, int J, int nsolve, int nblk) {
+  const int g = nsolve + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nblk * NB) return;
+  const int b = g / NB, r = g - b * NB;
+  tiles[((size_t)b * (J + 1)) * TSZ + (size_t)r * LDT + r] = 1.0;
+}
+
+__global__ void k_band_add(MeshView M, const int *__restrict__ elems, const double *__restrict__ hbb,
+                           double *tiles, int J, int nsolve, int *status) {
+  const int e = elems[blockIdx.x];
+  const int next = M.next, kd = M.nband - 1;
+  const int *bt = M.btog + (size_t)e * next;
+  const double *h = hbb + (size_t)e * next * next;
+  for (int idx = threadIdx.x; idx < next * next; idx += blockDim.x) {
+    const int i = idx / next, k = idx - i * next;
+    const int m = bt[i], n = bt[k];
+    if (m < nsolve && n < nsolve && n >= m) {
+      if (n - m > kd) {
+        atomicOr(status, 1 << SX_ERR_BAND);
+        continue;
+      }
+      tiles[tile_addr(m, n, J)] += h[idx];
+    }
+  }
+}
+
+// Mixed::augmentSC in boundary order (one thread: tiny, order-preserving).
+__global__ void k_band_mixed(MeshView M, double *tiles, int J, int nsolve) {
+  if (threadIdx.x || blockIdx.x) return;
+  const int np = M.np, nm = np - 1;
+  for (int b = 0; b < M.nbound; b++) {
+    if (M.b_kind[b] != SX_BC_MIXED) continue;
+    const int *bmap = M.btog + (size_t)M.b_elmt[b] * M.next;
+    const int side = M.b_side[b];
+    const double K = M.b_K[b];
+    const double *area = M.b_area + (size_t)b * np;
+    for (int i = 0; i < nm; i++) {
+      const int k = bmap[side * nm + i];
+      if (k < nsolve) tiles[tile_addr(k, k, J)] += K * area[i];
+    }
+    const int i = (side == 3) ? bmap[0] : bmap[side * nm + nm];
+    if (i < nsolve) tiles[tile_addr(i, i, J)] += K * area[nm];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled banded Cholesky
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void tile_load(double *dst, const double *__restrict__ src) {
+  const double2 *s = reinterpret_cast<const double2 *>(src);
+  double2 *d = reinterpret_cast<double2 *>(dst);
+  for (int i = threadIdx.x; i < TSZ / 2; i += blockDim.x) d[i] = s[i];
+}
+
+__device__ __forceinline__ void tile_store(double *dst, const double *src) {
+  const double2 *s = reinterpret_cast<const double2 *>(src);
+  double2 *d = reinterpret_cast<double2 *>(dst);
+  for (int i = threadIdx.x; i < TSZ / 2; i += blockDim.x) d[i] = s[i];
+}
+
+// Factor the diagonal tile of block column k and store its inverse.
+__global__ void k_potrf(const SysDesc *__restrict__ sys, int k) {
+  const SysDesc S = sys[blockIdx.x];
+  if (k >= S.nblk) return;
+  extern __shared__ __align__(16) double smp[];
+  double *A = smp, *X = smp + TSZ;
+  __shared__ int bad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *T = S.tiles + ((size_t)k * (S.J + 1)) * TSZ;
+  if (tid == 0) bad = 0;
+  tile_load(A, T);
+  __syncthreads();
+  for (int c = 0; c < NB; c++) {
+    double d = A[c * LDT + c];
+    if (!(d > 0.0)) {
+      if (tid == 0) bad = 1;
+      d = 1.0;
+    }
+    d = sqrt(d);
+    __syncthreads();
+    const double rd = 1.0 / d;
+    for (int j = c + 1 + tid; j < NB; j += nt) A[c * LDT + j] *= rd;
+    if (tid == 0) A[c * LDT + c] = d;
+    __syncthreads();
+    const int w = NB - c - 1;
+    for (int idx = tid; idx < w * w; idx += nt) {
+      const int i = c + 1 + idx / w, j = c + 1 + idx % w;
+      if (j >= i) A[i * LDT + j] -= A[c * LDT + i] * A[c * LDT + j];
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < NB * NB; idx += nt) {
+    const int i = idx / NB, j = idx % NB;
+    if (j < i) A[i * LDT + j] = 0.0;
+  }
+  __syncthreads();
+  tile_store(T, A);
+  // X = U^-1 (upper triangular), one column per thread, back substitution.
+  for (int idx = tid; idx < TSZ; idx += nt) X[idx] = 0.0;
+  __syncthreads();
+  for (int j = tid; j < NB; j += nt) {
+    X[j * LDT + j] = 1.0 / A[j * LDT + j];
+    for (int i = j - 1; i >= 0; i--) {
+      double s = 0.0;
+      for (int l = i + 1; l <= j; l++) s += A[i * LDT + l] * X[l * LDT + j];
+      X[i * LDT + j] = -s / A[i * LDT + i];
+    }
+  }
+  __syncthreads();
+  tile_store(S.dinv + (size_t)k * TSZ, X);
+  if (tid == 0 && bad) atomicOr(S.status, 1 << SX_ERR_NOT_SPD);
+}
+
+// C (+)= alpha * A^T B on NB x NB smem tiles; thread (ty, tx) of a 16x16
+// layout owns rows ty + 16a, cols tx + 16b.
+__device__ __forceinline__ void tile_gemm_tn(double *C, const double *A, const double *B,
+                                             double alpha, bool accumulate) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  for (int l = 0; l < NB; l++) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) av[a] = A[l * LDT + ty + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; b++) bv[b] = B[l * LDT + tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      double *c = &C[(ty + 16 * a) * LDT + tx + 16 * b];
+      *c = accumulate ? (*c + alpha * acc[a][b]) : alpha * acc[a][b];
+    }
+}
+
+// Off-diagonal tiles of block row k: U(k, k+i) = U_kk^-T A(k, k+i).
+__global__ void __launch_bounds__(256) k_trsm(const SysDesc *__restrict__ sys, int k) {
+  const SysDesc S = sys[blockIdx.y];
+  const int i = blockIdx.x + 1;
+  if (k >= S.nblk || i > S.J || k + i >= S.nblk) return;
+  extern __shared__ __align__(16) double smt[];
+  double *X = smt, *B = X + TSZ, *C = B + TSZ;
+  double *T = S.tiles + ((size_t)(k + i) * (S.J + 1) + i) * TSZ;
+  tile_load(X, S.dinv + (size_t)k * TSZ);
+  tile_load(B, T);
+  __syncthreads();
+  tile_gemm_tn(C, X, B, 1.0, false);
+  __syncthreads();
+  tile_store(T, C);
+}
+
+// Trailing update inside the band: A(k+i, k+j) -= U(k,k+i)^T U(k,k+j),
+// 1 <= i <= j <= J.
+__global__ void __launch_bounds__(256) k_update(const SysDesc *__restrict__ sys, int k,
+                                                const int2 *__restrict__ pairs) {
+  const SysDesc S = sys[blockIdx.y];
+  const int2 pr = pairs[blockIdx.x];
+  const int i = pr.x, j = pr.y;
+  if (k >= S.nblk || j > S.J || k + j >= S.nblk) return;
+  extern __shared__ __align__(16) double smt[];
+  double *A = smt, *B = A + TSZ, *C = B + TSZ;
+  const size_t J1 = S.J + 1;
+  double *Ct = S.tiles + ((size_t)(k + j) * J1 + (j - i)) * TSZ;
+  tile_load(A, S.tiles + ((size_t)(k + i) * J1 + i) * TSZ);
+  tile_load(B, S.tiles + ((size_t)(k + j) * J1 + j) * TSZ);
+  tile_load(C, Ct);
+  __syncthreads();
+  tile_gemm_tn(C, A, B, -1.0, true);
+  __syncthreads();
+  tile_store(Ct, C);
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi diagonal (JACPCG)
+// ---------------------------------------------------------------------------
+
+// Element::HelmholtzDiag (src/element.cpp:1512-1561), emap order.
+__global__ void k_elem_diag(MeshView M, double hCon, double *__restrict__ ediag) {
+  const int e = blockIdx.x, np = M.np, nn = M.npnp;
+  const size_t eo = (size_t)e * nn;
+  const bool q3 = M.hasQ3[e];
+  for (int a = threadIdx.x; a < nn; a += blockDim.x) {
+    const int ij = M.emap[a], i = ij / np, j = ij - i * np;
+    double s = 0.0;
+    for (int q = 0; q < np; q++) s += M.Q1[eo + i * np + q] * (M.D[q * np + j] * M.D[q * np + j]);
+    double dg = s;
+    s = 0.0;
+    for (int p = 0; p < np; p++) s += M.Q2[eo + p * np + j] * (M.D[p * np + i] * M.D[p * np + i]);
+    dg += s;
+    if (q3) dg += 2.0 * M.Q3[eo + ij] * M.D[j * np + j] * M.D[i * np + i];
+    dg += hCon * M.Q4[eo + ij];
+    ediag[eo + a] = dg;
+  }
+}
+
+// PC[g] = 1 / (mixed terms + sum of element diagonals) for boundary nodes,
+// 1 / element diagonal for interior nodes (src/matrix.cpp:290-310).
+__global__ void k_diag_dss(MeshView M, const double *__restrict__ ediag, double *pc, float *pcf) {
+  const int npts = M.nglobal + M.nel * M.nint;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= npts) return;
+  double s = 0.0;
+  if (g < M.nglobal) {
+    for (int q = M.nat_ptr[g]; q < M.nat_ptr[g + 1]; q++) {
+      const int bi = M.nat_idx[q], b = bi / M.np, i = bi - b * M.np;
+      if (M.b_kind[b] == SX_BC_MIXED) s += M.b_K[b] * M.b_area[bi];
+    }
+    for (int q = M.g2e_ptr[g]; q < M.g2e_ptr[g + 1]; q++) {
+      const int ei = M.g2e_idx[q], e = ei / M.next, i = ei - e * M.next;
+      s += ediag[(size_t)e * M.npnp + i];
+    }
+  } else {
+    const int r = g - M.nglobal, e = r / M.nint, i = r - e * M.nint;
+    s = ediag[(size_t)e * M.npnp + M.next + i];
+  }
+  pc[g] = 1.0 / s;
+  pcf[g] = (float)(1.0 / s);
+}
+
+// ---------------------------------------------------------------------------
+// Host drivers
+// ---------------------------------------------------------------------------
+
+static int check_status(DBuf<int> &st) {
+  int h = 0;
+  SX_CUDA(cudaMemcpy(&h, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h & (1 << SX_ERR_SINGULAR_HII)) {
+    set_error("interior matrix hii is not positive definite");
+    return SX_ERR_SINGULAR_HII;
+  }
+  if (h & (1 << SX_ERR_BAND)) {
+    set_error("btog couples nodes further apart than nband - 1");
+    return SX_ERR_BAND;
+  }
+  if (h & (1 << SX_ERR_NOT_SPD)) {
+    set_error("failed to factor Helmholtz matrix (not positive definite)");
+    return SX_ERR_NOT_SPD;
+  }
+  return SX_OK;
+}
+
+size_t System::bytes() const {
+  return (tiles.n + dinv.n + hbi.n + hii.n + pc.n) * 8 + (hbif.n + hiif.n + pcf.n) * 4;
+}
+
+int factor_batch(std::vector<System *> &systems, cudaStream_t st) {
+  if (systems.empty()) return SX_OK;
+  std::vector<SysDesc> hd(systems.size());
+  int maxblk = 0, maxJ = 0;
+  for (size_t s = 0; s < systems.size(); s++) {
+    System &S = *systems[s];
+    hd[s] = SysDesc{S.tiles.p, S.dinv.p, S.nblk, S.J, S.status.p};
+    maxblk = std::max(maxblk, S.nblk);
+    maxJ = std::max(maxJ, S.J);
+  }
+  DBuf<SysDesc> dd;
+  SX_TRY(dd.upload(hd.data(), hd.size()));
+  std::vector<int2> pairs;
+  for (int j = 1; j <= maxJ; j++)
+    for (int i = 1; i <= j; i++) pairs.push_back(make_int2(i, j));
+  DBuf<int2> dpairs;
+  if (!pairs.empty()) SX_TRY(dpairs.upload(pairs.data(), pairs.size()));
+  const size_t sm3 = 3 * TSZ * sizeof(double), sm2 = 2 * TSZ * sizeof(double);
+  SX_CUDA(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  SX_CUDA(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  SX_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  const int ns = (int)systems.size();
+  for (int k = 0; k < maxblk; k++) {
+    k_potrf<<<ns, 256, sm2, st>>>(dd.p, k);
+    if (maxJ > 0) {
+      k_trsm<<<dim3(maxJ, ns), 256, sm3, st>>>(dd.p, k);
+      k_update<<<dim3((unsigned)pairs.size(), ns), 256, sm3, st>>>(dd.p, k, dpairs.p);
+    }
+  }
+  SX_CUDA(cudaGetLastError());
+  SX_CUDA(cudaStreamSynchronize(st));
+  return SX_OK;
+}
+
+int system_build_direct(System &S, cudaStream_t st) {
+  sx_mesh_s &Mh = *S.mesh;
+  const MeshView M = Mh.view();
+  const double hCon = S.betak2 + S.lambda2;
+  S.singular = (S.lambda2 + S.betak2) < EPSSP && (Mh.nglobal - Mh.nsolve) == 0 && !Mh.mixed;
+  S.nsolve = S.singular ? Mh.nsolve - 1 : Mh.nsolve;
+  const int kd = Mh.nband - 1;
+  S.nblk = (S.nsolve + NB - 1) / NB;
+  S.J = (kd + NB - 1) / NB;
+  if (S.status.p == nullptr) SX_TRY(S.status.alloc(1));
+  SX_TRY(S.status.zero(st));
+  SX_TRY(S.hbi.alloc((size_t)Mh.nel * Mh.next * Mh.nint));
+  SX_TRY(S.hii.alloc((size_t)Mh.nel * Mh.nint * Mh.nint));
+  DBuf<double> hbb;
+  SX_TRY(hbb.alloc((size_t)Mh.nel * Mh.next * Mh.next));
+  const size_t smem = condense_smem(M);
+  SX_CUDA(cudaFuncSetAttribute(k_elem_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_elem_condense<<<Mh.nel, 256, smem, st>>>(M, hCon, S.hbi.p, S.hii.p, hbb.p, S.status.p);
+  SX_CUDA(cudaGetLastError());
+  const size_t ntiles = (size_t)std::max(S.nblk, 1) * (S.J + 1);
+  SX_TRY(S.tiles.alloc(ntiles * TSZ));
+  SX_TRY(S.tiles.zero(st));
+  SX_TRY(S.dinv.alloc((size_t)std::max(S.nblk, 1) * TSZ));
+  SX_TRY(S.dinv.zero(st));
+  if (S.nsolve > 0) {
+    const int npad = S.nblk * NB - S.nsolve;
+    if (npad > 0) k_band_identity_pad<<<(npad + 127) / 128, 128, 0, st>>>(S.tiles.p, S.J, S.nsolve, S.nblk);
+    for (size_t c = 0; c + 1 < Mh.colour_ptr.size(); c++) {
+      const int n = Mh.colour_ptr[c + 1] - Mh.colour_ptr[c];
+      if (n > 0)
+        k_band_add<<<n, 256, 0, st>>>(M, Mh.dcolour_elmt.p + Mh.colour_ptr[c], hbb.p, S.tiles.p, S.J,
+                                      S.nsolve, S.status.p);
+    }
+    if (Mh.mixed) k_band_mixed<<<1, 1, 0, st>>>(M, S.tiles.p, S.J, S.nsolve);
+    SX_CUDA(cudaGetLastError());
+  }
+  SX_CUDA(cudaStreamSynchronize(st));
+  SX_TRY(check_status(S.status));
+  return SX_OK;
+}
+
+int system_build_jacobi(System &S, cudaStream_t st) {
+  sx_mesh_s &Mh = *S.mesh;
+  const MeshView M = Mh.view();
+  const double hCon = S.betak2 + S.lambda2;
+  S.singular = (S.lambda2 + S.betak2) < EPSSP && (Mh.nglobal - Mh.nsolve) == 0 && !Mh.mixed;
+  S.nsolve = S.singular ? Mh.nsolve - 1 : Mh.nsolve;
+  const int npts = Mh.nglobal + Mh.nel * Mh.nint;
+  DBuf<double> ediag;
+  SX_TRY(ediag.alloc((size_t)Mh.nel * Mh.npnp));
+  SX_TRY(S.pc.alloc(npts));
+  SX_TRY(S.pcf.alloc(npts));
+  k_elem_diag<<<Mh.nel, 128, 0, st>>>(M, hCon, ediag.p);
+  k_diag_dss<<<(npts + 255) / 256, 256, 0, st>>>(M, ediag.p, S.pc.p, S.pcf.p);
+  SX_CUDA(cudaGetLastError());
+  SX_CUDA(cudaStreamSynchronize(st));
+  return SX_OK;
+}
+
+// Copy the factor out of the tiles into LAPACK "U" band storage, ldab = nband.
+int system_band_export(const System &S, double *ab) {
+  const sx_mesh_s &Mh = *S.mesh;
+  const int nband = Mh.nband, kd = nband - 1;
+  std::vector<double> t((size_t)S.tiles.n);
+  SX_CUDA(cudaMemcpy(t.data(), S.tiles.p, t.size() * 8, cudaMemcpyDeviceToHost));
+  std::memset(ab, 0, sizeof(double) * (size_t)S.nsolve * nband);
+  for (int n = 0; n < S.nsolve; n++)
+    for (int m = std::max(0, n - kd); m <= n; m++) ab[(size_t)n * nband + kd + m - n] = t[tile_addr(m, n, S.J)];
+  return SX_OK;
+}
+
+}  // namespace sx

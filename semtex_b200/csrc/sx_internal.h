@@ -1,0 +1,179 @@
+// sx_internal.h -- shared declarations of the semtex_b200 library (not part
+// of the public C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/semtex_b200.h"
+
+namespace sx {
+
+// Reference tolerances (veclib/utility.h:35,39).
+constexpr double EPSSP = 6.0e-7;
+constexpr double EPSDP = 6.0e-14;
+
+// Band tiles: the condensed matrix is held as nb x nb tiles; tile (k, j)
+// holds U(rows of block k-j, cols of block k).  Rows are padded to
+// LDT = NB + 1 doubles so that both row- and column-wise smem traversals
+// are free of bank conflicts.
+constexpr int NB = 64;
+constexpr int LDT = NB + 1;
+constexpr int TSZ = NB * LDT;  // doubles per tile (33280 B, 16-B multiple)
+
+constexpr int NP_MIN = 3;
+constexpr int NP_MAX = 12;
+
+struct Status {
+  int code = SX_OK;
+  std::string msg;
+};
+
+// Thread-local last error message, for sx_status_string callers.
+void set_error(const char *fmt, ...);
+
+#define SX_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      ::sx::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+      return (e_ == cudaErrorMemoryAllocation) ? SX_ERR_NOMEM : SX_ERR_CUDA;          \
+    }                                                                                  \
+  } while (0)
+
+#define SX_TRY(call)            \
+  do {                          \
+    int s_ = (call);            \
+    if (s_ != SX_OK) return s_; \
+  } while (0)
+
+// Device buffer with RAII release.
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error("cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+      return SX_ERR_NOMEM;
+    }
+    n = count;
+    return SX_OK;
+  }
+  int upload(const T *h, size_t count) {
+    SX_TRY(alloc(count));
+    SX_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+    return SX_OK;
+  }
+  int zero(cudaStream_t s = 0) {
+    SX_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    return SX_OK;
+  }
+};
+
+// Device-side view of a mesh, passed by value to kernels.
+struct MeshView {
+  int np, npnp, next, nint, nel;
+  int nglobal, nsolve_ns, nband;
+  const double *D;       // np*np row-major, D[i][j] = h_j'(z_i)
+  const int *emap;       // npnp
+  const double *Q1, *Q2, *Q3, *Q4, *Q8;  // nel*npnp (Q3 zero when absent)
+  const float *Q1f, *Q2f, *Q3f, *Q4f;    // FP32 copies (mixed precision)
+  const unsigned char *hasQ3;            // nel
+  const int *btog, *bmask, *emask;       // nel*next, nel*next, nel
+  const int *g2e_ptr, *g2e_idx;          // CSR: global node -> (e*next+i), element order
+  const int *g2e_last;                   // nglobal: last (e*next+i) writing node (local2global)
+  int nbound;
+  const int *b_elmt, *b_side, *b_kind;
+  const double *b_K, *b_C, *b_area;      // b_area: nbound*np
+  const int *nat_ptr, *nat_idx;          // CSR: global node -> (b*np+i) natural/mixed terms
+  int mixed;                             // any mixed boundary
+};
+
+struct sx_mesh_impl;
+struct System;
+
+}  // namespace sx
+
+struct sx_mesh_s {
+  int device = 0;
+  int np = 0, npnp = 0, next = 0, nint = 0, nel = 0;
+  int nglobal = 0, nsolve = 0, nband = 0, nbound = 0;
+  bool mixed = false;
+  std::vector<double> z, w, D;
+  std::vector<int> emap, pmap;
+  std::vector<double> Q1, Q2, Q3, Q4, Q8;  // host copies
+  std::vector<unsigned char> hasQ3;
+  std::vector<int> btog, bmask, emask;
+  std::vector<int> b_elmt, b_side, b_kind;
+  std::vector<double> b_K, b_C, b_area;
+  std::vector<int> colour_ptr, colour_elmt;  // element colouring (no shared nodes)
+  // device
+  sx::DBuf<double> dD, dQ1, dQ2, dQ3, dQ4, dQ8, dK, dC, darea;
+  sx::DBuf<float> dQ1f, dQ2f, dQ3f, dQ4f;
+  sx::DBuf<unsigned char> dhasQ3;
+  sx::DBuf<int> demap, dbtog, dbmask, demask, dg2e_ptr, dg2e_idx, dg2e_last, dbe, dbs, dbk;
+  sx::DBuf<int> dnat_ptr, dnat_idx, dcolour_elmt;
+  sx::MeshView view() const;
+};
+
+namespace sx {
+
+// One MatrixSys: a (lambda2, betak2, method) system on a mesh.
+struct System {
+  sx_mesh_s *mesh = nullptr;
+  double lambda2 = 0.0, betak2 = 0.0;
+  int method = SX_DIRECT;
+  bool singular = false;
+  int nsolve = 0;
+  int nblk = 0, J = 0;     // band tiles: nblk block columns, J off-diagonal tiles
+  DBuf<double> tiles;      // nblk*(J+1)*TSZ
+  DBuf<double> dinv;       // nblk*TSZ: inverse of the diagonal U tiles
+  DBuf<double> hbi;        // nel*next*nint  (hbi hii^-1, row-major next x nint)
+  DBuf<double> hii;        // nel*nint*nint  (hii^-1, row-major)
+  DBuf<float> hbif, hiif;  // FP32 copies for the mixed form
+  DBuf<double> pc;         // npts: inverse Jacobi diagonal (JACPCG)
+  DBuf<float> pcf;         // FP32 copy
+  DBuf<int> status;        // device status bits (1 << SX_ERR_*)
+  size_t bytes() const;
+};
+
+int system_build_direct(System &S, cudaStream_t st);
+int system_build_jacobi(System &S, cudaStream_t st);
+int system_band_export(const System &S, double *ab);  // LAPACK band, host
+
+// Solve workspace for up to `planes` planes of one system.
+struct Work {
+  int planes = 0;
+  DBuf<double> Fb;      // planes*nel*next condensed element boundary forcing
+  DBuf<double> rhs;     // planes*npad
+  DBuf<double> gess;    // planes*nglobal essential values
+  DBuf<int> status;     // device status word
+  int reserve(const sx_mesh_s &M, int planes, int npad);
+};
+
+// Direct solve of P planes that share system S (P <= 2 in the plain form).
+// u, f: plane pointers (device), bc: plane bc lines (device) or nullptr.
+int direct_solve_planes(const System &S, Work &W, double *const *u, double *const *f,
+                        const double *const *bc, int P, cudaStream_t st);
+
+}  // namespace sx

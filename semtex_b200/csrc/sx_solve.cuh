@@ -1,0 +1,76 @@
+// sx_solve.cuh -- job descriptors and the element operator shared by the
+// direct and iterative solve kernels.
+#pragma once
+
+#include "sx_internal.h"
+
+namespace sx {
+
+// A set of P planes sharing one system.  Plane p of u / f / bc is at
+// u + p*ustride etc.
+struct Job {
+  double *u;
+  double *f;
+  const double *bc;
+  long long ustride, fstride, bcstride;
+  int P;
+  double hCon;          // lambda2 + betak2
+  int nsolve;           // system nsolve (reduced by one when singular)
+  // DIRECT
+  const double *hbi, *hii;
+  const double *tiles, *dinv;
+  int nblk, J, npad;
+  double *rhs;          // P * rhs_stride
+  long long rhs_stride;
+  double *Fb;           // P * nel * next
+  double *gess;         // P * nglobal
+  // JACPCG
+  const double *pc;
+};
+
+// out = A_e u for one element (Element::HelmholtzOp + HelmholtzKern,
+// src/element.cpp:1564-1650, Cartesian): R = u DT, S = D u, pointwise
+// geometric factors, out = Q4 u hCon + DT S + R D.  All arrays np*np
+// row-major in shared memory; ends with __syncthreads().
+template <int NP, typename T>
+__device__ __forceinline__ void helm_op(const T *D, const T *Q1, const T *Q2, const T *Q3, const T *Q4,
+                                        bool q3, T hCon, const T *u, T *R, T *S, T *out, int nthreads) {
+  constexpr int NN = NP * NP;
+  for (int idx = threadIdx.x; idx < NN; idx += nthreads) {
+    const int i = idx / NP, j = idx - i * NP;
+    T r = 0, s = 0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      r += u[i * NP + k] * D[j * NP + k];
+      s += D[i * NP + k] * u[k * NP + j];
+    }
+    if (q3) {
+      R[idx] = Q1[idx] * r + Q3[idx] * s;
+      S[idx] = Q2[idx] * s + Q3[idx] * r;
+    } else {
+      R[idx] = Q1[idx] * r;
+      S[idx] = Q2[idx] * s;
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NN; idx += nthreads) {
+    const int i = idx / NP, j = idx - i * NP;
+    T t = Q4[idx] * u[idx] * hCon;
+    T a = 0, b = 0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      a += D[k * NP + i] * S[k * NP + j];
+      b += R[i * NP + k] * D[k * NP + j];
+    }
+    out[idx] = t + a + b;
+  }
+  __syncthreads();
+}
+
+int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
+                      cudaStream_t st);
+size_t band_smem(int pmax);
+// Set kernel attributes (max dynamic smem) ahead of any stream capture.
+int prepare_direct_kernels(const MeshView &M);
+
+}  // namespace sx
