@@ -93,6 +93,7 @@ typedef struct {
   int iterations_total; /* PCG: sum over planes                                 */
   int refinements;      /* mixed precision: outer refinement steps taken        */
   double final_rel_residual; /* mixed precision / PCG: max ||r||/||b||          */
+  int kernel_launches;  /* kernels this call enqueued (graph nodes included)    */
 } sx_solve_stats;
 
 /* ---- library ------------------------------------------------------------ */
@@ -131,6 +132,10 @@ SX_API int sx_modal_create_ex(sx_mesh mesh, int base_mode, int num_modes, const 
 SX_API int sx_modal_destroy(sx_modal modal);
 /* Band factor of local mode m, in LAPACK "U" band storage
  * (ldab = nband, veclib/lapack.h:107-108): nsolve*nband doubles. */
+/* Status of the device work enqueued so far on this system: synchronises
+ * the device, returns SX_OK or the first recorded device-side error (e.g.
+ * SX_ERR_TIMEOUT from a bounded wait) and clears it. */
+SX_API int sx_modal_status(sx_modal modal);
 /* Device memory held by the modal system (factors, element matrices). */
 SX_API unsigned long long sx_modal_device_bytes(sx_modal modal);
 SX_API int sx_modal_band(sx_modal modal, int m, double *ab, int *nsolve, int *singular);
@@ -159,6 +164,18 @@ SX_API int sx_field_solve_device(sx_modal modal, double *d_u, double *d_f, const
 SX_API int sx_field_solve_batched(sx_modal modal, double *d_u, double *d_f, const double *d_bc, int nz,
                            int plane_stride, int precision, double tol_rel, int max_refine,
                            void *stream, sx_solve_stats *stats);
+/* Batched form on HOST buffers: copies f (and bc) to the device, solves,
+ * copies u back; synchronous.  u is output only (the solve starts from
+ * zero).  Pinned (page-locked) host buffers give full copy bandwidth. */
+SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *f, const double *bc,
+                                int nz, int plane_stride, int precision, double tol_rel,
+                                int max_refine, sx_solve_stats *stats);
+
+/* Profiling hook (no reference counterpart): re-launch only the banded
+ * forward/backward sweeps of the last batched solve `reps` times on
+ * `stream`, so the dominant kernel can be timed on its own.  The RHS
+ * workspace is overwritten; call after sx_field_solve_batched. */
+SX_API int sx_profile_band_sweeps(sx_modal modal, int reps, void *stream);
 
 #ifdef __cplusplus
 }

@@ -143,9 +143,13 @@ class OracleSystem:
         f = np.ascontiguousarray(forcing, dtype=np.float64).reshape(-1).copy()
         u = (np.zeros(m.nplane) if unknown is None
              else np.ascontiguousarray(unknown, dtype=np.float64).reshape(-1).copy())
-        b = np.ascontiguousarray(bc, dtype=np.float64).reshape(-1)
-        if b.size == 0:
-            b = np.zeros(m.np)
+        nb = max(len(m.boundaries), 1)
+        if bc is None:
+            b = np.zeros(nb * m.np)
+        else:
+            b = np.ascontiguousarray(bc, dtype=np.float64).reshape(-1)
+        if b.size != nb * m.np:
+            raise ValueError(f"bc has {b.size} values, expected nbound*np = {nb * m.np}")
         it = lib().orc_solve_plane(self.h, u, f, b, tol_rel, step_max)
         return u, it
 

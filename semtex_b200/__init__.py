@@ -51,7 +51,7 @@ class MeshDesc(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("planes_solved", C.c_int), ("iterations_max", C.c_int),
                 ("iterations_total", C.c_int), ("refinements", C.c_int),
-                ("final_rel_residual", C.c_double)]
+                ("final_rel_residual", C.c_double), ("kernel_launches", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -80,8 +80,11 @@ def _load():
     L.sx_modal_band.argtypes = [vp, ip, P(dp), P(ip), P(ip)]
     L.sx_field_solve.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, dp, ip, P(SolveStats)]
     L.sx_field_solve_device.argtypes = [vp, vp, vp, vp, ip, ip, dp, ip, vp, P(SolveStats)]
-    if hasattr(L, "sx_field_solve_batched"):
-        L.sx_field_solve_batched.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(SolveStats)]
+    L.sx_field_solve_batched.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(SolveStats)]
+    L.sx_field_solve_batched_host.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, ip, dp, ip,
+                                              P(SolveStats)]
+    L.sx_profile_band_sweeps.argtypes = [vp, ip, vp]
+    L.sx_modal_status.argtypes = [vp]
     return L
 
 
@@ -221,6 +224,28 @@ class ModalMatrixSys:
                                         max_refine, stream, C.byref(st))
         _check(rc, "sx_field_solve_batched", allow=(OK, WARN_STEP_LIMIT))
         return st.as_dict()
+
+    def solve_batched_host(self, forcing, bc=None, out=None, precision=FP64, tol_rel=1e-12,
+                           max_refine=8):
+        """Batched form on host arrays (pinned arrays copy fastest); returns u."""
+        qm = self.mesh.qm
+        f = np.ascontiguousarray(forcing, dtype=np.float64)
+        nz = f.shape[0]
+        u = out if out is not None else np.empty_like(f)
+        b = self._bc_array(bc, nz)
+        st = SolveStats()
+        rc = lib.sx_field_solve_batched_host(self.h, _dptr(u), _dptr(f),
+                                             _dptr(b) if b is not None else None, nz, qm.nplane,
+                                             precision, tol_rel, max_refine, C.byref(st))
+        _check(rc, "sx_field_solve_batched_host", allow=(OK, WARN_STEP_LIMIT))
+        self.last_stats = st.as_dict()
+        return u
+
+    def profile_band_sweeps(self, reps, stream=0):
+        _check(lib.sx_profile_band_sweeps(self.h, reps, stream), "sx_profile_band_sweeps")
+
+    def status(self):
+        return _check(lib.sx_modal_status(self.h), "sx_modal_status")
 
     def close(self):
         if getattr(self, "h", None) and lib is not None:

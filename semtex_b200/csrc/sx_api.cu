@@ -32,6 +32,20 @@ struct sx_modal_s {
   const void *gkey[3] = {nullptr, nullptr, nullptr};
   int gnz = 0, gstride = 0, gprec = -1;
   DBuf<Job> bjobs;
+  std::vector<Job> gjobs;            // host copy of the captured jobs
+  int gC = 1, glaunches = 0;         // their band-sweep cluster size, kernel count
+  DBuf<int> dstatus;                 // device status bits of the last solves
+  std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
+  int cluster(int nj) {
+    auto it = cluster_for.find(nj);
+    if (it != cluster_for.end()) return it->second;
+    int J = 1;
+    for (auto &s : uniq) J = std::max(J, s->J);
+    // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
+    const int c = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2);
+    cluster_for[nj] = c;
+    return c;
+  }
   ~sx_modal_s() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (own) cudaStreamDestroy(own);
@@ -110,6 +124,8 @@ static int modal_build(sx_mesh m, int base_mode, int num_modes, const double *la
     }
     M->sys.push_back(found);
   }
+  SX_TRY(M->dstatus.alloc(1));
+  SX_TRY(M->dstatus.zero(st));
   SX_TRY(factor_batch(to_factor, st));
   for (System *S : to_factor) {
     int h = 0;
@@ -153,6 +169,25 @@ extern "C" int sx_modal_band(sx_modal s, int m, double *ab, int *nsolve, int *si
   if (S.method != SX_DIRECT) return SX_ERR_ARG;
   if (ab) SX_TRY(system_band_export(S, ab));
   return SX_OK;
+}
+
+// Device-side status of the solves enqueued so far (bounded waits that ran
+// out, ...).  Synchronises the device; clears the word when `clear`.
+static int take_status(sx_modal s, bool clear) {
+  int h = 0;
+  SX_CUDA(cudaDeviceSynchronize());
+  SX_CUDA(cudaMemcpy(&h, s->dstatus.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (clear && h) SX_CUDA(cudaMemset(s->dstatus.p, 0, sizeof(int)));
+  if (h & (1 << SX_ERR_TIMEOUT)) {
+    set_error("a bounded device-side wait ran out (band sweep)");
+    return SX_ERR_TIMEOUT;
+  }
+  return SX_OK;
+}
+
+extern "C" int sx_modal_status(sx_modal s) {
+  if (!s) return SX_ERR_ARG;
+  return take_status(s, true);
 }
 
 extern "C" unsigned long long sx_modal_device_bytes(sx_modal s) {
@@ -227,6 +262,7 @@ static Job make_job(sx_modal_s &M, const Group &g, int slot, double *u, double *
   j.Fb = M.Fb.p + (size_t)slot * Mh.nel * Mh.next;
   j.gess = M.gess.p + (size_t)slot * Mh.nglobal;
   j.pc = S.pc.p;
+  j.status = M.dstatus.p;
   return j;
 }
 
@@ -258,11 +294,14 @@ extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const
     const System &S = *s->sys[groups[i].mode];
     std::vector<Job> one(1, jobs[i]);
     if (S.method == SX_DIRECT) {
-      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st));
+      int nl = 0;
+      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st, s->cluster(1), &nl));
+      loc.kernel_launches += nl;
     } else {
       int iters = 0;
       double rr = 0.0;
-      const int r = pcg_solve_job(M, S, s->pcg, jobs[i], tol_rel, step_max, st, &iters, &rr);
+      const int r = pcg_solve_job(M, S, s->pcg, jobs[i], tol_rel, step_max, st, &iters, &rr,
+                                  &loc.kernel_launches);
       if (r != SX_OK && r != SX_WARN_STEP_LIMIT) return r;
       if (r == SX_WARN_STEP_LIMIT) rc = SX_WARN_STEP_LIMIT;
       loc.iterations_max = std::max(loc.iterations_max, iters);
@@ -290,6 +329,7 @@ extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc
   const int rc = sx_field_solve_device(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride,
                                        tol_rel, step_max, nullptr, stats);
   if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  SX_TRY(take_status(s, true));
   SX_CUDA(cudaMemcpy(u, s->hu.p, n * 8, cudaMemcpyDeviceToHost));
   return rc;
 }
@@ -343,9 +383,12 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
     const MeshView M = s->mesh->view();
     // warm the kernel attributes outside capture
     SX_TRY(prepare_direct_kernels(M));
+    const int C = s->cluster((int)jobs.size());
     cudaGraph_t g = nullptr;
     SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st);
+    const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches);
+    s->gjobs = jobs;
+    s->gC = C;
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc != SX_OK) {
       if (g) cudaGraphDestroy(g);
@@ -363,10 +406,40 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
     s->gprec = precision;
   }
   SX_CUDA(cudaGraphLaunch(s->gexec, st));
-  if (!stream) SX_CUDA(cudaStreamSynchronize(st));
+  if (!stream) SX_TRY(take_status(s, true));
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->planes_solved = planes;
+    stats->kernel_launches = s->glaunches;
   }
+  return SX_OK;
+}
+
+extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *f, const double *bc,
+                                           int nz, int plane_stride, int precision, double tol_rel,
+                                           int max_refine, sx_solve_stats *stats) {
+  if (!s || !u || !f || nz <= 0 || plane_stride <= 0) return SX_ERR_ARG;
+  const size_t n = (size_t)nz * plane_stride;
+  const size_t nbc = (size_t)nz * std::max(s->mesh->nbound, 1) * s->mesh->np;
+  if (s->hu.n < n) SX_TRY(s->hu.alloc(n));
+  if (s->hf.n < n) SX_TRY(s->hf.alloc(n));
+  if (bc && s->hbc.n < nbc) SX_TRY(s->hbc.alloc(nbc));
+  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
+  cudaStream_t st = s->own;
+  SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));
+  if (bc) SX_CUDA(cudaMemcpyAsync(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice, st));
+  const int rc = sx_field_solve_batched(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride,
+                                        precision, tol_rel, max_refine, st, stats);
+  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  SX_CUDA(cudaMemcpyAsync(u, s->hu.p, n * 8, cudaMemcpyDeviceToHost, st));
+  SX_CUDA(cudaStreamSynchronize(st));
+  SX_TRY(take_status(s, true));
+  return rc;
+}
+
+extern "C" int sx_profile_band_sweeps(sx_modal s, int reps, void *stream) {
+  if (!s || reps <= 0 || s->gjobs.empty()) return SX_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int r = 0; r < reps; r++) SX_TRY(band_sweep_jobs(s->bjobs.p, s->gjobs, s->gC, st));
   return SX_OK;
 }

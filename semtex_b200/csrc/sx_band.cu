@@ -1,0 +1,360 @@
+// sx_band.cu -- banded triangular solves U^T y = b, U x = y (LAPACK
+// dpbtrs "U" as called at src/field.cpp:609) on the tiled band factor.
+//
+// Both sweeps are left-looking over block columns of NB rows:
+//   forward  y_k = D_k^T (b_k - sum_{j>=1} T(k,j)^T   y_{k-j})
+//   backward x_k = D_k   (y_k - sum_{j>=1} T(k+j,j)   x_{k+j})
+// with T(k,j) = U(rows of block k-j, cols of block k) and D_k = U_kk^-1.
+//
+// One thread-block cluster of C CTAs works on one system (all P right-hand
+// sides of the job at once).  The leader CTA (rank 0) owns the critical
+// path: the j = 1 tile (needs the block just solved) and D_k; ranks 1..C-1
+// own the older tiles j >= 2 round-robin, so they run ahead while the
+// leader finishes the previous block.  Tiles stream into each CTA through a
+// ring of 1-D TMA bulk copies (cp.async.bulk + mbarrier complete_tx).
+// Partial sums go to the leader, and each solved block goes back to every
+// rank's ring of recent blocks, over distributed shared memory with
+// mbarrier release/acquire at cluster scope.  Partials are combined in rank
+// order, so the result does not depend on timing.
+//
+// Every wait is bounded (clock64); on timeout the kernel records
+// SX_ERR_TIMEOUT in the status word, drains its own bulk copies (bounded),
+// meets the other CTAs at a final cluster barrier and returns.
+#include "sx_kernels.cuh"
+#include "sx_ptx.cuh"
+#include "sx_solve.cuh"
+
+namespace sx {
+
+constexpr long long WAIT_LIMIT = 4000000000LL;  // ~2 s at 1.9 GHz
+
+struct SweepGeom {
+  int nblk, J, C, rank;
+  // tiles owned by `rank` at sequence step t (t < nblk: forward block t,
+  // else backward block 2 nblk - 1 - t); D_k is always last, on rank 0.
+  __device__ __forceinline__ int jmax(int t) const {
+    return t < nblk ? min(J, t) : min(J, nblk - 1 - (2 * nblk - 1 - t));
+  }
+  __device__ __forceinline__ int count(int t) const {
+    const int jm = jmax(t);
+    if (C == 1) return jm + 1;
+    if (rank == 0) return (jm >= 1 ? 1 : 0) + 1;
+    const int j0 = rank + 1;
+    return jm >= j0 ? (jm - j0) / (C - 1) + 1 : 0;
+  }
+  // j of the idx-th owned tile (0 = D_k)
+  __device__ __forceinline__ int jat(int t, int idx) const {
+    const int jm = jmax(t);
+    if (C == 1) return idx < jm ? jm - idx : 0;
+    if (rank == 0) return (jm >= 1 && idx == 0) ? 1 : 0;
+    const int j0 = rank + 1;
+    const int top = j0 + ((jm - j0) / (C - 1)) * (C - 1);
+    return top - idx * (C - 1);
+  }
+};
+
+__device__ __forceinline__ const double *tile_src(const Job &Jb, int t, int j) {
+  const int nblk = Jb.nblk;
+  const size_t J1 = Jb.J + 1;
+  if (t < nblk) {
+    const int k = t;
+    return j ? Jb.tiles + ((size_t)k * J1 + j) * TSZ : Jb.dinv + (size_t)k * TSZ;
+  }
+  const int k = 2 * nblk - 1 - t;
+  return j ? Jb.tiles + ((size_t)(k + j) * J1 + j) * TSZ : Jb.dinv + (size_t)k * TSZ;
+}
+
+template <int PMAX>
+__global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ jobs, int C, int S, int Wmax) {
+  const int rank = (int)cluster_ctarank();
+  const Job Jb = jobs[blockIdx.x / C];
+  const int P = Jb.P, nblk = Jb.nblk, W = Jb.J + 2;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  double *ring = reinterpret_cast<double *>(smraw);      // S * TSZ
+  double *ybuf = ring + (size_t)S * TSZ;                 // Wmax * PMAX * NB
+  double *pbuf = ybuf + (size_t)Wmax * PMAX * NB;        // 2 * (C-1) * PMAX * NB
+  double *qpart = pbuf + (size_t)2 * max(C - 1, 1) * PMAX * NB;  // 4 * PMAX * NB
+  double *acc = qpart + 4 * PMAX * NB;                   // PMAX * NB
+  double *yk = acc + PMAX * NB;                          // PMAX * NB
+  uint64_t *full = reinterpret_cast<uint64_t *>(yk + PMAX * NB);  // S
+  uint64_t *ybar = full + S;                             // Wmax
+  uint64_t *pbar = ybar + Wmax;                          // 2
+  __shared__ int abort_flag;
+
+  const int tid = threadIdx.x, c = tid & (NB - 1), q = tid >> 6;
+  const SweepGeom G{nblk, Jb.J, C, rank};
+  if (tid == 0) {
+    for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+    for (int w = 0; w < Wmax; w++) mbar_init(&ybar[w], 1);
+    mbar_init(&pbar[0], max(C - 1, 1));
+    mbar_init(&pbar[1], max(C - 1, 1));
+    fence_mbar_init_cluster();
+    abort_flag = 0;
+  }
+  __syncthreads();
+  cluster_sync_all();
+
+  const int T = 2 * nblk;
+  // producer state (thread 0): next tile (tp, ip); counters are uniform.
+  int tp = 0, ip = 0;
+  long long nissued = 0, ncons = 0;
+  auto produce = [&](long long limit) {
+    while (nissued < limit) {
+      while (tp < T && ip >= G.count(tp)) {
+        tp++;
+        ip = 0;
+      }
+      if (tp >= T) return;
+      const int j = G.jat(tp, ip);
+      double *dst = ring + (size_t)(nissued % S) * TSZ;
+      uint64_t *bar = &full[nissued % S];
+      mbar_arrive_expect_tx(bar, (uint32_t)(TSZ * sizeof(double)));
+      bulk_g2s(dst, tile_src(Jb, tp, j), (uint32_t)(TSZ * sizeof(double)), bar);
+      nissued++;
+      ip++;
+    }
+  };
+  if (tid == 0) produce(S);
+
+  for (int t = 0; t < T; t++) {
+    const bool fwd = t < nblk;
+    const int k = fwd ? t : 2 * nblk - 1 - t;
+    const int n = G.count(t);
+    double s[PMAX];
+#pragma unroll
+    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
+    bool bad = false;
+    for (int idx = 0; idx < n; idx++) {
+      const int j = G.jat(t, idx);
+      if (j == 0) break;  // D_k: handled below by the leader
+      const int slot = (int)(ncons % S);
+      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), WAIT_LIMIT)) bad = true;
+      const int src = t - j, w = src % W;
+      if (rank != 0 && !mbar_wait(&ybar[w], (uint32_t)((src / W) & 1), WAIT_LIMIT)) bad = true;
+      if (bad) abort_flag = 1;
+      __syncthreads();
+      if (abort_flag) break;
+      const double *Tt = ring + (size_t)slot * TSZ;
+      const double *yv = ybuf + (size_t)w * PMAX * NB;
+      if (fwd) {
+#pragma unroll 4
+        for (int rr = q * 16; rr < q * 16 + 16; rr++) {
+          const double tv = Tt[rr * LDT + c];
+#pragma unroll
+          for (int p = 0; p < PMAX; p++)
+            if (p < P) s[p] += tv * yv[p * NB + rr];
+        }
+      } else {
+#pragma unroll 4
+        for (int cc = q * 16; cc < q * 16 + 16; cc++) {
+          const double tv = Tt[c * LDT + cc];
+#pragma unroll
+          for (int p = 0; p < PMAX; p++)
+            if (p < P) s[p] += tv * yv[p * NB + cc];
+        }
+      }
+      __syncthreads();
+      ncons++;
+      if (tid == 0) produce(ncons + S);
+    }
+    if (abort_flag) break;
+    // reduce the four row quarters in fixed order
+#pragma unroll
+    for (int p = 0; p < PMAX; p++)
+      if (p < P) qpart[(q * PMAX + p) * NB + c] = s[p];
+    __syncthreads();
+    if (rank != 0) {
+      // The leader reads pbuf[t & 1] of step t-2 before it publishes block
+      // t-2; seeing that block means the slot is free again.
+      if (t >= 2) {
+        const int src = t - 2;
+        if (!mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) abort_flag = 1;
+        __syncthreads();
+        if (abort_flag) break;
+      }
+      // partial -> leader's pbuf[t & 1][rank-1]
+      if (q == 0) {
+        for (int p = 0; p < P; p++) {
+          const double v = qpart[(0 * PMAX + p) * NB + c] + qpart[(1 * PMAX + p) * NB + c] +
+                           qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
+          double *dst = pbuf + ((size_t)((t & 1) * (C - 1) + (rank - 1)) * PMAX + p) * NB + c;
+          st_cluster_f64(map_rank(dst, 0), v);
+        }
+        fence_acq_rel_cluster();
+      }
+      __syncthreads();
+      if (tid == 0) mbar_arrive_cluster(map_rank(&pbar[t & 1], 0));
+      continue;
+    }
+    // ---- leader: combine partials, apply D_k, broadcast ----
+    if (C > 1) {
+      if (!mbar_wait(&pbar[t & 1], (uint32_t)((t >> 1) & 1), WAIT_LIMIT)) abort_flag = 1;
+    }
+    {
+      const int slot = (int)(ncons % S);
+      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), WAIT_LIMIT)) abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    if (q == 0) {
+      for (int p = 0; p < P; p++) {
+        double v = qpart[(0 * PMAX + p) * NB + c] + qpart[(1 * PMAX + p) * NB + c] +
+                   qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
+        for (int r = 1; r < C; r++) v += pbuf[((size_t)((t & 1) * (C - 1) + (r - 1)) * PMAX + p) * NB + c];
+        acc[p * NB + c] = Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] - v;
+      }
+    }
+    __syncthreads();
+    {
+      const double *Dk = ring + (size_t)(ncons % S) * TSZ;
+#pragma unroll
+      for (int p = 0; p < PMAX; p++) s[p] = 0.0;
+      for (int cc = q * 16; cc < q * 16 + 16; cc++) {
+        const double dv = fwd ? Dk[cc * LDT + c] : Dk[c * LDT + cc];
+#pragma unroll
+        for (int p = 0; p < PMAX; p++)
+          if (p < P) s[p] += dv * acc[p * NB + cc];
+      }
+    }
+    __syncthreads();  // all reads of D_k done
+    ncons++;
+    if (tid == 0) produce(ncons + S);
+#pragma unroll
+    for (int p = 0; p < PMAX; p++)
+      if (p < P) qpart[(q * PMAX + p) * NB + c] = s[p];
+    __syncthreads();
+    if (q == 0)
+      for (int p = 0; p < P; p++) {
+        const double v = qpart[(0 * PMAX + p) * NB + c] + qpart[(1 * PMAX + p) * NB + c] +
+                         qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
+        yk[p * NB + c] = v;
+        Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] = v;
+      }
+    __syncthreads();
+    // broadcast block t into slot t % W of every rank's ring
+    const int w = t % W;
+    const int tot = C * P * NB;
+    for (int i = tid; i < tot; i += 256) {
+      const int r = i / (P * NB), rem = i - r * P * NB, p = rem / NB, cc = rem - p * NB;
+      double *dst = ybuf + ((size_t)w * PMAX + p) * NB + cc;
+      if (r == 0)
+        *dst = yk[p * NB + cc];
+      else
+        st_cluster_f64(map_rank(dst, (uint32_t)r), yk[p * NB + cc]);
+    }
+    fence_acq_rel_cluster();
+    __syncthreads();
+    if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[w], (uint32_t)tid));
+  }
+
+  if (abort_flag) {
+    if (tid == 0) {
+      atomicOr(Jb.status, 1 << SX_ERR_TIMEOUT);
+      // drain this CTA's bulk copies still in flight (bounded)
+      for (long long i = ncons; i < nissued; i++) mbar_wait(&full[i % S], (uint32_t)((i / S) & 1), WAIT_LIMIT);
+    }
+    __syncthreads();
+  }
+  cluster_sync_all();
+}
+
+size_t sweep_smem(int pmax, int C, int S, int Wmax) {
+  return sizeof(double) * ((size_t)S * TSZ + (size_t)Wmax * pmax * NB +
+                           (size_t)2 * std::max(C - 1, 1) * pmax * NB + 6 * (size_t)pmax * NB) +
+         sizeof(uint64_t) * (S + Wmax + 2);
+}
+
+// Dynamic shared memory available to the sweep kernels: the opt-in limit
+// minus their static shared memory.
+static int smem_optin() {
+  static int v = 0;
+  if (!v) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes a2, a8;
+    cudaFuncGetAttributes(&a2, k_band_sweep<2>);
+    cudaFuncGetAttributes(&a8, k_band_sweep<8>);
+    v = optin - (int)std::max(a2.sharedSizeBytes, a8.sharedSizeBytes);
+  }
+  return v;
+}
+
+// Launch both sweeps for every job: cluster size C per job.
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st) {
+  const int nj = (int)hjobs.size();
+  if (nj == 0) return SX_OK;
+  int maxP = 0, Wmax = 0;
+  for (const Job &j : hjobs) {
+    maxP = std::max(maxP, j.P);
+    Wmax = std::max(Wmax, j.J + 2);
+  }
+  if (maxP > 8) return SX_ERR_UNSUPPORTED;
+  const int pmax = maxP <= 2 ? 2 : 8;
+  const int limit = smem_optin();
+  int S = 4;
+  while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)limit) S--;
+  const size_t sm = sweep_smem(pmax, C, S, Wmax);
+  if (sm > (size_t)limit) {
+    set_error("band sweep needs %zu B of shared memory (limit %d)", sm, limit);
+    return SX_ERR_UNSUPPORTED;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C * nj, 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (pmax == 2)
+    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<2>, djobs, C, S, Wmax));
+  else
+    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<8>, djobs, C, S, Wmax));
+  return SX_OK;
+}
+
+int prepare_band_kernels() {
+  const int limit = smem_optin();
+  SX_CUDA(cudaFuncSetAttribute(k_band_sweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  SX_CUDA(cudaFuncSetAttribute(k_band_sweep<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  SX_CUDA(cudaFuncSetAttribute(k_band_sweep<2>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  SX_CUDA(cudaFuncSetAttribute(k_band_sweep<8>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  return SX_OK;
+}
+
+// Largest cluster size (<= cmax) for which `nj` clusters can be resident at
+// once; at least 1.
+int pick_cluster(int nj, int cmax, int pmax, int Wmax) {
+  int best = 1;
+  for (int C = 1; C <= cmax; C++) {
+    int S = 4;
+    while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * nj, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = sweep_smem(pmax, C, S, Wmax);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    const cudaError_t e = pmax == 2 ? cudaOccupancyMaxActiveClusters(&n, k_band_sweep<2>, &cfg)
+                                    : cudaOccupancyMaxActiveClusters(&n, k_band_sweep<8>, &cfg);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (n >= nj) best = C;
+  }
+  return best;
+}
+
+}  // namespace sx

@@ -289,7 +289,7 @@ int global_op(const MeshView &M, double hCon, const double *x, double *y, double
 }
 
 int pcg_solve_job(const MeshView &M, const System &S, PcgWork &W, const Job &job, double tol_rel,
-                  int step_max, cudaStream_t st, int *iters_max, double *rel_res) {
+                  int step_max, cudaStream_t st, int *iters_max, double *rel_res, int *launches) {
   SX_TRY(W.reserve(M));
   const int npts = M.nglobal + M.nel * M.nint;
   const int nsolve = S.nsolve, nzero = M.nglobal - nsolve;
@@ -343,6 +343,14 @@ int pcg_solve_job(const MeshView &M, const System &S, PcgWork &W, const Job &job
       r2 = hs[S_R2];
     }
     if (i == step_max) rc = SX_WARN_STEP_LIMIT;
+    // kernels enqueued for this plane: RHS + initial residual (10, + 3 range
+    // zeroings when there are essential nodes, + 1 for BC values), 9 (+1)
+    // per iteration body, 1 to unpack
+    if (launches) {
+      const int zr = nzero > 0 ? 1 : 0;
+      const int bodies = (i == step_max) ? i - 1 : i;
+      *launches += 10 + 3 * zr + (bc ? 1 : 0) + bodies * (9 + zr) + 1;
+    }
     k_g2l<<<M.nel, 128, 0, st>>>(M, W.x.p, g, u);
     SX_CUDA(cudaGetLastError());
     *iters_max = std::max(*iters_max, i);

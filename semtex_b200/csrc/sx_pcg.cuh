@@ -16,7 +16,7 @@ struct PcgWork {
 // Solve every plane of `job` with the reference's JACPCG iteration
 // (src/field.cpp:627-720).  Returns SX_OK or SX_WARN_STEP_LIMIT.
 int pcg_solve_job(const MeshView &M, const System &S, PcgWork &W, const Job &job, double tol_rel,
-                  int step_max, cudaStream_t st, int *iters_max, double *rel_res);
+                  int step_max, cudaStream_t st, int *iters_max, double *rel_res, int *launches);
 
 // y = A x on global vectors (Field::HelmholtzOperator, src/field.cpp:771-856).
 int global_op(const MeshView &M, double hCon, const double *x, double *y, double *Ye, cudaStream_t st);

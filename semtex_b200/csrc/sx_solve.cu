@@ -13,8 +13,8 @@
 //   k_rhs_dss     direct-stiffness sum of F_b into the global RHS in element
 //                 order, then <h, w> natural/mixed terms in boundary order, then
 //                 the essential tail zeroed (src/field.cpp:892-924)
-//   k_band_fwd    U^T y = b   } banded triangular solves, LAPACK dpbtrs "U"
-//   k_band_bwd    U x = y     } (src/field.cpp:609), over nb x nb tiles
+//   band sweeps   U^T y = b, U x = y: LAPACK dpbtrs "U" (src/field.cpp:609),
+//                 one thread-block cluster per job (sx_band.cu)
 //   k_backsub     global2localSC: u_i = hii^-1 F_i - (hii^-1 h_ib) u_b
 //                 (src/element.cpp:398-438), then setEssential
 //                 (src/field.cpp:1022-1040)
@@ -135,141 +135,6 @@ __global__ void k_rhs_dss(MeshView M, const Job *__restrict__ jobs) {
 }
 
 // ---------------------------------------------------------------------------
-// Banded triangular solves over tiles
-// ---------------------------------------------------------------------------
-
-// Forward: y_k = D_k^T (b_k - sum_j T(k,j)^T y_{k-j}), D_k = U_kk^-1.
-// Thread t owns column c = t % 64 and row quarter q = t / 64.
-template <int PMAX>
-__global__ void __launch_bounds__(256) k_band_fwd(const Job *__restrict__ jobs) {
-  const Job J = jobs[blockIdx.x];
-  const int P = J.P, nblk = J.nblk, Jt = J.J;
-  extern __shared__ __align__(16) double smb[];
-  double *T = smb;                      // TSZ
-  double *part = T + TSZ;               // 4 * PMAX * NB
-  double *acc = part + 4 * PMAX * NB;   // PMAX * NB
-  const int tid = threadIdx.x, c = tid & (NB - 1), q = tid >> 6;
-  for (int k = 0; k < nblk; k++) {
-    double s[PMAX];
-#pragma unroll
-    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
-    const int jmax = min(Jt, k);
-    for (int j = jmax; j >= 1; j--) {
-      __syncthreads();
-      const double2 *src = reinterpret_cast<const double2 *>(J.tiles + ((size_t)k * (Jt + 1) + j) * TSZ);
-      for (int i = tid; i < TSZ / 2; i += 256) reinterpret_cast<double2 *>(T)[i] = src[i];
-      __syncthreads();
-      const size_t ro = (size_t)(k - j) * NB;
-#pragma unroll 4
-      for (int rr = q * 16; rr < q * 16 + 16; rr++) {
-        const double tv = T[rr * LDT + c];
-#pragma unroll
-        for (int p = 0; p < PMAX; p++)
-          if (p < P) s[p] += tv * J.rhs[(size_t)p * J.rhs_stride + ro + rr];
-      }
-    }
-#pragma unroll
-    for (int p = 0; p < PMAX; p++)
-      if (p < P) part[(q * PMAX + p) * NB + c] = s[p];
-    __syncthreads();
-    if (q == 0)
-      for (int p = 0; p < P; p++) {
-        const double t = part[(0 * PMAX + p) * NB + c] + part[(1 * PMAX + p) * NB + c] +
-                         part[(2 * PMAX + p) * NB + c] + part[(3 * PMAX + p) * NB + c];
-        acc[p * NB + c] = J.rhs[(size_t)p * J.rhs_stride + (size_t)k * NB + c] - t;
-      }
-    const double2 *src = reinterpret_cast<const double2 *>(J.dinv + (size_t)k * TSZ);
-    for (int i = tid; i < TSZ / 2; i += 256) reinterpret_cast<double2 *>(T)[i] = src[i];
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
-    for (int cc = q * 16; cc < q * 16 + 16; cc++) {
-      const double dv = T[cc * LDT + c];
-#pragma unroll
-      for (int p = 0; p < PMAX; p++)
-        if (p < P) s[p] += dv * acc[p * NB + cc];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < PMAX; p++)
-      if (p < P) part[(q * PMAX + p) * NB + c] = s[p];
-    __syncthreads();
-    if (q == 0)
-      for (int p = 0; p < P; p++)
-        J.rhs[(size_t)p * J.rhs_stride + (size_t)k * NB + c] =
-            part[(0 * PMAX + p) * NB + c] + part[(1 * PMAX + p) * NB + c] +
-            part[(2 * PMAX + p) * NB + c] + part[(3 * PMAX + p) * NB + c];
-    __syncthreads();
-  }
-}
-
-// Backward: x_k = D_k (y_k - sum_j T(k+j,j) x_{k+j}).
-// Thread t owns row r = t % 64 and column quarter q = t / 64.
-template <int PMAX>
-__global__ void __launch_bounds__(256) k_band_bwd(const Job *__restrict__ jobs) {
-  const Job J = jobs[blockIdx.x];
-  const int P = J.P, nblk = J.nblk, Jt = J.J;
-  extern __shared__ __align__(16) double smb[];
-  double *T = smb;
-  double *part = T + TSZ;
-  double *acc = part + 4 * PMAX * NB;
-  const int tid = threadIdx.x, r = tid & (NB - 1), q = tid >> 6;
-  for (int k = nblk - 1; k >= 0; k--) {
-    double s[PMAX];
-#pragma unroll
-    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
-    const int jmax = min(Jt, nblk - 1 - k);
-    for (int j = jmax; j >= 1; j--) {
-      __syncthreads();
-      const double2 *src =
-          reinterpret_cast<const double2 *>(J.tiles + ((size_t)(k + j) * (Jt + 1) + j) * TSZ);
-      for (int i = tid; i < TSZ / 2; i += 256) reinterpret_cast<double2 *>(T)[i] = src[i];
-      __syncthreads();
-      const size_t co = (size_t)(k + j) * NB;
-#pragma unroll 4
-      for (int cc = q * 16; cc < q * 16 + 16; cc++) {
-        const double tv = T[r * LDT + cc];
-#pragma unroll
-        for (int p = 0; p < PMAX; p++)
-          if (p < P) s[p] += tv * J.rhs[(size_t)p * J.rhs_stride + co + cc];
-      }
-    }
-#pragma unroll
-    for (int p = 0; p < PMAX; p++)
-      if (p < P) part[(q * PMAX + p) * NB + r] = s[p];
-    __syncthreads();
-    if (q == 0)
-      for (int p = 0; p < P; p++) {
-        const double t = part[(0 * PMAX + p) * NB + r] + part[(1 * PMAX + p) * NB + r] +
-                         part[(2 * PMAX + p) * NB + r] + part[(3 * PMAX + p) * NB + r];
-        acc[p * NB + r] = J.rhs[(size_t)p * J.rhs_stride + (size_t)k * NB + r] - t;
-      }
-    const double2 *src = reinterpret_cast<const double2 *>(J.dinv + (size_t)k * TSZ);
-    for (int i = tid; i < TSZ / 2; i += 256) reinterpret_cast<double2 *>(T)[i] = src[i];
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
-    for (int cc = q * 16; cc < q * 16 + 16; cc++) {
-      const double dv = T[r * LDT + cc];
-#pragma unroll
-      for (int p = 0; p < PMAX; p++)
-        if (p < P) s[p] += dv * acc[p * NB + cc];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < PMAX; p++)
-      if (p < P) part[(q * PMAX + p) * NB + r] = s[p];
-    __syncthreads();
-    if (q == 0)
-      for (int p = 0; p < P; p++)
-        J.rhs[(size_t)p * J.rhs_stride + (size_t)k * NB + r] =
-            part[(0 * PMAX + p) * NB + r] + part[(1 * PMAX + p) * NB + r] +
-            part[(2 * PMAX + p) * NB + r] + part[(3 * PMAX + p) * NB + r];
-    __syncthreads();
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Interior back-substitution + essential values
 // ---------------------------------------------------------------------------
 
@@ -342,23 +207,6 @@ static int prepare_np() {
   return SX_OK;
 }
 
-int prepare_direct_kernels(const MeshView &M) {
-  switch (M.np) {
-#define SX_CASE(n) \
-  case n: SX_TRY(prepare_np<n>()); break;
-    SX_CASE(3) SX_CASE(4) SX_CASE(5) SX_CASE(6) SX_CASE(7) SX_CASE(8) SX_CASE(9) SX_CASE(10)
-    SX_CASE(11) SX_CASE(12)
-#undef SX_CASE
-    default: return SX_ERR_UNSUPPORTED;
-  }
-  const size_t s2 = band_smem(2), s8 = band_smem(8);
-  SX_CUDA(cudaFuncSetAttribute(k_band_fwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
-  SX_CUDA(cudaFuncSetAttribute(k_band_bwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
-  SX_CUDA(cudaFuncSetAttribute(k_band_fwd<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
-  SX_CUDA(cudaFuncSetAttribute(k_band_bwd<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s8));
-  return SX_OK;
-}
-
 static void dispatch_elem(const MeshView &M, const Job *djobs, int njobs, bool rhs, cudaStream_t st) {
   switch (M.np) {
 #define SX_CASE(n) \
@@ -370,15 +218,24 @@ static void dispatch_elem(const MeshView &M, const Job *djobs, int njobs, bool r
   }
 }
 
-size_t band_smem(int pmax) { return sizeof(double) * (TSZ + 5 * pmax * NB); }
+int prepare_direct_kernels(const MeshView &M) {
+  switch (M.np) {
+#define SX_CASE(n) \
+  case n: SX_TRY(prepare_np<n>()); break;
+    SX_CASE(3) SX_CASE(4) SX_CASE(5) SX_CASE(6) SX_CASE(7) SX_CASE(8) SX_CASE(9) SX_CASE(10)
+    SX_CASE(11) SX_CASE(12)
+#undef SX_CASE
+    default: return SX_ERR_UNSUPPORTED;
+  }
+  return prepare_band_kernels();
+}
 
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st) {
+                      cudaStream_t st, int C, int *launches) {
   const int nj = (int)hjobs.size();
-  int maxP = 0, maxpad = 0;
+  int maxpad = 0;
   bool any_bc = false;
   for (const Job &j : hjobs) {
-    maxP = std::max(maxP, j.P);
     maxpad = std::max(maxpad, j.npad);
     any_bc |= j.bc != nullptr;
     SX_CUDA(cudaMemsetAsync(j.gess, 0, sizeof(double) * (size_t)j.P * M.nglobal, st));
@@ -386,21 +243,10 @@ int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job
   if (any_bc) k_essential<<<dim3(1, nj), 32, 0, st>>>(M, djobs);
   dispatch_elem(M, djobs, nj, true, st);
   k_rhs_dss<<<dim3((maxpad + 255) / 256, nj), 256, 0, st>>>(M, djobs);
-  if (maxP > 8) {
-    set_error("at most 8 planes per job");
-    return SX_ERR_UNSUPPORTED;
-  }
-  if (maxP <= 2) {
-    const size_t sm = band_smem(2);
-    k_band_fwd<2><<<nj, 256, sm, st>>>(djobs);
-    k_band_bwd<2><<<nj, 256, sm, st>>>(djobs);
-  } else {
-    const size_t sm = band_smem(8);
-    k_band_fwd<8><<<nj, 256, sm, st>>>(djobs);
-    k_band_bwd<8><<<nj, 256, sm, st>>>(djobs);
-  }
+  SX_TRY(band_sweep_jobs(djobs, hjobs, C, st));
   dispatch_elem(M, djobs, nj, false, st);
   SX_CUDA(cudaGetLastError());
+  if (launches) *launches = (any_bc ? 1 : 0) + 4;
   return SX_OK;
 }
 

@@ -26,6 +26,7 @@ struct Job {
   double *gess;         // P * nglobal
   // JACPCG
   const double *pc;
+  int *status;          // device status bits (1 << SX_ERR_*)
 };
 
 // out = A_e u for one element (Element::HelmholtzOp + HelmholtzKern,
@@ -67,9 +68,14 @@ __device__ __forceinline__ void helm_op(const T *D, const T *Q1, const T *Q2, co
   __syncthreads();
 }
 
+// Direct solve of all jobs; the band sweeps run one cluster of C CTAs per job.
+// Returns the number of kernels launched through *launches when non-null.
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st);
-size_t band_smem(int pmax);
+                      cudaStream_t st, int C, int *launches = nullptr);
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st);
+int prepare_band_kernels();
+int pick_cluster(int nj, int cmax, int pmax, int Wmax);
+size_t sweep_smem(int pmax, int C, int S, int Wmax);
 // Set kernel attributes (max dynamic smem) ahead of any stream capture.
 int prepare_direct_kernels(const MeshView &M);
 

@@ -1,0 +1,137 @@
+"""Seeded synthetic Helmholtz workloads.
+
+The reference publishes no benchmark data set.  These builders are
+seeded stand-ins with the shapes of the five benchmark configurations (mesh,
+order, planes, per-mode Helmholtz constants, forcing law); each returns a
+``Workload`` with the mesh, the per-mode (lambda2, betak2) and the forcing
+planes in semtex's Fourier plane order (plane 0 mode 0, plane 1 Nyquist,
+planes 2k / 2k+1 Re / Im of mode k).
+
+Equation convention: semtex solves  div grad u - lambda^2 u = f
+(src/field.h:15-21), so manufactured forcings carry that sign.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mesh import QuadMesh, edge_maps, rect_mesh
+
+
+@dataclass
+class Workload:
+    name: str
+    mesh: QuadMesh
+    nz: int
+    beta: float
+    lambda2: np.ndarray          # per local mode
+    betak2: np.ndarray           # per local mode
+    forcing: np.ndarray          # (nz, nplane)
+    exact: np.ndarray | None = None
+    seed: int = 0
+    info: dict = field(default_factory=dict)
+
+    @property
+    def num_modes(self):
+        return len(self.lambda2)
+
+    @property
+    def planes_solved(self):
+        """Planes the solve touches: plane 1 (Nyquist) is skipped."""
+        return 1 if self.nz == 1 else self.nz - 1
+
+    @property
+    def dof_per_plane(self):
+        return self.mesh.n_unique
+
+    @property
+    def dof_solves(self):
+        return self.dof_per_plane * self.planes_solved
+
+
+def scatter_global(m: QuadMesh, gvals: np.ndarray) -> np.ndarray:
+    """Continuous field from values per unique node: gvals has
+    nglobal + nel*nint entries (element-boundary globals first, then each
+    element's interior nodes in edge-map order); returns the element plane."""
+    emap, _ = edge_maps(m.np)
+    out = np.zeros((m.nel, m.npnp))
+    bvals = gvals[: m.nglobal][m.btog]                        # (nel, next)
+    ivals = gvals[m.nglobal:].reshape(m.nel, m.nint)          # (nel, nint)
+    out[:, emap[: m.next]] = bvals
+    out[:, emap[m.next:]] = ivals
+    return out.reshape(-1)
+
+
+def _jittered_channel(nx, ny, np_, jitter, seed, lx=2 * np.pi):
+    return rect_mesh(nx, ny, np_, 0.0, lx, 0.0, 1.0, jitter=jitter, seed=seed, periodic_x=True,
+                     bc={"bottom": "D", "top": "D"})
+
+
+def config1():
+    """Unit square, 4x4 straight quads, N=8, lambda2=1, u = sin(pi x) sin(pi y)."""
+    m = rect_mesh(4, 4, 9)
+    f = -(2 * np.pi ** 2 + 1.0) * m.eval_nodes(lambda x, y: np.sin(np.pi * x) * np.sin(np.pi * y))
+    exact = m.eval_nodes(lambda x, y: np.sin(np.pi * x) * np.sin(np.pi * y))
+    return Workload("cfg1_unit_square_4x4_N8", m, 1, 0.0, np.array([1.0]), np.array([0.0]),
+                    f[None], exact[None], seed=1)
+
+
+def fourier_forcing(m: QuadMesh, nz: int, rng, decay=8.0):
+    """Gaussian random Fourier coefficients N(0,1) e^{-k/decay} per unique
+    node, Re and Im planes independent, scattered continuously."""
+    n = m.n_unique
+    f = np.zeros((nz, m.nplane))
+    for plane in range(nz):
+        if plane == 1 and nz > 1:
+            continue
+        k = plane >> 1
+        f[plane] = scatter_global(m, rng.standard_normal(n) * np.exp(-k / decay))
+    return f
+
+
+def config2(nx=32, ny=32, np_=9, nz=64, seed=2):
+    """[0,2pi]x[0,1], 32x32 quads jittered +-15%, N=8, nz=64 (modes 0..31),
+    beta=1, lambda2 = 1/(nu dt) = 1e6 with nu = dt = 1e-3, betak2 = k^2."""
+    m = _jittered_channel(nx, ny, np_, 0.15, seed)
+    rng = np.random.default_rng(seed)
+    nm = max(nz // 2, 1)
+    lam = np.full(nm, 1.0 / (1e-3 * 1e-3))
+    bk2 = np.arange(nm, dtype=np.float64) ** 2
+    f = fourier_forcing(m, nz, rng)
+    return Workload(f"cfg2_channel_{nx}x{ny}_N{np_ - 1}_nz{nz}", m, nz, 1.0, lam, bk2, f, seed=seed,
+                    info={"jitter": 0.15, "nu": 1e-3, "dt": 1e-3})
+
+
+def config3(nx=64, ny=64, np_=11, nz=128, seed=3):
+    """64x64 quads jittered +-20%, N=10, nz=128 (65 modes incl. Nyquist),
+    lambda2_k log-uniform in [1e-2, 1e4] (total Helmholtz constant per mode),
+    manufactured u = sum_k a_k sin(pi y) cos(k z) cos(3x), a_k ~ N(0,1) k^-2
+    (a_0 uses k=1 scaling).  Only cos(kz): Im planes zero."""
+    m = _jittered_channel(nx, ny, np_, 0.20, seed)
+    rng = np.random.default_rng(seed)
+    nm = nz // 2
+    lam = np.exp(rng.uniform(np.log(1e-2), np.log(1e4), size=nm))
+    bk2 = np.zeros(nm)
+    a = rng.standard_normal(nm) * np.maximum(np.arange(nm), 1.0) ** -2.0
+    shape = m.eval_nodes(lambda x, y: np.sin(np.pi * y) * np.cos(3 * x))
+    f = np.zeros((nz, m.nplane))
+    exact = np.zeros((nz, m.nplane))
+    for k in range(nm):
+        # semtex sign: div grad u - lam u = f, with -(pi^2 + 9) from the x,y parts
+        plane = 2 * k
+        exact[plane] = a[k] * shape
+        f[plane] = -(np.pi ** 2 + 9.0 + lam[k]) * a[k] * shape
+    return Workload(f"cfg3_channel_{nx}x{ny}_N{np_ - 1}_nz{nz}", m, nz, 1.0, lam, bk2, f, exact,
+                    seed=seed, info={"jitter": 0.20})
+
+
+def small_channel(nx=8, ny=6, np_=9, nz=16, lam=1e6, seed=7, jitter=0.15):
+    """Small config-2-shaped case for parity tests."""
+    m = _jittered_channel(nx, ny, np_, jitter, seed)
+    rng = np.random.default_rng(seed)
+    nm = max(nz // 2, 1)
+    lamv = np.full(nm, float(lam))
+    bk2 = np.arange(nm, dtype=np.float64) ** 2
+    return Workload(f"channel_{nx}x{ny}_N{np_ - 1}_nz{nz}", m, nz, 1.0, lamv, bk2,
+                    fourier_forcing(m, nz, rng), seed=seed)
