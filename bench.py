@@ -258,10 +258,36 @@ def run_ours(args, rank, world):
     u_batched = u_dev.cpu().numpy().copy()
     clk.start()
     ms_batched = timed(step_batched, args.steps, args.warmup)
-    clocks = clk.stop()
 
     st_b = S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride, sx.FP64, stream=sptr)
-    launches_per_step = int(st_b["kernel_launches"])
+    launches_fp64 = int(st_b["kernel_launches"])
+
+    # batched mixed precision: FP32 PCG inner iterations, FP64 refinement
+    mixed_stats = {}
+
+    def step_mixed():
+        f_work.copy_(f_src)
+        mixed_stats.update(S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride,
+                                           sx.MIXED_FP32, tol_rel=args.tol, max_refine=20,
+                                           stream=sptr))
+
+    step_mixed()
+    torch.cuda.synchronize()
+    u_mixed = u_dev.cpu().numpy().copy()
+    sp = [0] + list(range(2, nz)) if base == 0 else list(range(nz))
+    mixed_err = rel_err(u_mixed[sp], u_batched[sp])
+    ms_mixed = timed(step_mixed, args.steps, args.warmup)
+    clocks = clk.stop()
+    mixed_ok = max(mixed_err) <= 1e-10
+    if dist is not None:
+        t = torch.tensor([0.0 if mixed_ok else 1.0], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mixed_ok = t.item() == 0.0
+    # headline: the fastest batched form that meets the 1e-10 bar
+    use_mixed = mixed_ok and ms_mixed < ms_batched
+    head_prec = sx.MIXED_FP32 if use_mixed else sx.FP64
+    ms_head = ms_mixed if use_mixed else ms_batched
+    launches_per_step = int(mixed_stats.get("kernel_launches", 0)) if use_mixed else launches_fp64
 
     # dominant kernel: the banded sweeps, timed on their own stream
     reps = max(3, args.steps)
@@ -292,12 +318,12 @@ def run_ours(args, rank, world):
     u_host = torch.empty_like(f_host).pin_memory()
     fh, uh = f_host.numpy(), u_host.numpy()
     for _ in range(args.warmup):
-        S.solve_batched_host(fh, out=uh, precision=sx.FP64)
+        S.solve_batched_host(fh, out=uh, precision=head_prec, tol_rel=args.tol, max_refine=20)
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.solve_batched_host(fh, out=uh, precision=sx.FP64)
+        S.solve_batched_host(fh, out=uh, precision=head_prec, tol_rel=args.tol, max_refine=20)
     e2e_s = (time.perf_counter() - t0) / args.steps
     if dist is not None:
         t = torch.tensor([e2e_s], device=dev)
@@ -305,22 +331,29 @@ def run_ours(args, rank, world):
         e2e_s = float(t.item())
 
     total_dofs = dofs * world
-    value = total_dofs / (ms_batched * 1e-3)
+    value = total_dofs / (ms_head * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_batched, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if use_mixed else "f64",
         "data": "synthetic (seeded Gaussian Fourier forcing)",
         "config": {"workload": w.name, "elements": m.nel, "order": m.np - 1, "nz": nz,
                    "modes_per_gpu": nmodes, "planes_solved_per_gpu": planes_solved,
                    "dof_per_plane": w.dof_per_plane, "nglobal": m.nglobal, "nsolve": m.nsolve,
-                   "nband": m.nband, "lambda2": float(w.lambda2[0]), "form": "batched FP64",
+                   "nband": m.nband, "lambda2": float(w.lambda2[0]),
+                   "form": "batched mixed (FP32 PCG + FP64 refinement)" if use_mixed else "batched FP64",
                    "parallelism": f"modes split over {world} GPU(s), no collective",
                    "l2": "working set (factors %.1f GB) >> L2" % (S.device_bytes / 1e9)},
         "plain_fp64": {"value": total_dofs / (ms_plain * 1e-3), "ms_per_step": ms_plain},
-        "batched_fp64": {"value": value, "ms_per_step": ms_batched,
+        "batched_fp64": {"value": total_dofs / (ms_batched * 1e-3), "ms_per_step": ms_batched,
                          "rel_err_vs_plain": rel_err(u_batched[[0] + list(range(2, nz))],
                                                      u_plain[[0] + list(range(2, nz))])},
+        "batched_mixed": {"value": total_dofs / (ms_mixed * 1e-3), "ms_per_step": ms_mixed,
+                          "rel_err_vs_fp64": mixed_err, "meets_1e-10": mixed_ok,
+                          "refinements": mixed_stats.get("refinements"),
+                          "inner_iterations": mixed_stats.get("iterations_max"),
+                          "final_rel_residual": mixed_stats.get("final_rel_residual")},
+        "speedup_mixed_vs_plain": ms_plain / ms_mixed,
         "setup_s": setup_s,
         "roofline": roofline,
         "e2e": {"value": total_dofs / e2e_s, "unit": UNIT,
@@ -342,6 +375,45 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """Bounded runs of one kernel family for ncu captures (not a bench line).
+
+    band : band sweeps of a config-2-shaped channel with 32 x 16 quads and
+           nz = 16 (8 systems, ~0.5 GB of factors, larger than L2)
+    mixed: the mixed-precision batched form on the full config-2 workload
+           with Jacobi systems only (no band factors, ~0.3 GB resident)
+    """
+    import torch
+    import semtex_b200 as sx
+    from semtex_b200.workloads import config2
+    torch.cuda.set_device(0)
+    if args.profile == "band":
+        w = config2(ny=16, nz=16)
+        method = sx.DIRECT
+    else:
+        w = config2()
+        method = sx.JACPCG
+    m = w.mesh
+    S = sx.ModalMatrixSys(sx.Mesh(m), num_modes=w.num_modes, method=method,
+                          lambda2_modes=w.lambda2, betak2_modes=w.betak2)
+    f_src = torch.tensor(w.forcing, device="cuda")
+    f = torch.empty_like(f_src)
+    u = torch.zeros_like(f_src)
+    sptr = torch.cuda.current_stream().cuda_stream
+    for _ in range(max(1, args.steps)):
+        f.copy_(f_src)
+        if args.profile == "band":
+            S.solve_batched(u.data_ptr(), f.data_ptr(), 0, w.nz, m.nplane, sx.FP64, stream=sptr)
+        else:
+            S.solve_batched(u.data_ptr(), f.data_ptr(), 0, w.nz, m.nplane, sx.MIXED_FP32,
+                            tol_rel=args.tol, max_refine=20, stream=sptr)
+    if args.profile == "band":
+        S.profile_band_sweeps(max(1, args.steps), sptr)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.profile, "workload": w.name, "nband": m.nband,
+                      "nsolve": m.nsolve, "modes": w.num_modes}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -349,9 +421,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--tol", type=float, default=1e-12,
+                    help="FP64 relative residual at which the mixed form stops")
+    ap.add_argument("--profile", choices=["band", "mixed"], default=None,
+                    help="bounded run of one kernel family for ncu (no bench line)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -171,6 +171,13 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
                                 int nz, int plane_stride, int precision, double tol_rel,
                                 int max_refine, sx_solve_stats *stats);
 
+/* Schedule knobs of the batched forms (no reference counterpart), set by
+ * the autotuner or by hand; value <= 0 restores the default.
+ *   SX_TUNE_INNER_ITERS   FP32 PCG iterations per refinement round (12)
+ *   SX_TUNE_BAND_CLUSTER  CTAs per cluster in the band sweeps (auto)     */
+enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2 };
+SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
+
 /* Profiling hook (no reference counterpart): re-launch only the banded
  * forward/backward sweeps of the last batched solve `reps` times on
  * `stream`, so the dominant kernel can be timed on its own.  The RHS

@@ -29,6 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libsemtex_b200.so")
 DIRECT, JACPCG, MIXED_SOLVER = 0, 1, 2
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
+TUNE_INNER_ITERS, TUNE_BAND_CLUSTER = 1, 2
 
 
 class SolverError(RuntimeError):
@@ -85,6 +86,7 @@ def _load():
                                               P(SolveStats)]
     L.sx_profile_band_sweeps.argtypes = [vp, ip, vp]
     L.sx_modal_status.argtypes = [vp]
+    L.sx_modal_tune.argtypes = [vp, ip, ip]
     return L
 
 
@@ -240,6 +242,14 @@ class ModalMatrixSys:
         _check(rc, "sx_field_solve_batched_host", allow=(OK, WARN_STEP_LIMIT))
         self.last_stats = st.as_dict()
         return u
+
+    def tune(self, inner_iters=None, band_cluster=None):
+        """Schedule knobs of the batched forms (None leaves a knob alone, 0
+        restores its default)."""
+        if inner_iters is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_INNER_ITERS, int(inner_iters)), "sx_modal_tune")
+        if band_cluster is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_BAND_CLUSTER, int(band_cluster)), "sx_modal_tune")
 
     def profile_band_sweeps(self, reps, stream=0):
         _check(lib.sx_profile_band_sweeps(self.h, reps, stream), "sx_profile_band_sweeps")

@@ -4,6 +4,7 @@
 
 #include "sx_internal.h"
 #include "sx_kernels.cuh"
+#include "sx_mixed.cuh"
 #include "sx_pcg.cuh"
 #include "sx_solve.cuh"
 
@@ -35,8 +36,15 @@ struct sx_modal_s {
   std::vector<Job> gjobs;            // host copy of the captured jobs
   int gC = 1, glaunches = 0;         // their band-sweep cluster size, kernel count
   DBuf<int> dstatus;                 // device status bits of the last solves
+  // mixed-precision batched form
+  MixedWork mixed;
+  const void *mkey[3] = {nullptr, nullptr, nullptr};
+  int mnz = 0, mstride = 0;
+  int n_inner = 12;                  // FP32 PCG iterations per refinement round
   std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
+  int forced_cluster = 0;
   int cluster(int nj) {
+    if (forced_cluster > 0) return forced_cluster;
     auto it = cluster_for.find(nj);
     if (it != cluster_for.end()) return it->second;
     int J = 1;
@@ -183,6 +191,26 @@ static int take_status(sx_modal s, bool clear) {
     return SX_ERR_TIMEOUT;
   }
   return SX_OK;
+}
+
+extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
+  if (!s) return SX_ERR_ARG;
+  switch (knob) {
+    case SX_TUNE_INNER_ITERS:
+      if (value > 1000) return SX_ERR_ARG;
+      s->n_inner = value > 0 ? value : 12;
+      return SX_OK;
+    case SX_TUNE_BAND_CLUSTER:
+      if (value > 16) return SX_ERR_ARG;
+      s->forced_cluster = value > 0 ? value : 0;
+      if (s->gexec) {  // the captured batched graph bakes in the cluster size
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+      }
+      return SX_OK;
+    default:
+      return SX_ERR_ARG;
+  }
 }
 
 extern "C" int sx_modal_status(sx_modal s) {
@@ -334,13 +362,52 @@ extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc
   return rc;
 }
 
+// Mixed-precision batched form: every solved plane of every mode in one
+// FP32-PCG / FP64-refinement iteration (sx_mixed.cu).
 static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
                                int plane_stride, double tol_rel, int max_refine, void *stream,
                                sx_solve_stats *stats) {
-  (void)s; (void)d_u; (void)d_f; (void)d_bc; (void)nz; (void)plane_stride; (void)tol_rel;
-  (void)max_refine; (void)stream; (void)stats;
-  set_error("mixed-precision batched form not built yet");
-  return SX_ERR_UNSUPPORTED;
+  std::vector<Group> groups;
+  SX_TRY(plane_groups(*s, nz, groups));
+  int planes = 0;
+  for (auto &g : groups) planes += g.P;
+  SX_TRY(reserve_ws(*s, planes));
+  for (auto &u : s->uniq)
+    if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, 0));
+  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
+  const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
+  std::vector<MxPlane> mp;
+  int slot = 0;
+  for (auto &g : groups) {
+    const System &S = *s->sys[g.mode];
+    for (int p = 0; p < g.P; p++) {
+      const int plane = g.plane0 + p;
+      MxPlane x;
+      x.u = d_u + (long long)plane * plane_stride;
+      x.f = d_f + (long long)plane * plane_stride;
+      x.bc = d_bc ? d_bc + (long long)plane * bcstride : nullptr;
+      x.gess = s->gess.p + (size_t)slot * s->mesh->nglobal;
+      x.pc = S.pc.p;
+      x.pcf = S.pcf.p;
+      x.hCon = S.betak2 + S.lambda2;
+      x.nsolve = S.nsolve;
+      mp.push_back(x);
+      slot++;
+    }
+  }
+  const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
+                         s->mstride == plane_stride && s->mixed.n_inner == s->n_inner);
+  const MeshView M = s->mesh->view();
+  const int rc = mixed_solve(M, s->mixed, mp, rebuild, tol_rel, max_refine, s->n_inner, st, stats);
+  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  s->mkey[0] = d_u;
+  s->mkey[1] = d_f;
+  s->mkey[2] = d_bc;
+  s->mnz = nz;
+  s->mstride = plane_stride;
+  if (!stream) SX_TRY(take_status(s, true));
+  return rc;
 }
 
 // Batched form: every mode's planes in each launch (one job per mode), the

@@ -468,10 +468,17 @@ int system_build_direct(System &S, cudaStream_t st) {
 
 int system_build_jacobi(System &S, cudaStream_t st) {
   sx_mesh_s &Mh = *S.mesh;
-  const MeshView M = Mh.view();
-  const double hCon = S.betak2 + S.lambda2;
   S.singular = (S.lambda2 + S.betak2) < EPSSP && (Mh.nglobal - Mh.nsolve) == 0 && !Mh.mixed;
   S.nsolve = S.singular ? Mh.nsolve - 1 : Mh.nsolve;
+  return system_build_jacobi_diag(S, st);
+}
+
+// Inverse Jacobi diagonal only (also used by DIRECT systems for the
+// mixed-precision form).
+int system_build_jacobi_diag(System &S, cudaStream_t st) {
+  sx_mesh_s &Mh = *S.mesh;
+  const MeshView M = Mh.view();
+  const double hCon = S.betak2 + S.lambda2;
   const int npts = Mh.nglobal + Mh.nel * Mh.nint;
   DBuf<double> ediag;
   SX_TRY(ediag.alloc((size_t)Mh.nel * Mh.npnp));

@@ -98,6 +98,7 @@ struct MeshView {
   const int *emap;       // npnp
   const double *Q1, *Q2, *Q3, *Q4, *Q8;  // nel*npnp (Q3 zero when absent)
   const float *Q1f, *Q2f, *Q3f, *Q4f;    // FP32 copies (mixed precision)
+  const float *Df;                       // FP32 copy of D
   const unsigned char *hasQ3;            // nel
   const int *btog, *bmask, *emask;       // nel*next, nel*next, nel
   const int *g2e_ptr, *g2e_idx;          // CSR: global node -> (e*next+i), element order
@@ -129,7 +130,7 @@ struct sx_mesh_s {
   std::vector<int> colour_ptr, colour_elmt;  // element colouring (no shared nodes)
   // device
   sx::DBuf<double> dD, dQ1, dQ2, dQ3, dQ4, dQ8, dK, dC, darea;
-  sx::DBuf<float> dQ1f, dQ2f, dQ3f, dQ4f;
+  sx::DBuf<float> dQ1f, dQ2f, dQ3f, dQ4f, dDf;
   sx::DBuf<unsigned char> dhasQ3;
   sx::DBuf<int> demap, dbtog, dbmask, demask, dg2e_ptr, dg2e_idx, dg2e_last, dbe, dbs, dbk;
   sx::DBuf<int> dnat_ptr, dnat_idx, dcolour_elmt;
@@ -159,6 +160,7 @@ struct System {
 
 int system_build_direct(System &S, cudaStream_t st);
 int system_build_jacobi(System &S, cudaStream_t st);
+int system_build_jacobi_diag(System &S, cudaStream_t st);
 int system_band_export(const System &S, double *ab);  // LAPACK band, host
 
 // Solve workspace for up to `planes` planes of one system.

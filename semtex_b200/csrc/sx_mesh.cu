@@ -191,7 +191,7 @@ sx::MeshView sx_mesh_s::view() const {
   v.nglobal = nglobal; v.nsolve_ns = nsolve; v.nband = nband;
   v.D = dD.p; v.emap = demap.p;
   v.Q1 = dQ1.p; v.Q2 = dQ2.p; v.Q3 = dQ3.p; v.Q4 = dQ4.p; v.Q8 = dQ8.p;
-  v.Q1f = dQ1f.p; v.Q2f = dQ2f.p; v.Q3f = dQ3f.p; v.Q4f = dQ4f.p;
+  v.Q1f = dQ1f.p; v.Q2f = dQ2f.p; v.Q3f = dQ3f.p; v.Q4f = dQ4f.p; v.Df = dDf.p;
   v.hasQ3 = dhasQ3.p;
   v.btog = dbtog.p; v.bmask = dbmask.p; v.emask = demask.p;
   v.g2e_ptr = dg2e_ptr.p; v.g2e_idx = dg2e_idx.p; v.g2e_last = dg2e_last.p;
@@ -353,6 +353,8 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   SX_TRY(M->dQ2f.upload(f2.data(), tot));
   SX_TRY(M->dQ3f.upload(f3.data(), tot));
   SX_TRY(M->dQ4f.upload(f4.data(), tot));
+  std::vector<float> df(M->D.begin(), M->D.end());
+  SX_TRY(M->dDf.upload(df.data(), df.size()));
   SX_TRY(M->dhasQ3.upload(M->hasQ3.data(), nel));
   SX_TRY(M->dbtog.upload(M->btog.data(), tb));
   SX_TRY(M->dbmask.upload(M->bmask.data(), tb));

@@ -1,0 +1,128 @@
+"""GPU tests of the batched forms.
+
+* batched FP64 (all modes per launch, captured graph) equals the plain
+  mode-by-mode form to rounding (rel <= 1e-13), for every band-sweep
+  cluster size;
+* the mixed-precision form (FP32 Jacobi-PCG inner iterations, FP64
+  refinement) matches the oracle's FP64 direct solve within 1e-10 relative
+  L2 and max norm, on the config-2 shape and on the reference goldens;
+* results are deterministic (bitwise equal on repeat).
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleMesh, solve_planes
+from tests.problems import PROBLEMS_2D, build_2d, golden_ok
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-10
+
+
+def rel_errs(a, b):
+    a = np.asarray(a).ravel()
+    b = np.asarray(b).ravel()
+    return (np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300),
+            np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def sx():
+    import semtex_b200
+    return semtex_b200
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def solved_planes(nz):
+    return [0] + list(range(2, nz)) if nz > 1 else [0]
+
+
+def _setup(sx, w, method=0):
+    mesh = sx.Mesh(w.mesh)
+    S = sx.ModalMatrixSys(mesh, num_modes=w.num_modes, method=method,
+                          lambda2_modes=w.lambda2, betak2_modes=w.betak2)
+    return mesh, S
+
+
+def _run_device(torch, S, w, batched=True, precision=0, tol=1e-12, bc=None):
+    f = torch.tensor(w.forcing, device="cuda")
+    u = torch.zeros_like(f)
+    b = None if bc is None else torch.tensor(bc, device="cuda")
+    bptr = 0 if b is None else b.data_ptr()
+    if batched:
+        st = S.solve_batched(u.data_ptr(), f.data_ptr(), bptr, w.nz, w.mesh.nplane, precision, tol,
+                             max_refine=40)
+    else:
+        st = S.solve_device(u.data_ptr(), f.data_ptr(), bptr, w.nz, w.mesh.nplane)
+    torch.cuda.synchronize()
+    S.status()
+    return u.cpu().numpy(), st
+
+
+@pytest.mark.parametrize("cluster", [0, 1, 2, 3, 5])
+def test_batched_fp64_equals_plain(sx, torch, cluster):
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=8, ny=8, np_=9, nz=12, lam=1e6, seed=11)
+    _, S = _setup(sx, w)
+    S.tune(band_cluster=cluster)
+    up, _ = _run_device(torch, S, w, batched=False)
+    ub, st = _run_device(torch, S, w, batched=True)
+    sp = solved_planes(w.nz)
+    l2, mx = rel_errs(ub[sp], up[sp])
+    assert l2 <= 1e-13 and mx <= 1e-13, (cluster, l2, mx)
+    assert st["planes_solved"] == w.nz - 1
+
+
+@pytest.mark.parametrize("lam,inner", [(1e6, 12), (1e3, 30)])
+def test_mixed_matches_oracle(sx, torch, lam, inner):
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=6, ny=5, np_=9, nz=6, lam=lam, seed=5)
+    _, S = _setup(sx, w)
+    S.tune(inner_iters=inner)
+    um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32, tol=1e-12)
+    assert st["final_rel_residual"] <= 1e-12
+    uo, _ = solve_planes(OracleMesh(w.mesh), 0.0, 1.0, w.forcing, None,
+                         lambda2_per_mode=w.lambda2)
+    sp = solved_planes(w.nz)
+    l2, mx = rel_errs(um[sp], uo[sp])
+    assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (lam, l2, mx, st)
+
+
+@pytest.mark.parametrize("name", ["helmholtz1", "laplace1", "laplace4"])
+def test_mixed_regress_goldens(sx, torch, name):
+    m, p, f, bc, exact = build_2d(name)
+    from semtex_b200.workloads import Workload
+    w = Workload(name, m, 1, 0.0, np.array([p["lambda2"]]), np.array([0.0]), f)
+    _, S = _setup(sx, w)
+    S.tune(inner_iters=200)
+    um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32, tol=1e-13, bc=bc)
+    uo, _ = solve_planes(OracleMesh(m), p["lambda2"], 0.0, f, bc)
+    l2, mx = rel_errs(um, uo)
+    assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (name, l2, mx, st)
+    err = np.abs(um[0] - exact).max()
+    if p["golden"] is not None:
+        assert golden_ok(err, p["golden"]), err
+
+
+def test_mixed_deterministic(sx, torch):
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=6, ny=6, np_=7, nz=8, lam=1e5, seed=9)
+    _, S = _setup(sx, w)
+    a, _ = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
+    b, _ = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
+    assert np.array_equal(a, b)
+
+
+def test_batched_host_entry(sx, torch):
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=5, ny=4, np_=6, nz=6, lam=10.0, seed=3)
+    _, S = _setup(sx, w)
+    ud, _ = _run_device(torch, S, w, batched=True)
+    uh = S.solve_batched_host(w.forcing)
+    sp = solved_planes(w.nz)
+    assert np.array_equal(uh[sp], ud[sp])
