@@ -184,6 +184,55 @@ SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
  * workspace is overwritten; call after sx_field_solve_batched. */
 SX_API int sx_profile_band_sweeps(sx_modal modal, int reps, void *stream);
 
+/* ---- serving loop (no reference counterpart) -----------------------------
+ * A request loop for Helmholtz solves of different meshes, orders and mode
+ * counts.  Requests are admitted in arrival order as device slots and memory
+ * free up (bounded by hbm_budget); admitted requests run concurrently, each
+ * on its own stream.  Element geometry and per-mode systems (Jacobi
+ * diagonals, or factored condensed matrices for SX_FP64) stay resident
+ * across requests, keyed by (mesh, lambda2, betak2), with least-recently-
+ * used eviction.  A request's result does not depend on what else is in
+ * flight. */
+typedef struct sx_server_s *sx_server;
+
+typedef struct {
+  unsigned long long hbm_budget; /* device bytes for caches + in-flight work; 0 = 80% of free */
+  int slots;                     /* requests on the device at once; 0 = 4                      */
+  int precision;                 /* SX_MIXED_FP32 (PCG) or SX_FP64 (DIRECT, cached factors)     */
+  double tol_rel;                /* mixed: FP64 relative residual target; 0 = 1e-12            */
+  int max_refine;                /* mixed: refinement rounds cap; 0 = 30                        */
+  int inner_iters;               /* mixed: FP32 PCG iterations per round; 0 = 12                */
+} sx_server_config;
+
+typedef struct {
+  const sx_mesh_desc *mesh;      /* copied at submit                                          */
+  int base_mode, num_modes;
+  const double *lambda2;         /* num_modes, copied                                         */
+  const double *betak2;          /* num_modes, copied                                         */
+  int nz, plane_stride;          /* planes in semtex order, as sx_field_solve                 */
+  const double *f;               /* nz*plane_stride forcing, copied at submit                 */
+  const double *bc;              /* nz*nbound*np or NULL, copied                              */
+  double *u;                     /* nz*plane_stride, written before the request completes     */
+} sx_request;
+
+typedef struct {
+  unsigned long long submitted, completed, failed, rejected;
+  unsigned long long mesh_hits, mesh_misses, system_hits, system_misses, evictions;
+  unsigned long long bytes_cached, bytes_budget;
+  double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency of completed requests     */
+} sx_server_stats;
+
+SX_API int sx_server_create(const sx_server_config *cfg, sx_server *out);
+/* Queue a request; returns at once with its id.  SX_ERR_CAPACITY when the
+ * request alone cannot fit in hbm_budget. */
+SX_API int sx_server_submit(sx_server s, const sx_request *req, unsigned long long *id);
+/* Wait for a request (timeout_s < 0: no limit); *status is its solve status. */
+SX_API int sx_server_wait(sx_server s, unsigned long long id, double timeout_s, int *status,
+                          double *latency_ms);
+SX_API int sx_server_get_stats(sx_server s, sx_server_stats *st);
+/* Finishes the queued requests, then releases everything. */
+SX_API int sx_server_destroy(sx_server s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,29 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_ulonglong), ("slots", C.c_int), ("precision", C.c_int),
+                ("tol_rel", C.c_double), ("max_refine", C.c_int), ("inner_iters", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("mesh", C.POINTER(MeshDesc)), ("base_mode", C.c_int), ("num_modes", C.c_int),
+                ("lambda2", C.POINTER(C.c_double)), ("betak2", C.POINTER(C.c_double)),
+                ("nz", C.c_int), ("plane_stride", C.c_int),
+                ("f", C.POINTER(C.c_double)), ("bc", C.POINTER(C.c_double)),
+                ("u", C.POINTER(C.c_double))]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_ulonglong) for n in
+                ("submitted", "completed", "failed", "rejected", "mesh_hits", "mesh_misses",
+                 "system_hits", "system_misses", "evictions", "bytes_cached", "bytes_budget")] + \
+               [("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `python -m semtex_b200.build` "
@@ -87,6 +110,11 @@ def _load():
     L.sx_profile_band_sweeps.argtypes = [vp, ip, vp]
     L.sx_modal_status.argtypes = [vp]
     L.sx_modal_tune.argtypes = [vp, ip, ip]
+    L.sx_server_create.argtypes = [P(ServerConfig), P(vp)]
+    L.sx_server_submit.argtypes = [vp, P(Request), P(C.c_ulonglong)]
+    L.sx_server_wait.argtypes = [vp, C.c_ulonglong, dp, P(ip), P(dp)]
+    L.sx_server_get_stats.argtypes = [vp, P(ServerStats)]
+    L.sx_server_destroy.argtypes = [vp]
     return L
 
 
@@ -119,23 +147,28 @@ def _check(st, what, allow=(OK,)):
     return st
 
 
+def mesh_desc(qm: QuadMesh):
+    """sx_mesh_desc for a QuadMesh; returns (desc, arrays to keep alive)."""
+    nb, be, bs, bk, bK, bC = qm.bc_arrays()
+    k = dict(
+        x=np.ascontiguousarray(qm.x, dtype=np.float64).reshape(-1),
+        y=np.ascontiguousarray(qm.y, dtype=np.float64).reshape(-1),
+        btog=np.ascontiguousarray(qm.btog, dtype=np.int32).reshape(-1),
+        bmask=np.ascontiguousarray(qm.bmask, dtype=np.int32).reshape(-1),
+        be=be.astype(np.int32), bs=bs.astype(np.int32), bk=bk.astype(np.int32),
+        bK=bK.astype(np.float64), bC=bC.astype(np.float64))
+    d = MeshDesc(qm.np, qm.nel, _dptr(k["x"]), _dptr(k["y"]), _iptr(k["btog"]),
+                 _iptr(k["bmask"]), qm.nglobal, qm.nsolve, qm.nband, nb,
+                 _iptr(k["be"]), _iptr(k["bs"]), _iptr(k["bk"]), _dptr(k["bK"]), _dptr(k["bC"]))
+    return d, k
+
+
 class Mesh:
     """A QuadMesh uploaded to the GPU (geometry factors + numbering)."""
 
     def __init__(self, qm: QuadMesh):
         self.qm = qm
-        nb, be, bs, bk, bK, bC = qm.bc_arrays()
-        self._keep = dict(
-            x=np.ascontiguousarray(qm.x, dtype=np.float64).reshape(-1),
-            y=np.ascontiguousarray(qm.y, dtype=np.float64).reshape(-1),
-            btog=np.ascontiguousarray(qm.btog, dtype=np.int32).reshape(-1),
-            bmask=np.ascontiguousarray(qm.bmask, dtype=np.int32).reshape(-1),
-            be=be.astype(np.int32), bs=bs.astype(np.int32), bk=bk.astype(np.int32),
-            bK=bK.astype(np.float64), bC=bC.astype(np.float64))
-        k = self._keep
-        d = MeshDesc(qm.np, qm.nel, _dptr(k["x"]), _dptr(k["y"]), _iptr(k["btog"]),
-                     _iptr(k["bmask"]), qm.nglobal, qm.nsolve, qm.nband, nb,
-                     _iptr(k["be"]), _iptr(k["bs"]), _iptr(k["bk"]), _dptr(k["bK"]), _dptr(k["bC"]))
+        d, self._keep = mesh_desc(qm)
         h = C.c_void_p()
         _check(lib.sx_mesh_create(C.byref(d), C.byref(h)), "sx_mesh_create")
         self.h = h
@@ -260,6 +293,59 @@ class ModalMatrixSys:
     def close(self):
         if getattr(self, "h", None) and lib is not None:
             lib.sx_modal_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Server:
+    """Continuous-batching request loop (sx_server_*): requests of any mesh,
+    order and mode count are admitted as device slots and memory free up,
+    run concurrently, and keep geometry and systems resident across requests.
+    """
+
+    def __init__(self, slots=4, precision=MIXED_FP32, hbm_budget=0, tol_rel=1e-12,
+                 max_refine=30, inner_iters=12):
+        cfg = ServerConfig(int(hbm_budget), slots, precision, tol_rel, max_refine, inner_iters)
+        h = C.c_void_p()
+        _check(lib.sx_server_create(C.byref(cfg), C.byref(h)), "sx_server_create")
+        self.h = h
+        self._live = {}
+
+    def submit(self, qm: QuadMesh, lambda2_modes, betak2_modes, forcing, bc=None, base_mode=0):
+        """Queue one solve; returns its id.  forcing: (nz, nplane)."""
+        d, keep = mesh_desc(qm)
+        lam = np.ascontiguousarray(lambda2_modes, dtype=np.float64)
+        bk2 = np.ascontiguousarray(betak2_modes, dtype=np.float64)
+        f = np.ascontiguousarray(forcing, dtype=np.float64).reshape(-1, qm.nplane)
+        nz = f.shape[0]
+        u = np.zeros_like(f)
+        b = None
+        if bc is not None:
+            nb = max(len(qm.boundaries), 1)
+            b = np.ascontiguousarray(np.broadcast_to(bc, (nz, nb, qm.np)), dtype=np.float64)
+        req = Request(C.pointer(d), base_mode, len(lam), _dptr(lam), _dptr(bk2), nz, qm.nplane,
+                      _dptr(f), _dptr(b) if b is not None else None, _dptr(u))
+        rid = C.c_ulonglong()
+        _check(lib.sx_server_submit(self.h, C.byref(req), C.byref(rid)), "sx_server_submit")
+        self._live[rid.value] = u          # the output buffer must outlive the request
+        return rid.value
+
+    def wait(self, rid, timeout_s=-1.0):
+        """(status, latency_ms, u) of a submitted request."""
+        st, lat = C.c_int(), C.c_double()
+        _check(lib.sx_server_wait(self.h, rid, timeout_s, C.byref(st), C.byref(lat)), "sx_server_wait")
+        return st.value, lat.value, self._live.pop(rid)
+
+    def stats(self):
+        s = ServerStats()
+        _check(lib.sx_server_get_stats(self.h, C.byref(s)), "sx_server_get_stats")
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.sx_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -2,11 +2,7 @@
 #include <cmath>
 #include <cstring>
 
-#include "sx_internal.h"
-#include "sx_kernels.cuh"
-#include "sx_mixed.cuh"
-#include "sx_pcg.cuh"
-#include "sx_solve.cuh"
+#include "sx_modal.h"
 
 namespace sx {
 const char *last_error();
@@ -14,53 +10,45 @@ const char *last_error();
 
 using namespace sx;
 
-struct sx_modal_s {
-  sx_mesh_s *mesh = nullptr;
-  int base_mode = 0, num_modes = 0, method = SX_DIRECT;
-  std::vector<std::shared_ptr<System>> sys;   // per local mode
-  std::vector<std::shared_ptr<System>> uniq;  // distinct systems
-  // solve workspace, sized for all planes at once
-  int ws_planes = 0;
-  DBuf<double> rhs, Fb, gess;
-  PcgWork pcg;
-  DBuf<Job> djobs;
-  // host-pointer entry: device staging
-  DBuf<double> hu, hf, hbc;
-  size_t npad_max = 0;
-  // batched form: captured graph and the arguments it was captured for
-  cudaStream_t own = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  const void *gkey[3] = {nullptr, nullptr, nullptr};
-  int gnz = 0, gstride = 0, gprec = -1;
-  DBuf<Job> bjobs;
-  std::vector<Job> gjobs;            // host copy of the captured jobs
-  int gC = 1, glaunches = 0;         // their band-sweep cluster size, kernel count
-  DBuf<int> dstatus;                 // device status bits of the last solves
-  // mixed-precision batched form
-  MixedWork mixed;
-  const void *mkey[3] = {nullptr, nullptr, nullptr};
-  int mnz = 0, mstride = 0;
-  int n_inner = 12;                  // FP32 PCG iterations per refinement round
-  std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
-  int forced_cluster = 0;
-  int cluster(int nj) {
-    if (forced_cluster > 0) return forced_cluster;
-    auto it = cluster_for.find(nj);
-    if (it != cluster_for.end()) return it->second;
-    int J = 1;
-    for (auto &s : uniq) J = std::max(J, s->J);
-    // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
-    const int c = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2);
-    cluster_for[nj] = c;
-    return c;
-  }
-  ~sx_modal_s() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (own) cudaStreamDestroy(own);
-  }
-};
+// ---------------------------------------------------------------------------
+// sx_modal_s
+// ---------------------------------------------------------------------------
 
-extern "C" const char *sx_version(void) { return "semtex_b200 0.1 (sm_100a)"; }
+int sx_modal_s::cluster(int nj) {
+  if (forced_cluster > 0) return forced_cluster;
+  auto it = cluster_for.find(nj);
+  if (it != cluster_for.end()) return it->second;
+  int J = 1;
+  for (auto &s : uniq) J = std::max(J, s->J);
+  // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
+  const int c = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2);
+  cluster_for[nj] = c;
+  return c;
+}
+
+void sx_modal_s::rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vector<std::shared_ptr<System>> s) {
+  mesh = m;
+  base_mode = base;
+  num_modes = nmodes;
+  method = meth;
+  sys = std::move(s);
+  uniq.clear();
+  for (auto &x : sys)
+    if (std::find(uniq.begin(), uniq.end(), x) == uniq.end()) uniq.push_back(x);
+  if (gexec) cudaGraphExecDestroy(gexec);
+  gexec = nullptr;
+  gkey[0] = gkey[1] = gkey[2] = nullptr;
+  mkey[0] = mkey[1] = mkey[2] = nullptr;
+  gjobs.clear();
+  cluster_for.clear();
+}
+
+sx_modal_s::~sx_modal_s() {
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (own && !own_stream_external) cudaStreamDestroy(own);
+}
+
+extern "C" const char *sx_version(void) { return "semtex_b200 0.2 (sm_100a)"; }
 
 extern "C" const char *sx_status_string(int s) {
   switch (s) {
@@ -94,6 +82,60 @@ static bool same_constants(const System &S, double lambda2, double betak2, int m
          S.method == method;
 }
 
+namespace sx {
+
+int modal_populate(sx_modal_s &M, const double *lam, const double *bk2, const SystemProvider *prov,
+                   cudaStream_t st) {
+  std::vector<System *> to_factor;
+  M.sys.clear();
+  M.uniq.clear();
+  for (int l = 0; l < M.num_modes; l++) {
+    const int mode = M.base_mode + l;
+    int kind = M.method;
+    if (M.method == SX_MIXED) kind = (mode == 0) ? SX_DIRECT : SX_JACPCG;  // src/matrix.cpp:93-96
+    std::shared_ptr<System> found;
+    for (auto &s : M.uniq)
+      if (same_constants(*s, lam[l], bk2[l], kind)) {
+        found = s;
+        break;
+      }
+    if (!found && prov) {
+      SX_TRY((*prov)(lam[l], bk2[l], kind, found));
+    } else if (!found) {
+      found = std::make_shared<System>();
+      found->mesh = M.mesh;
+      found->lambda2 = lam[l];
+      found->betak2 = bk2[l];
+      found->method = kind;
+      if (kind == SX_DIRECT) {
+        SX_TRY(system_build_direct(*found, st));
+        if (found->nsolve > 0) to_factor.push_back(found.get());
+      } else {
+        SX_TRY(system_build_jacobi(*found, st));
+      }
+    }
+    if (std::find(M.uniq.begin(), M.uniq.end(), found) == M.uniq.end()) M.uniq.push_back(found);
+    M.sys.push_back(found);
+  }
+  if (!M.dstatus.p) {
+    SX_TRY(M.dstatus.alloc(1));
+    SX_TRY(M.dstatus.zero(st));
+  }
+  SX_TRY(factor_batch(to_factor, st));
+  for (System *S : to_factor) {
+    int h = 0;
+    SX_CUDA(cudaMemcpyAsync(&h, S->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SX_CUDA(cudaStreamSynchronize(st));
+    if (h & (1 << SX_ERR_NOT_SPD)) {
+      set_error("failed to factor Helmholtz matrix (lambda2=%g, betak2=%g)", S->lambda2, S->betak2);
+      return SX_ERR_NOT_SPD;
+    }
+  }
+  return SX_OK;
+}
+
+}  // namespace sx
+
 static int modal_build(sx_mesh m, int base_mode, int num_modes, const double *lam, const double *bk2,
                        int method, sx_modal *out) {
   if (!m || !out || num_modes <= 0 || base_mode < 0 || method < SX_DIRECT || method > SX_MIXED)
@@ -104,45 +146,7 @@ static int modal_build(sx_mesh m, int base_mode, int num_modes, const double *la
   M->base_mode = base_mode;
   M->num_modes = num_modes;
   M->method = method;
-  cudaStream_t st = 0;
-  std::vector<System *> to_factor;
-  for (int l = 0; l < num_modes; l++) {
-    const int mode = base_mode + l;
-    int kind = method;
-    if (method == SX_MIXED) kind = (mode == 0) ? SX_DIRECT : SX_JACPCG;  // src/matrix.cpp:93-96
-    std::shared_ptr<System> found;
-    for (auto &s : M->uniq)
-      if (same_constants(*s, lam[l], bk2[l], kind)) {
-        found = s;
-        break;
-      }
-    if (!found) {
-      found = std::make_shared<System>();
-      found->mesh = m;
-      found->lambda2 = lam[l];
-      found->betak2 = bk2[l];
-      found->method = kind;
-      if (kind == SX_DIRECT) {
-        SX_TRY(system_build_direct(*found, st));
-        if (found->nsolve > 0) to_factor.push_back(found.get());
-      } else {
-        SX_TRY(system_build_jacobi(*found, st));
-      }
-      M->uniq.push_back(found);
-    }
-    M->sys.push_back(found);
-  }
-  SX_TRY(M->dstatus.alloc(1));
-  SX_TRY(M->dstatus.zero(st));
-  SX_TRY(factor_batch(to_factor, st));
-  for (System *S : to_factor) {
-    int h = 0;
-    SX_CUDA(cudaMemcpy(&h, S->status.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h & (1 << SX_ERR_NOT_SPD)) {
-      set_error("failed to factor Helmholtz matrix (lambda2=%g, betak2=%g)", S->lambda2, S->betak2);
-      return SX_ERR_NOT_SPD;
-    }
-  }
+  SX_TRY(modal_populate(*M, lam, bk2, nullptr, 0));
   *out = M.release();
   return SX_OK;
 }
@@ -180,12 +184,17 @@ extern "C" int sx_modal_band(sx_modal s, int m, double *ab, int *nsolve, int *si
 }
 
 // Device-side status of the solves enqueued so far (bounded waits that ran
-// out, ...).  Synchronises the device; clears the word when `clear`.
-static int take_status(sx_modal s, bool clear) {
+// out, ...).  Synchronises `st` (the whole device when st is null) and
+// clears the word when `clear`.
+static int take_status(sx_modal s, bool clear, cudaStream_t st = nullptr, bool device = true) {
   int h = 0;
-  SX_CUDA(cudaDeviceSynchronize());
-  SX_CUDA(cudaMemcpy(&h, s->dstatus.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (clear && h) SX_CUDA(cudaMemset(s->dstatus.p, 0, sizeof(int)));
+  if (device)
+    SX_CUDA(cudaDeviceSynchronize());
+  else
+    SX_CUDA(cudaStreamSynchronize(st));
+  SX_CUDA(cudaMemcpyAsync(&h, s->dstatus.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SX_CUDA(cudaStreamSynchronize(st));
+  if (clear && h) SX_CUDA(cudaMemsetAsync(s->dstatus.p, 0, sizeof(int), st));
   if (h & (1 << SX_ERR_TIMEOUT)) {
     set_error("a bounded device-side wait ran out (band sweep)");
     return SX_ERR_TIMEOUT;
@@ -251,16 +260,16 @@ static int plane_groups(const sx_modal_s &M, int nz, std::vector<Group> &g) {
   return SX_OK;
 }
 
+// Workspace for `planes` planes; reallocates only what is too small (the
+// serving loop reuses one workspace across meshes).
 static int reserve_ws(sx_modal_s &M, int planes) {
   const sx_mesh_s &Mh = *M.mesh;
   size_t npad = 1;
   for (auto &s : M.uniq) npad = std::max(npad, (size_t)std::max(s->nblk, 1) * NB);
-  if (planes <= M.ws_planes && npad <= M.npad_max) return SX_OK;
-  SX_TRY(M.rhs.alloc((size_t)planes * npad));
-  SX_TRY(M.Fb.alloc((size_t)planes * Mh.nel * Mh.next));
-  SX_TRY(M.gess.alloc((size_t)planes * Mh.nglobal));
-  M.ws_planes = planes;
   M.npad_max = npad;
+  if (M.rhs.n < (size_t)planes * npad) SX_TRY(M.rhs.alloc((size_t)planes * npad));
+  if (M.Fb.n < (size_t)planes * Mh.nel * Mh.next) SX_TRY(M.Fb.alloc((size_t)planes * Mh.nel * Mh.next));
+  if (M.gess.n < (size_t)planes * Mh.nglobal) SX_TRY(M.gess.alloc((size_t)planes * Mh.nglobal));
   return SX_OK;
 }
 
@@ -365,60 +374,36 @@ extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc
 // Mixed-precision batched form: every solved plane of every mode in one
 // FP32-PCG / FP64-refinement iteration (sx_mixed.cu).
 static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
-                               int plane_stride, double tol_rel, int max_refine, void *stream,
+                               int plane_stride, double tol_rel, int max_refine, cudaStream_t st,
                                sx_solve_stats *stats) {
   std::vector<Group> groups;
   SX_TRY(plane_groups(*s, nz, groups));
-  int planes = 0;
-  for (auto &g : groups) planes += g.P;
-  SX_TRY(reserve_ws(*s, planes));
   for (auto &u : s->uniq)
-    if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, 0));
-  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
-  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
-  const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
-  std::vector<MxPlane> mp;
-  int slot = 0;
-  for (auto &g : groups) {
-    const System &S = *s->sys[g.mode];
-    for (int p = 0; p < g.P; p++) {
-      const int plane = g.plane0 + p;
-      MxPlane x;
-      x.u = d_u + (long long)plane * plane_stride;
-      x.f = d_f + (long long)plane * plane_stride;
-      x.bc = d_bc ? d_bc + (long long)plane * bcstride : nullptr;
-      x.gess = s->gess.p + (size_t)slot * s->mesh->nglobal;
-      x.pc = S.pc.p;
-      x.pcf = S.pcf.p;
-      x.hCon = S.betak2 + S.lambda2;
-      x.nsolve = S.nsolve;
-      mp.push_back(x);
-      slot++;
-    }
-  }
+    if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, st));
+  std::vector<MxGroup> mg;
+  for (auto &g : groups) mg.push_back({g.mode, g.plane0, g.P, s->sys[g.mode].get()});
+  const int nyq = (nz > 1 && s->base_mode == 0) ? 1 : -1;
   const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
                          s->mstride == plane_stride && s->mixed.n_inner == s->n_inner);
   const MeshView M = s->mesh->view();
-  const int rc = mixed_solve(M, s->mixed, mp, rebuild, tol_rel, max_refine, s->n_inner, st, stats);
+  const int rc = mixed_solve(M, s->mixed, mg, nz, nyq, s->num_modes, d_u, d_f, d_bc, plane_stride, rebuild,
+                             tol_rel, max_refine, s->n_inner, s->use_graphs, st, stats);
   if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
   s->mkey[0] = d_u;
   s->mkey[1] = d_f;
   s->mkey[2] = d_bc;
   s->mnz = nz;
   s->mstride = plane_stride;
-  if (!stream) SX_TRY(take_status(s, true));
   return rc;
 }
 
-// Batched form: every mode's planes in each launch (one job per mode), the
-// whole sequence captured once into a CUDA graph and replayed.
-extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
-                                      int plane_stride, int precision, double tol_rel, int max_refine,
-                                      void *stream, sx_solve_stats *stats) {
-  if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
-  if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+namespace sx {
+
+// Batched forms on stream st (no device-wide synchronisation).
+int solve_batched_on(sx_modal_s *s, double *d_u, double *d_f, const double *d_bc, int nz, int plane_stride,
+                     int precision, double tol_rel, int max_refine, cudaStream_t st, sx_solve_stats *stats) {
   if (precision == SX_MIXED_FP32)
-    return mixed_solve_batched(s, d_u, d_f, d_bc, nz, plane_stride, tol_rel, max_refine, stream, stats);
+    return mixed_solve_batched(s, d_u, d_f, d_bc, nz, plane_stride, tol_rel, max_refine, st, stats);
   std::vector<Group> groups;
   SX_TRY(plane_groups(*s, nz, groups));
   for (auto &g : groups)
@@ -429,11 +414,10 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
   int planes = 0;
   for (auto &g : groups) planes += g.P;
   SX_TRY(reserve_ws(*s, planes));
-  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
-  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
   const bool same = s->gexec && s->gkey[0] == d_u && s->gkey[1] == d_f && s->gkey[2] == d_bc &&
                     s->gnz == nz && s->gstride == plane_stride && s->gprec == precision;
-  if (!same) {
+  const MeshView M = s->mesh->view();
+  if (!same || !s->use_graphs) {
     if (s->gexec) {
       cudaGraphExecDestroy(s->gexec);
       s->gexec = nullptr;
@@ -446,40 +430,60 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
       slot += g.P;
     }
     if (s->bjobs.n < jobs.size()) SX_TRY(s->bjobs.alloc(jobs.size()));
-    SX_CUDA(cudaMemcpy(s->bjobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice));
-    const MeshView M = s->mesh->view();
-    // warm the kernel attributes outside capture
+    SX_CUDA(cudaMemcpyAsync(s->bjobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
+    SX_CUDA(cudaStreamSynchronize(st));
     SX_TRY(prepare_direct_kernels(M));
     const int C = s->cluster((int)jobs.size());
-    cudaGraph_t g = nullptr;
-    SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches);
     s->gjobs = jobs;
     s->gC = C;
-    const cudaError_t ce = cudaStreamEndCapture(st, &g);
-    if (rc != SX_OK) {
-      if (g) cudaGraphDestroy(g);
-      return rc;
+    if (!s->use_graphs) {
+      SX_TRY(direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches));
+    } else {
+      cudaGraph_t g = nullptr;
+      SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches);
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (rc != SX_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      SX_CUDA(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
+      cudaGraphDestroy(g);
+      SX_CUDA(ie);
+      s->gkey[0] = d_u;
+      s->gkey[1] = d_f;
+      s->gkey[2] = d_bc;
+      s->gnz = nz;
+      s->gstride = plane_stride;
+      s->gprec = precision;
     }
-    SX_CUDA(ce);
-    const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
-    cudaGraphDestroy(g);
-    SX_CUDA(ie);
-    s->gkey[0] = d_u;
-    s->gkey[1] = d_f;
-    s->gkey[2] = d_bc;
-    s->gnz = nz;
-    s->gstride = plane_stride;
-    s->gprec = precision;
   }
-  SX_CUDA(cudaGraphLaunch(s->gexec, st));
-  if (!stream) SX_TRY(take_status(s, true));
+  if (s->use_graphs) SX_CUDA(cudaGraphLaunch(s->gexec, st));
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->planes_solved = planes;
     stats->kernel_launches = s->glaunches;
   }
   return SX_OK;
+}
+
+}  // namespace sx
+
+// Batched form: every mode's planes in each launch (one job per mode), the
+// whole sequence captured once into a CUDA graph and replayed.
+extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
+                                      int plane_stride, int precision, double tol_rel, int max_refine,
+                                      void *stream, sx_solve_stats *stats) {
+  if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+  if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
+  const int rc = solve_batched_on(s, d_u, d_f, d_bc, nz, plane_stride, precision, tol_rel, max_refine, st,
+                                  stats);
+  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  if (!stream) SX_TRY(take_status(s, true));
+  return rc;
 }
 
 extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *f, const double *bc,
@@ -495,12 +499,11 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
   cudaStream_t st = s->own;
   SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));
   if (bc) SX_CUDA(cudaMemcpyAsync(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice, st));
-  const int rc = sx_field_solve_batched(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride,
-                                        precision, tol_rel, max_refine, st, stats);
+  const int rc = solve_batched_on(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride, precision,
+                                  tol_rel, max_refine, st, stats);
   if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
   SX_CUDA(cudaMemcpyAsync(u, s->hu.p, n * 8, cudaMemcpyDeviceToHost, st));
-  SX_CUDA(cudaStreamSynchronize(st));
-  SX_TRY(take_status(s, true));
+  SX_TRY(take_status(s, true, st, false));
   return rc;
 }
 

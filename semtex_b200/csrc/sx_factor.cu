@@ -402,12 +402,12 @@ int factor_batch(std::vector<System *> &systems, cudaStream_t st) {
     maxJ = std::max(maxJ, S.J);
   }
   DBuf<SysDesc> dd;
-  SX_TRY(dd.upload(hd.data(), hd.size()));
+  SX_TRY(dd.upload_on(hd.data(), hd.size(), st));
   std::vector<int2> pairs;
   for (int j = 1; j <= maxJ; j++)
     for (int i = 1; i <= j; i++) pairs.push_back(make_int2(i, j));
   DBuf<int2> dpairs;
-  if (!pairs.empty()) SX_TRY(dpairs.upload(pairs.data(), pairs.size()));
+  if (!pairs.empty()) SX_TRY(dpairs.upload_on(pairs.data(), pairs.size(), st));
   const size_t sm3 = 3 * TSZ * sizeof(double), sm2 = 2 * TSZ * sizeof(double);
   SX_CUDA(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   SX_CUDA(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
@@ -439,7 +439,7 @@ int system_build_direct(System &S, cudaStream_t st) {
   SX_TRY(S.hbi.alloc((size_t)Mh.nel * Mh.next * Mh.nint));
   SX_TRY(S.hii.alloc((size_t)Mh.nel * Mh.nint * Mh.nint));
   DBuf<double> hbb;
-  SX_TRY(hbb.alloc((size_t)Mh.nel * Mh.next * Mh.next));
+  SX_TRY(hbb.alloc_on((size_t)Mh.nel * Mh.next * Mh.next, st));
   const size_t smem = condense_smem(M);
   SX_CUDA(cudaFuncSetAttribute(k_elem_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_elem_condense<<<Mh.nel, 256, smem, st>>>(M, hCon, S.hbi.p, S.hii.p, hbb.p, S.status.p);
@@ -481,7 +481,7 @@ int system_build_jacobi_diag(System &S, cudaStream_t st) {
   const double hCon = S.betak2 + S.lambda2;
   const int npts = Mh.nglobal + Mh.nel * Mh.nint;
   DBuf<double> ediag;
-  SX_TRY(ediag.alloc((size_t)Mh.nel * Mh.npnp));
+  SX_TRY(ediag.alloc_on((size_t)Mh.nel * Mh.npnp, st));
   SX_TRY(S.pc.alloc(npts));
   SX_TRY(S.pcf.alloc(npts));
   k_elem_diag<<<Mh.nel, 128, 0, st>>>(M, hCon, ediag.p);

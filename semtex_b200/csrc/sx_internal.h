@@ -38,6 +38,9 @@ struct Status {
 // Thread-local last error message, for sx_status_string callers.
 void set_error(const char *fmt, ...);
 
+// GLL points, weights and derivative matrix (row-major D[i][j] = h_j'(z_i)).
+void gll_tables(int np, std::vector<double> &z, std::vector<double> &w, std::vector<double> &D);
+
 #define SX_CUDA(call)                                                                  \
   do {                                                                                 \
     cudaError_t e_ = (call);                                                           \
@@ -54,18 +57,48 @@ void set_error(const char *fmt, ...);
   } while (0)
 
 // Device buffer with RAII release.
+// alloc()/upload() use cudaMalloc (long-lived data); alloc_on()/upload_on()
+// use the stream-ordered allocator on a stream, so releasing a temporary
+// never synchronises the device (cudaFree would).
 template <typename T>
 struct DBuf {
   T *p = nullptr;
   size_t n = 0;
+  bool ordered = false;
+  cudaStream_t os = nullptr;
   DBuf() = default;
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (ordered)
+        cudaFreeAsync(p, os);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    ordered = false;
+  }
+  int alloc_on(size_t count, cudaStream_t s) {
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&p), count * sizeof(T), s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error("cudaMallocAsync(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+      return SX_ERR_NOMEM;
+    }
+    n = count;
+    ordered = true;
+    os = s;
+    return SX_OK;
+  }
+  int upload_on(const T *h, size_t count, cudaStream_t s) {
+    SX_TRY(alloc_on(count, s));
+    SX_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return SX_OK;
   }
   int alloc(size_t count) {
     release();
@@ -103,6 +136,8 @@ struct MeshView {
   const int *btog, *bmask, *emask;       // nel*next, nel*next, nel
   const int *g2e_ptr, *g2e_idx;          // CSR: global node -> (e*next+i), element order
   const int *g2e_last;                   // nglobal: last (e*next+i) writing node (local2global)
+  const int4 *g2e4;                      // nglobal: first 4 CSR entries, -1 padded, .w = -2 if more
+  const unsigned long long *owner;       // nel: bit a set when element e is node btog[e][a]'s last writer
   int nbound;
   const int *b_elmt, *b_side, *b_kind;
   const double *b_K, *b_C, *b_area;      // b_area: nbound*np
@@ -134,6 +169,8 @@ struct sx_mesh_s {
   sx::DBuf<unsigned char> dhasQ3;
   sx::DBuf<int> demap, dbtog, dbmask, demask, dg2e_ptr, dg2e_idx, dg2e_last, dbe, dbs, dbk;
   sx::DBuf<int> dnat_ptr, dnat_idx, dcolour_elmt;
+  sx::DBuf<int4> dg2e4;
+  sx::DBuf<unsigned long long> downer;
   sx::MeshView view() const;
 };
 

@@ -195,6 +195,7 @@ sx::MeshView sx_mesh_s::view() const {
   v.hasQ3 = dhasQ3.p;
   v.btog = dbtog.p; v.bmask = dbmask.p; v.emask = demask.p;
   v.g2e_ptr = dg2e_ptr.p; v.g2e_idx = dg2e_idx.p; v.g2e_last = dg2e_last.p;
+  v.g2e4 = dg2e4.p; v.owner = downer.p;
   v.nbound = nbound; v.b_elmt = dbe.p; v.b_side = dbs.p; v.b_kind = dbk.p;
   v.b_K = dK.p; v.b_C = dC.p; v.b_area = darea.p;
   v.nat_ptr = dnat_ptr.p; v.nat_idx = dnat_idx.p;
@@ -362,6 +363,22 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   SX_TRY(M->dg2e_ptr.upload(ptr.data(), ptr.size()));
   SX_TRY(M->dg2e_idx.upload(idx.data(), idx.size()));
   SX_TRY(M->dg2e_last.upload(last.data(), last.size()));
+  {
+    std::vector<int4> g4(d->nglobal);
+    for (int g = 0; g < d->nglobal; g++) {
+      int v[4] = {-1, -1, -1, -1};
+      const int n = ptr[g + 1] - ptr[g];
+      for (int k = 0; k < std::min(n, 4); k++) v[k] = idx[ptr[g] + k];
+      if (n > 4) v[3] = -2;  // more than 4 contributions: walk the CSR
+      g4[g] = make_int4(v[0], v[1], v[2], v[3]);
+    }
+    SX_TRY(M->dg2e4.upload(g4.data(), g4.size()));
+    std::vector<unsigned long long> own(nel, 0ull);
+    for (int e = 0; e < nel; e++)
+      for (int a = 0; a < next; a++)
+        if (last[M->btog[(size_t)e * next + a]] == e * next + a) own[e] |= 1ull << a;
+    SX_TRY(M->downer.upload(own.data(), own.size()));
+  }
   std::vector<int> be(M->b_elmt), bs(M->b_side), bk(M->b_kind);
   if (nb == 0) { be.push_back(0); bs.push_back(0); bk.push_back(0); M->b_K.push_back(0); M->b_C.push_back(0); }
   SX_TRY(M->dbe.upload(be.data(), be.size()));

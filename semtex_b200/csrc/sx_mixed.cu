@@ -5,26 +5,34 @@
 //
 //   b      = FP64 RHS of the JACPCG branch (constrain + buildRHS,
 //            src/field.cpp:641-650), essential tail zero
-//   repeat   d  = FP32 Jacobi-PCG on  A d = r  (n_inner iterations,
+//   repeat   d  = FP32 Jacobi-PCG on  A d = r  (n_inner iterations of
 //                 src/field.cpp:672-704 with FP32 vectors and operator)
 //            x += d              (FP64)
 //            r  = b - A x        (FP64 operator, FP64 residual)
 //   until  ||r|| <= tol ||b|| for every plane
 //
+// Layout: vectors are plane-interleaved, V[g * PP + p] (node g, plane p),
+// so a gather or scatter through btog moves 32 consecutive planes of one
+// node in one coalesced access, and index, geometry and operator tables are
+// loaded once for all planes.  Thread mapping everywhere: lane = plane
+// within a chunk of 32 (blockIdx.y = chunk), warp = node row.
+//
 // One inner iteration is two kernels, each with its reduction fused in:
-//   k_mx_op32   p <- z + beta p (z = PC r) on the fly, element operator
-//               q_e = A_e p_e (FP32 sum factorisation), interior q stored,
-//               boundary contributions to an element-local buffer, and
-//               p.q = sum_e p_e . q_e (equal to the assembled dot because p
-//               vanishes on essential nodes)
-//   k_mx_upd    direct-stiffness gather of q (element order), d += alpha p,
-//               r -= alpha q, rho = r.(PC r)
-// Reductions are two-level and deterministic: per-block partials, the last
-// block to finish sums them in index order.  Each refinement round is one
-// captured CUDA graph; the host reads the residual norms between rounds.
+//   k_x_op32  p <- z + beta p (z = PC r) on the fly, element operator
+//             q_e = A_e p_e (FP32 sum factorisation), interior q stored,
+//             boundary contributions to an element-local buffer, and
+//             p.q = sum_e p_e . q_e (the assembled dot: p vanishes on
+//             essential nodes)
+//   k_x_upd   direct-stiffness gather of q (element order), d += alpha p,
+//             r -= alpha q, rho = r.(PC r)
+// Reductions are two-level and deterministic: per-block partials per plane,
+// the last block of a chunk sums them in index order.  Each refinement round
+// is one captured CUDA graph; the host reads the residual norms between
+// rounds.
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <mutex>
 
 #include "sx_kernels.cuh"
 #include "sx_mixed.cuh"
@@ -32,169 +40,304 @@
 
 namespace sx {
 
-// ---------------------------------------------------------------------------
-// deterministic per-plane reduction of a pair of values
-// ---------------------------------------------------------------------------
+constexpr int MX_ROWS = 8;  // node rows per 256-thread block
 
-__device__ __forceinline__ void reduce_pair(double a, double b, double *part, unsigned *cnt, int maxblk,
-                                            int nblk, int plane, int bid, double *outA, double *outB) {
-  __shared__ double sa[32], sb[32];
+__device__ __forceinline__ int gidx(const MeshView &M, int e, int a) {
+  return a < M.next ? M.btog[(size_t)e * M.next + a] : M.nglobal + e * M.nint + (a - M.next);
+}
+
+__device__ __forceinline__ bool real_plane(const MxParams &P, int p) { return p < P.nz && p != P.nyq; }
+
+// Direct-stiffness sum of element-local boundary values at global node g,
+// in element order (the CSR order): up to four loads issued together.
+template <typename T>
+__device__ __forceinline__ T dss_gather(const MeshView &M, const T *__restrict__ Y, int g, int PP, int p) {
+  const int4 q = M.g2e4[g];
+  if (q.w == -2) {
+    T s = 0;
+    for (int k = M.g2e_ptr[g]; k < M.g2e_ptr[g + 1]; k++) s += Y[(size_t)M.g2e_idx[k] * PP + p];
+    return s;
+  }
+  const T v0 = Y[(size_t)q.x * PP + p];
+  const T v1 = q.y >= 0 ? Y[(size_t)q.y * PP + p] : T(0);
+  const T v2 = q.z >= 0 ? Y[(size_t)q.z * PP + p] : T(0);
+  const T v3 = q.w >= 0 ? Y[(size_t)q.w * PP + p] : T(0);
+  return ((v0 + v1) + v2) + v3;
+}
+
+__device__ __forceinline__ int pc_col(const MxParams &P, int p) { return min(p >> 1, P.M - 1); }
+
+// FP64 element results: boundary slots as an element-local buffer
+// [nel][next][PP] (gathered through btog's CSR), then interior nodes in
+// global order [nel*nint][PP].
+__device__ __forceinline__ size_t ye_index(const MeshView &M, int e, int a, int PP) {
+  return a < M.next ? ((size_t)e * M.next + a) * PP
+                    : ((size_t)M.nel * M.next + (size_t)e * M.nint + (a - M.next)) * PP;
+}
+
+// Per-plane sums over the 8 rows of the block, then over the blocks of the
+// chunk (last block, index order).
+__device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, unsigned *cnt, int G, double *outA,
+                                              double *outB) {
+  __shared__ double sa[MX_ROWS][MX_CH], sb[MX_ROWS][MX_CH];
   __shared__ int last;
-  a = warp_sum(a);
-  b = warp_sum(b);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-  if (l == 0) {
-    sa[w] = a;
-    sb[w] = b;
-  }
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.y * MX_CH + lane;
+  sa[row][lane] = a;
+  sb[row][lane] = b;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  // partials laid out [block][plane][2] so the final pass reads them
+  // coalesced across the lanes (planes)
+  const int PPc = gridDim.y * MX_CH;
+  if (row == 0) {
     double ta = 0.0, tb = 0.0;
-    for (int i = 0; i < nw; i++) {
-      ta += sa[i];
-      tb += sb[i];
+    for (int r = 0; r < MX_ROWS; r++) {
+      ta += sa[r][lane];
+      tb += sb[r][lane];
     }
-    double *pp = part + ((size_t)plane * maxblk + bid) * 2;
-    pp[0] = ta;
-    pp[1] = tb;
-    __threadfence();
-    const unsigned t = atomicAdd(&cnt[plane], 1u);
-    last = (t == (unsigned)(nblk - 1));
+    double2 *pp = reinterpret_cast<double2 *>(part) + (size_t)blockIdx.x * PPc + p;
+    *pp = make_double2(ta, tb);
   }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&cnt[blockIdx.y], 1u) == gridDim.x - 1);
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const double *pp = part + (size_t)plane * maxblk * 2;
   double ta = 0.0, tb = 0.0;
-  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
-    ta += __ldcg(&pp[2 * i]);
-    tb += __ldcg(&pp[2 * i + 1]);
+  const double2 *pp = reinterpret_cast<const double2 *>(part) + p;
+  int bx = row;
+#pragma unroll 1
+  for (; bx + 3 * MX_ROWS < G; bx += 4 * MX_ROWS) {
+    const double2 v0 = __ldcg(&pp[(size_t)bx * PPc]);
+    const double2 v1 = __ldcg(&pp[(size_t)(bx + MX_ROWS) * PPc]);
+    const double2 v2 = __ldcg(&pp[(size_t)(bx + 2 * MX_ROWS) * PPc]);
+    const double2 v3 = __ldcg(&pp[(size_t)(bx + 3 * MX_ROWS) * PPc]);
+    ta += v0.x; tb += v0.y;
+    ta += v1.x; tb += v1.y;
+    ta += v2.x; tb += v2.y;
+    ta += v3.x; tb += v3.y;
   }
-  ta = warp_sum(ta);
-  tb = warp_sum(tb);
-  __syncthreads();
-  if (l == 0) {
-    sa[w] = ta;
-    sb[w] = tb;
+  for (; bx < G; bx += MX_ROWS) {
+    const double2 v = __ldcg(&pp[(size_t)bx * PPc]);
+    ta += v.x;
+    tb += v.y;
   }
+  sa[row][lane] = ta;
+  sb[row][lane] = tb;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (row == 0) {
     double fa = 0.0, fb = 0.0;
-    for (int i = 0; i < nw; i++) {
-      fa += sa[i];
-      fb += sb[i];
+    for (int r = 0; r < MX_ROWS; r++) {
+      fa += sa[r][lane];
+      fb += sb[r][lane];
     }
-    if (outA) *outA = fa;
-    if (outB) *outB = fb;
-    cnt[plane] = 0;
+    if (outA) outA[p] = fa;
+    if (outB) outB[p] = fb;
+  }
+  if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
+}
+
+// GLL derivative matrices for np = 3..12, FP32 and FP64, in constant memory:
+// the operator indexes them with warp-uniform subscripts (lanes are planes),
+// so every read is a constant-cache broadcast and stays off the shared-memory
+// pipe.  Filled once per device from the same GLL routine as the mesh.
+constexpr int D_TOTAL = 645;  // sum of np^2, np = 3..12
+__constant__ float c_Df[D_TOTAL];
+__constant__ double c_Dd[D_TOTAL];
+template <int NP>
+struct DOff {
+  static constexpr int v = DOff<NP - 1>::v + (NP - 1) * (NP - 1);
+};
+template <>
+struct DOff<3> {
+  static constexpr int v = 0;
+};
+template <typename T>
+__device__ __forceinline__ T cD(int i);
+template <>
+__device__ __forceinline__ float cD<float>(int i) {
+  return c_Df[i];
+}
+template <>
+__device__ __forceinline__ double cD<double>(int i) {
+  return c_Dd[i];
+}
+
+static int ensure_constD() {
+  static std::mutex mu;
+  static std::vector<char> done(256, 0);
+  int dev = 0;
+  SX_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 256 && done[dev]) return SX_OK;
+  std::vector<float> f(D_TOTAL);
+  std::vector<double> d(D_TOTAL);
+  int off = 0;
+  for (int np = NP_MIN; np <= NP_MAX; np++) {
+    std::vector<double> z, w, D;
+    gll_tables(np, z, w, D);
+    for (int k = 0; k < np * np; k++) {
+      d[off + k] = D[k];
+      f[off + k] = (float)D[k];
+    }
+    off += np * np;
+  }
+  SX_CUDA(cudaMemcpyToSymbol(c_Df, f.data(), sizeof(float) * D_TOTAL));
+  SX_CUDA(cudaMemcpyToSymbol(c_Dd, d.data(), sizeof(double) * D_TOTAL));
+  if (dev < 256) done[dev] = 1;
+  return SX_OK;
+}
+
+// Sum-factorised element operator on plane-interleaved smem arrays
+// U, R, S [NN][32]: out(idx) for the calling lane (Element::HelmholtzOp +
+// HelmholtzKern, src/element.cpp:1564-1650).
+template <int NP, typename T>
+__device__ __forceinline__ void op_stage1(const T *, const T *Q1, const T *Q2, const T *Q3, bool q3, const T *U,
+                                          T *R, T *S) {
+  constexpr int NN = NP * NP, DO = DOff<NP>::v;
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int idx = row; idx < NN; idx += MX_ROWS) {
+    const int i = idx / NP, j = idx - i * NP;
+    T r = 0, s = 0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      r += U[(i * NP + k) * MX_CH + lane] * cD<T>(DO + j * NP + k);
+      s += cD<T>(DO + i * NP + k) * U[(k * NP + j) * MX_CH + lane];
+    }
+    if (q3) {
+      R[idx * MX_CH + lane] = Q1[idx] * r + Q3[idx] * s;
+      S[idx * MX_CH + lane] = Q2[idx] * s + Q3[idx] * r;
+    } else {
+      R[idx * MX_CH + lane] = Q1[idx] * r;
+      S[idx * MX_CH + lane] = Q2[idx] * s;
+    }
   }
 }
 
-// global index of local (edge-map order) node a of element e
-__device__ __forceinline__ int gidx(const MeshView &M, int e, int a) {
-  return a < M.next ? M.btog[(size_t)e * M.next + a] : M.nglobal + e * M.nint + (a - M.next);
+template <int NP, typename T>
+__device__ __forceinline__ T op_stage2(const T *, const T *Q4, T hcon, const T *U, const T *R, const T *S, int idx) {
+  constexpr int DO = DOff<NP>::v;
+  const int lane = threadIdx.x & 31;
+  const int i = idx / NP, j = idx - i * NP;
+  T t = Q4[idx] * U[idx * MX_CH + lane] * hcon;
+  T a = 0, b = 0;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    a += cD<T>(DO + k * NP + i) * S[(k * NP + j) * MX_CH + lane];
+    b += R[(i * NP + k) * MX_CH + lane] * cD<T>(DO + k * NP + j);
+  }
+  return t + a + b;
 }
 
 // ---------------------------------------------------------------------------
 // RHS (FP64)
 // ---------------------------------------------------------------------------
 
-__global__ void k_mx_ess(MeshView M, const MxPlane *__restrict__ planes) {
-  const MxPlane P = planes[blockIdx.x];
-  if (threadIdx.x || P.bc == nullptr) return;
+__global__ void k_x_ess(MeshView M, MxParams P) {
+  const int p = blockIdx.x;
+  if (threadIdx.x || !P.bc || !real_plane(P, p)) return;
   const int np = M.np, nm = np - 1;
+  double *g = P.gess + (size_t)p * M.nglobal;
+  const double *bc = P.bc + (size_t)p * P.bcstride;
   for (int b = 0; b < M.nbound; b++) {
     if (M.b_kind[b] != SX_BC_ESSENTIAL) continue;
     const int *bmap = M.btog + (size_t)M.b_elmt[b] * M.next;
     const int side = M.b_side[b];
-    const double *src = P.bc + (size_t)b * np;
-    for (int i = 0; i < nm; i++) P.gess[bmap[side * nm + i]] = src[i];
+    const double *src = bc + (size_t)b * np;
+    for (int i = 0; i < nm; i++) g[bmap[side * nm + i]] = src[i];
     if (side == 3)
-      P.gess[bmap[0]] = src[nm];
+      g[bmap[0]] = src[nm];
     else
-      P.gess[bmap[side * nm + nm]] = src[nm];
+      g[bmap[side * nm + nm]] = src[nm];
   }
 }
 
-// Ye[plane][e] = -(M f + H g) in edge-map order (Field::constrain).
+// Ye[(e*NN + a)*PP + p] = -(M f + H g) at edge-map slot a (Field::constrain).
 template <int NP>
-__global__ void __launch_bounds__(128) k_mx_constrain(MeshView M, const MxPlane *__restrict__ planes,
-                                                      double *__restrict__ Ye) {
+__global__ void __launch_bounds__(256) k_x_constrain(MeshView M, MxParams P, double *__restrict__ Ye) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1);
-  const MxPlane P = planes[blockIdx.y];
-  const int e = blockIdx.x, tid = threadIdx.x;
-  __shared__ double D[NN], Q[4][NN], u[NN], R[NN], S[NN], out[NN], F[NN];
+  extern __shared__ __align__(16) double smx[];
+  double *F = smx, *U = F + NN * MX_CH, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
+  __shared__ double D[NN], Q[5][NN];
   __shared__ int emap[NN];
+  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  const int p0 = blockIdx.y * MX_CH, p = p0 + lane;
   const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 128) {
+  for (int i = tid; i < NN; i += 256) {
     D[i] = M.D[i];
+    Q[0][i] = M.Q1[eo + i];
+    Q[1][i] = M.Q2[eo + i];
+    Q[2][i] = M.Q3[eo + i];
+    Q[3][i] = M.Q4[eo + i];
+    Q[4][i] = M.Q8[eo + i];
     emap[i] = M.emap[i];
-    F[i] = P.f[eo + i] * M.Q8[eo + i];
-  }
-  if (M.emask[e]) {
-    for (int i = tid; i < NN; i += 128) {
-      Q[0][i] = M.Q1[eo + i];
-      Q[1][i] = M.Q2[eo + i];
-      Q[2][i] = M.Q3[eo + i];
-      Q[3][i] = M.Q4[eo + i];
-      u[i] = 0.0;
-    }
-    __syncthreads();
-    for (int a = tid; a < NE; a += 128) u[emap[a]] = P.gess[M.btog[(size_t)e * NE + a]];
-    __syncthreads();
-    helm_op<NP, double>(D, Q[0], Q[1], Q[2], Q[3], M.hasQ3[e] != 0, P.hCon, u, R, S, out, 128);
-    for (int i = tid; i < NN; i += 128) F[i] += out[i];
   }
   __syncthreads();
-  double *y = Ye + ((size_t)blockIdx.y * M.nel + e) * NN;
-  for (int a = tid; a < NN; a += 128) y[a] = -F[emap[a]];
+  // transpose the forcing in: plane by plane, contiguous element values
+  for (int q = 0; q < MX_CH; q++) {
+    const int pl = p0 + q;
+    const bool rp = real_plane(P, pl);
+    for (int k = tid; k < NN; k += 256)
+      F[k * MX_CH + q] = rp ? Q[4][k] * P.f[(size_t)pl * P.stride + eo + k] : 0.0;
+  }
+  __syncthreads();
+  if (M.emask[e]) {
+    const double *g = P.gess + (size_t)p * M.nglobal;
+    const bool rp = real_plane(P, p);
+    for (int a = row; a < NN; a += MX_ROWS)
+      U[emap[a] * MX_CH + lane] = (rp && a < NE) ? g[M.btog[(size_t)e * NE + a]] : 0.0;
+    __syncthreads();
+    op_stage1<NP, double>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
+    __syncthreads();
+    const double hc = P.hcon[p];
+    for (int idx = row; idx < NN; idx += MX_ROWS)
+      F[idx * MX_CH + lane] += op_stage2<NP, double>(D, Q[3], hc, U, R, S, idx);
+    __syncthreads();
+  }
+  for (int a = row; a < NN; a += MX_ROWS) Ye[ye_index(M, e, a, P.PP) + p] = -F[emap[a] * MX_CH + lane];
 }
 
 // b = DSS(Ye) + <h,w>, essential tail zero; x = 0, d = 0, r = b (FP32),
-// p_0 = PC r; reduces ||b||^2 and rho_0.
-__global__ void __launch_bounds__(256) k_mx_rhs(MeshView M, const MxPlane *__restrict__ planes,
-                                                const double *__restrict__ Ye, double *b64, double *x64,
-                                                float *r32, float *d32, float *p0, MxScal *scal,
-                                                double *part, unsigned *cnt, int maxblk) {
-  const int plane = blockIdx.y;
-  const MxPlane P = planes[plane];
+// p_0 = PC r; per-plane ||b||^2 and rho_0.
+__global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const double *__restrict__ Ye, double *b64,
+                                               double *x64, float *r32, float *d32, float *p0, double *b2,
+                                               double *rho0, double *part, unsigned *cnt) {
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t o = (size_t)plane * npts;
+  const int ns = P.nsolve[p], c = pc_col(P, p);
+  const bool rp = real_plane(P, p);
   double bb = 0.0, rz = 0.0;
-  if (g < npts) {
+  for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
     double s = 0.0;
-    const double *y = Ye + (size_t)plane * M.nel * M.npnp;
     if (g < M.nglobal) {
-      if (g < P.nsolve) {
-        for (int q = M.g2e_ptr[g]; q < M.g2e_ptr[g + 1]; q++) {
-          const int ei = M.g2e_idx[q], e = ei / M.next, i = ei - e * M.next;
-          s += y[(size_t)e * M.npnp + i];
-        }
-        for (int q = M.nat_ptr[g]; q < M.nat_ptr[g + 1]; q++) {
-          const int bi = M.nat_idx[q], bnd = bi / M.np;
-          if (M.b_kind[bnd] == SX_BC_NATURAL)
-            s += (P.bc ? P.bc[bi] : 0.0) * M.b_area[bi];
-          else
-            s += (M.b_K[bnd] * M.b_C[bnd]) * M.b_area[bi];
-        }
+      if (g < ns) {
+        s = dss_gather(M, Ye, g, PP, p);
+        if (rp)
+          for (int q = M.nat_ptr[g]; q < M.nat_ptr[g + 1]; q++) {
+            const int bi = M.nat_idx[q], bnd = bi / M.np;
+            if (M.b_kind[bnd] == SX_BC_NATURAL)
+              s += (P.bc ? P.bc[(size_t)p * P.bcstride + bi] : 0.0) * M.b_area[bi];
+            else
+              s += (M.b_K[bnd] * M.b_C[bnd]) * M.b_area[bi];
+          }
       }
     } else {
-      const int r = g - M.nglobal, e = r / M.nint, i = r - e * M.nint;
-      s = y[(size_t)e * M.npnp + M.next + i];
+      s = Ye[((size_t)M.nel * M.next + (g - M.nglobal)) * PP + p];
     }
-    b64[o + g] = s;
-    x64[o + g] = 0.0;
+    const size_t o = (size_t)g * PP + p;
+    b64[o] = s;
+    x64[o] = 0.0;
     const float rf = (float)s;
-    r32[o + g] = rf;
-    d32[o + g] = 0.0f;
-    const float z = P.pcf[g] * rf;
-    p0[o + g] = z;
-    bb = s * s;
-    rz = (double)rf * (double)z;
+    r32[o] = rf;
+    d32[o] = 0.0f;
+    const float z = P.pcf[(size_t)g * P.M + c] * rf;
+    p0[o] = z;
+    bb += s * s;
+    rz += (double)rf * (double)z;
   }
-  double *ob = &scal[plane].b2;
-  reduce_pair(bb, rz, part, cnt, maxblk, gridDim.x, plane, blockIdx.x, ob, &scal[plane].rho[0]);
+  chunk_reduce2(bb, rz, part, cnt, gridDim.x, b2, rho0);
 }
 
 // ---------------------------------------------------------------------------
@@ -202,97 +345,128 @@ __global__ void __launch_bounds__(256) k_mx_rhs(MeshView M, const MxPlane *__res
 // ---------------------------------------------------------------------------
 
 template <int NP>
-__global__ void __launch_bounds__(128) k_mx_op32(MeshView M, const MxPlane *__restrict__ planes,
-                                                 const float *__restrict__ r32, const float *__restrict__ pold,
-                                                 float *__restrict__ pnew, float *__restrict__ q32,
-                                                 float *__restrict__ Yb, MxScal *scal, int it,
-                                                 double *part, unsigned *cnt, int maxblk) {
+__global__ void __launch_bounds__(256) k_x_op32(MeshView M, MxParams P, const float *__restrict__ r32,
+                                                const float *__restrict__ pold, float *__restrict__ pnew,
+                                                float *__restrict__ q32, float *__restrict__ Yb,
+                                                const double *rho_i, const double *rho_im1, double *pq_out, int it,
+                                                double *part, unsigned *cnt) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
-  const int plane = blockIdx.y;
-  const MxPlane P = planes[plane];
-  const int e = blockIdx.x, tid = threadIdx.x;
-  const int npts = M.nglobal + M.nel * M.nint;
-  const size_t o = (size_t)plane * npts;
-  __shared__ float D[NN], Q[4][NN], u[NN], R[NN], S[NN], out[NN];
-  __shared__ int emap[NN];
+  constexpr int NA = (NN + MX_ROWS - 1) / MX_ROWS;  // nodes per warp row
+  extern __shared__ __align__(16) float smf[];
+  float *U = smf, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
+  __shared__ float D[NN], Q[4][NN];
+  __shared__ int emap[NN], gtab[NN];
+  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const size_t eo = (size_t)e * NN;
-  float beta = 0.0f;
-  if (it > 0) {
-    const double rn = scal[plane].rho[it & 1], ro = scal[plane].rho[(it - 1) & 1];
-    beta = (ro != 0.0) ? (float)(rn / ro) : 0.0f;
-  }
-  for (int i = tid; i < NN; i += 128) {
+  for (int i = tid; i < NN; i += 256) {
     D[i] = M.Df[i];
     Q[0][i] = M.Q1f[eo + i];
     Q[1][i] = M.Q2f[eo + i];
     Q[2][i] = M.Q3f[eo + i];
     Q[3][i] = M.Q4f[eo + i];
     emap[i] = M.emap[i];
+    gtab[i] = (i < NE) ? M.btog[(size_t)e * NE + i] : M.nglobal + e * NI + (i - NE);
   }
+  float beta = 0.0f;
+  if (it > 0) {
+    const double rn = rho_i[p], ro = rho_im1[p];
+    beta = (ro != 0.0) ? (float)(rn / ro) : 0.0f;
+  }
+  const int c = pc_col(P, p);
+  // one writer per global node: the last element that touches it
+  const unsigned long long own = M.owner[e];
   __syncthreads();
-  for (int a = tid; a < NN; a += 128) {
-    const int g = gidx(M, e, a);
-    float pv;
-    if (it == 0) {
-      pv = pold[o + g];
-    } else {
-      const float z = P.pcf[g] * r32[o + g];
-      pv = z + beta * pold[o + g];
-      // one writer per global node: the last element that touches it
-      if (a >= NE || M.g2e_last[g] == e * NE + a) pnew[o + g] = pv;
+  // gather: every load of this thread issued before any is used
+  float pv[NA], rv[NA], cv[NA];
+#pragma unroll
+  for (int t = 0; t < NA; t++) {
+    const int a = row + t * MX_ROWS;
+    if (a < NN) {
+      const int g = gtab[a];
+      const size_t o = (size_t)g * PP + p;
+      pv[t] = pold[o];
+      if (it > 0) {
+        rv[t] = r32[o];
+        cv[t] = P.pcf[(size_t)g * P.M + c];
+      }
     }
-    u[emap[a]] = pv;
+  }
+#pragma unroll
+  for (int t = 0; t < NA; t++) {
+    const int a = row + t * MX_ROWS;
+    if (a < NN) {
+      float v = pv[t];
+      if (it > 0) {
+        v = cv[t] * rv[t] + beta * v;
+        if (a >= NE || ((own >> a) & 1ull)) pnew[(size_t)gtab[a] * PP + p] = v;
+      }
+      U[emap[a] * MX_CH + lane] = v;
+    }
   }
   __syncthreads();
-  helm_op<NP, float>(D, Q[0], Q[1], Q[2], Q[3], M.hasQ3[e] != 0, (float)P.hCon, u, R, S, out, 128);
+  op_stage1<NP, float>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
+  __syncthreads();
+  const float hc = (float)P.hcon[p];
   double pq = 0.0;
-  for (int a = tid; a < NN; a += 128) {
-    const float qv = out[emap[a]];
-    pq += (double)(u[emap[a]] * qv);
+  for (int a = row; a < NN; a += MX_ROWS) {
+    const int idx = emap[a];
+    const float t = op_stage2<NP, float>(D, Q[3], hc, U, R, S, idx);
+    pq += (double)(U[idx * MX_CH + lane] * t);
     if (a < NE)
-      Yb[((size_t)plane * M.nel + e) * NE + a] = qv;
+      Yb[((size_t)e * NE + a) * PP + p] = t;
     else
-      q32[o + M.nglobal + (size_t)e * NI + (a - NE)] = qv;
+      q32[(size_t)gtab[a] * PP + p] = t;
   }
-  reduce_pair(pq, 0.0, part, cnt, maxblk, gridDim.x, plane, blockIdx.x, &scal[plane].pq[it & 1], nullptr);
+  chunk_reduce2(pq, 0.0, part, cnt, gridDim.x, pq_out, nullptr);
 }
 
-__global__ void __launch_bounds__(256) k_mx_upd(MeshView M, const MxPlane *__restrict__ planes,
-                                                const float *__restrict__ pcur, const float *__restrict__ q32,
-                                                const float *__restrict__ Yb, float *d32, float *r32,
-                                                double *x64, MxScal *scal, int it, int last, double *part,
-                                                unsigned *cnt, int maxblk) {
-  const int plane = blockIdx.y;
-  const MxPlane P = planes[plane];
+__global__ void __launch_bounds__(256) k_x_upd(MeshView M, MxParams P, const float *__restrict__ pcur,
+                                               const float *__restrict__ q32, const float *__restrict__ Yb,
+                                               float *d32, float *r32, double *x64, const double *rho_i,
+                                               const double *pq_i, double *rho_next, int last, double *part,
+                                               unsigned *cnt) {
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t o = (size_t)plane * npts;
-  const double rho = scal[plane].rho[it & 1], pq = scal[plane].pq[it & 1];
-  const float alpha = (pq > 0.0) ? (float)(rho / pq) : 0.0f;
+  const int ns = P.nsolve[p], c = pc_col(P, p);
+  const double pq = pq_i[p];
+  const float alpha = (pq > 0.0) ? (float)(rho_i[p] / pq) : 0.0f;
   double rz = 0.0;
-  if (g < npts) {
-    float q = 0.0f;
-    if (g < M.nglobal) {
-      if (g < P.nsolve) {
-        const float *yb = Yb + (size_t)plane * M.nel * M.next;
-        for (int k = M.g2e_ptr[g]; k < M.g2e_ptr[g + 1]; k++) q += yb[M.g2e_idx[k]];
+  constexpr int UNR = 4;  // nodes per thread per pass, loads issued together
+  const int stride = gridDim.x * MX_ROWS;
+  for (int base = blockIdx.x * MX_ROWS + row; base < npts; base += stride * UNR) {
+    float qv[UNR], pv[UNR], dv[UNR], rv[UNR], cv[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      const int g = base + u * stride;
+      if (g < npts) {
+        const size_t o = (size_t)g * PP + p;
+        pv[u] = pcur[o];
+        dv[u] = d32[o];
+        rv[u] = r32[o];
+        cv[u] = P.pcf[(size_t)g * P.M + c];
+        qv[u] = (g >= M.nglobal) ? q32[o] : (g < ns ? dss_gather(M, Yb, g, PP, p) : 0.0f);
       }
-    } else {
-      q = q32[o + g];
     }
-    const float p = pcur[o + g];
-    const float d = d32[o + g] + alpha * p;
-    const float r = r32[o + g] - alpha * q;
-    r32[o + g] = r;
-    if (last)
-      x64[o + g] += (double)d;
-    else
-      d32[o + g] = d;
-    const float z = P.pcf[g] * r;
-    rz = (double)r * (double)z;
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      const int g = base + u * stride;
+      if (g < npts) {
+        const size_t o = (size_t)g * PP + p;
+        const float d = dv[u] + alpha * pv[u];
+        const float r = rv[u] - alpha * qv[u];
+        r32[o] = r;
+        if (last)
+          x64[o] += (double)d;
+        else
+          d32[o] = d;
+        const float z = cv[u] * r;
+        rz += (double)r * (double)z;
+      }
+    }
   }
-  reduce_pair(rz, 0.0, part, cnt, maxblk, gridDim.x, plane, blockIdx.x, &scal[plane].rho[(it + 1) & 1],
-              nullptr);
+  chunk_reduce2(rz, 0.0, part, cnt, gridDim.x, rho_next, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -300,17 +474,17 @@ __global__ void __launch_bounds__(256) k_mx_upd(MeshView M, const MxPlane *__res
 // ---------------------------------------------------------------------------
 
 template <int NP>
-__global__ void __launch_bounds__(128) k_mx_op64(MeshView M, const MxPlane *__restrict__ planes,
-                                                 const double *__restrict__ x64, double *__restrict__ Ye) {
+__global__ void __launch_bounds__(256) k_x_op64(MeshView M, MxParams P, const double *__restrict__ x64,
+                                                double *__restrict__ Ye) {
   constexpr int NN = NP * NP;
-  const MxPlane P = planes[blockIdx.y];
-  const int e = blockIdx.x, tid = threadIdx.x;
-  const int npts = M.nglobal + M.nel * M.nint;
-  const size_t o = (size_t)blockIdx.y * npts;
-  __shared__ double D[NN], Q[4][NN], u[NN], R[NN], S[NN], out[NN];
+  extern __shared__ __align__(16) double smx[];
+  double *U = smx, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
+  __shared__ double D[NN], Q[4][NN];
   __shared__ int emap[NN];
+  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 128) {
+  for (int i = tid; i < NN; i += 256) {
     D[i] = M.D[i];
     Q[0][i] = M.Q1[eo + i];
     Q[1][i] = M.Q2[eo + i];
@@ -319,68 +493,76 @@ __global__ void __launch_bounds__(128) k_mx_op64(MeshView M, const MxPlane *__re
     emap[i] = M.emap[i];
   }
   __syncthreads();
-  for (int a = tid; a < NN; a += 128) u[emap[a]] = x64[o + gidx(M, e, a)];
+  for (int a = row; a < NN; a += MX_ROWS) U[emap[a] * MX_CH + lane] = x64[(size_t)gidx(M, e, a) * PP + p];
   __syncthreads();
-  helm_op<NP, double>(D, Q[0], Q[1], Q[2], Q[3], M.hasQ3[e] != 0, P.hCon, u, R, S, out, 128);
-  double *y = Ye + ((size_t)blockIdx.y * M.nel + e) * NN;
-  for (int a = tid; a < NN; a += 128) y[a] = out[emap[a]];
+  op_stage1<NP, double>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
+  __syncthreads();
+  const double hc = P.hcon[p];
+  for (int a = row; a < NN; a += MX_ROWS)
+    Ye[ye_index(M, e, a, PP) + p] = op_stage2<NP, double>(D, Q[3], hc, U, R, S, emap[a]);
 }
 
 // r = b - A x (FP64), essential tail zero; restart the inner solve:
-// r32 = r, d = 0, p_0 = PC r; reduces ||r||^2 and rho_0.
-__global__ void __launch_bounds__(256) k_mx_res(MeshView M, const MxPlane *__restrict__ planes,
-                                                const double *__restrict__ Ye, const double *__restrict__ b64,
-                                                float *r32, float *d32, float *p0, MxScal *scal, double *part,
-                                                unsigned *cnt, int maxblk) {
-  const int plane = blockIdx.y;
-  const MxPlane P = planes[plane];
+// r32 = r, d = 0, p_0 = PC r; per-plane ||r||^2 and rho_0.
+__global__ void __launch_bounds__(256) k_x_res(MeshView M, MxParams P, const double *__restrict__ Ye,
+                                               const double *__restrict__ b64, float *r32, float *d32, float *p0,
+                                               double *r2, double *rho0, double *part, unsigned *cnt) {
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t o = (size_t)plane * npts;
+  const int ns = P.nsolve[p], c = pc_col(P, p);
   double rr = 0.0, rz = 0.0;
-  if (g < npts) {
+  for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
     double ax = 0.0;
     bool solve = true;
-    const double *y = Ye + (size_t)plane * M.nel * M.npnp;
     if (g < M.nglobal) {
-      solve = g < P.nsolve;
-      if (solve)
-        for (int q = M.g2e_ptr[g]; q < M.g2e_ptr[g + 1]; q++) {
-          const int ei = M.g2e_idx[q], e = ei / M.next, i = ei - e * M.next;
-          ax += y[(size_t)e * M.npnp + i];
-        }
+      solve = g < ns;
+      if (solve) ax = dss_gather(M, Ye, g, PP, p);
     } else {
-      const int r = g - M.nglobal, e = r / M.nint, i = r - e * M.nint;
-      ax = y[(size_t)e * M.npnp + M.next + i];
+      ax = Ye[((size_t)M.nel * M.next + (g - M.nglobal)) * PP + p];
     }
-    const double r = solve ? b64[o + g] - ax : 0.0;
+    const size_t o = (size_t)g * PP + p;
+    const double r = solve ? b64[o] - ax : 0.0;
     const float rf = (float)r;
-    r32[o + g] = rf;
-    d32[o + g] = 0.0f;
-    const float z = P.pcf[g] * rf;
-    p0[o + g] = z;
-    rr = r * r;
-    rz = (double)rf * (double)z;
+    r32[o] = rf;
+    d32[o] = 0.0f;
+    const float z = P.pcf[(size_t)g * P.M + c] * rf;
+    p0[o] = z;
+    rr += r * r;
+    rz += (double)rf * (double)z;
   }
-  reduce_pair(rr, rz, part, cnt, maxblk, gridDim.x, plane, blockIdx.x, &scal[plane].r2, &scal[plane].rho[0]);
+  chunk_reduce2(rr, rz, part, cnt, gridDim.x, r2, rho0);
 }
 
 // u = x at element nodes, essential values from gess (global2local +
-// setEssential, src/field.cpp:710-713, 1022-1040).
-__global__ void k_mx_unpack(MeshView M, const MxPlane *__restrict__ planes, const double *__restrict__ x64) {
-  const MxPlane P = planes[blockIdx.y];
-  const int e = blockIdx.x;
-  const int npts = M.nglobal + M.nel * M.nint;
-  const size_t o = (size_t)blockIdx.y * npts, eo = (size_t)e * M.npnp;
-  for (int a = threadIdx.x; a < M.npnp; a += blockDim.x) {
+// setEssential, src/field.cpp:710-713, 1022-1040); transposed back to the
+// caller's plane-major layout through shared memory.
+template <int NP>
+__global__ void __launch_bounds__(256) k_x_unpack(MeshView M, MxParams P, const double *__restrict__ x64) {
+  constexpr int NN = NP * NP, NE = 4 * (NP - 1);
+  __shared__ double V[NN * MX_CH];
+  __shared__ int emap[NN];
+  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  const int p0 = blockIdx.y * MX_CH, p = p0 + lane, PP = P.PP;
+  for (int i = tid; i < NN; i += 256) emap[i] = M.emap[i];
+  __syncthreads();
+  const bool masked = M.emask[e] != 0;
+  for (int a = row; a < NN; a += MX_ROWS) {
     double v;
-    if (a < M.next) {
-      const int g = M.btog[(size_t)e * M.next + a];
-      v = (M.emask[e] && M.bmask[(size_t)e * M.next + a]) ? P.gess[g] : x64[o + g];
+    if (a < NE) {
+      const int g = M.btog[(size_t)e * NE + a];
+      v = (masked && M.bmask[(size_t)e * NE + a]) ? P.gess[(size_t)p * M.nglobal + g] : x64[(size_t)g * PP + p];
     } else {
-      v = x64[o + M.nglobal + (size_t)e * M.nint + (a - M.next)];
+      v = x64[((size_t)M.nglobal + (size_t)e * M.nint + (a - NE)) * PP + p];
     }
-    P.u[eo + M.emap[a]] = v;
+    V[emap[a] * MX_CH + lane] = v;
+  }
+  __syncthreads();
+  for (int q = 0; q < MX_CH; q++) {
+    const int pl = p0 + q;
+    if (!real_plane(P, pl)) continue;
+    double *u = P.u + (size_t)pl * P.stride + (size_t)e * NN;
+    for (int k = tid; k < NN; k += 256) u[k] = V[k * MX_CH + q];
   }
 }
 
@@ -403,65 +585,77 @@ __global__ void k_mx_unpack(MeshView M, const MxPlane *__restrict__ planes, cons
     default: break;                                            \
   }
 
-static int reserve(const MeshView &M, MixedWork &W, int planes) {
-  const int npts = M.nglobal + M.nel * M.nint;
-  if (planes <= W.planes && npts == W.npts) return SX_OK;
-  const size_t n = (size_t)planes * npts;
-  SX_TRY(W.b64.alloc(n));
-  SX_TRY(W.x64.alloc(n));
-  SX_TRY(W.Ye64.alloc((size_t)planes * M.nel * M.npnp));
-  SX_TRY(W.r32.alloc(n));
-  SX_TRY(W.d32.alloc(n));
-  SX_TRY(W.pA.alloc(n));
-  SX_TRY(W.pB.alloc(n));
-  SX_TRY(W.q32.alloc(n));
-  SX_TRY(W.Yb32.alloc((size_t)planes * M.nel * M.next));
-  SX_TRY(W.scal.alloc(planes));
-  W.maxblk = std::max(M.nel, (npts + 255) / 256);
-  SX_TRY(W.partA.alloc((size_t)planes * W.maxblk * 2));
-  SX_TRY(W.cntA.alloc(planes));
-  SX_TRY(W.cntA.zero());
-  W.hscal.resize(planes);
-  W.planes = planes;
-  W.npts = npts;
+static int grid_nodes(int npts) {
+  // node-loop kernels: a fixed grid, up to 6 blocks of 8 node rows per SM,
+  // each thread taking 4 nodes per pass
+  return std::max(1, std::min((npts + 4 * MX_ROWS - 1) / (4 * MX_ROWS), 6 * 148));
+}
+
+template <int NP>
+static int set_smem_attrs() {
+  constexpr int NN = NP * NP;
+  SX_CUDA(cudaFuncSetAttribute(k_x_constrain<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(4 * NN * MX_CH * sizeof(double))));
+  SX_CUDA(cudaFuncSetAttribute(k_x_op64<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(3 * NN * MX_CH * sizeof(double))));
+  SX_CUDA(cudaFuncSetAttribute(k_x_op32<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(3 * NN * MX_CH * sizeof(float))));
   return SX_OK;
 }
 
-static int enqueue_init(const MeshView &M, MixedWork &W, int P, bool any_bc, cudaStream_t st, int *nl) {
-  const int npts = W.npts;
+struct Launch {
+  const MeshView &M;
+  MixedWork &W;
+  cudaStream_t st;
+  int chunks() const { return W.PP / MX_CH; }
+  MxScalPtrs sp() const {
+    double *s = W.scal.p;
+    const int PP = W.PP;
+    return {s, s + PP, s + 2 * PP, s + 3 * PP, s + 4 * PP, s + 5 * PP};
+  }
+};
+
+static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream_t st, int *nl) {
+  const int npts = W.npts, nch = W.PP / MX_CH, NN = M.npnp;
+  const MxParams P = W.prm;
+  const MxScalPtrs s = Launch{M, W, st}.sp();
   *nl = 0;
   if (any_bc) {
-    k_mx_ess<<<P, 32, 0, st>>>(M, W.dplanes.p);
+    k_x_ess<<<W.PP, 32, 0, st>>>(M, P);
     (*nl)++;
   }
-  SX_NP_SWITCH_M(M.np, (k_mx_constrain<N_><<<dim3(M.nel, P), 128, 0, st>>>(M, W.dplanes.p, W.Ye64.p)));
-  k_mx_rhs<<<dim3((npts + 255) / 256, P), 256, 0, st>>>(M, W.dplanes.p, W.Ye64.p, W.b64.p, W.x64.p, W.r32.p,
-                                                        W.d32.p, W.pA.p, W.scal.p, W.partA.p, W.cntA.p,
-                                                        W.maxblk);
+  const size_t sm64x4 = 4 * NN * MX_CH * sizeof(double);
+  SX_NP_SWITCH_M(M.np, (k_x_constrain<N_><<<dim3(M.nel, nch), 256, sm64x4, st>>>(M, P, W.Ye64.p)));
+  k_x_rhs<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.x64.p, W.r32.p, W.d32.p, W.pA.p, s.b2,
+                                          s.rho0, W.part.p, W.cnt.p);
   *nl += 2;
+  (void)npts;
   SX_CUDA(cudaGetLastError());
   return SX_OK;
 }
 
-static int enqueue_round(const MeshView &M, MixedWork &W, int P, int n_inner, cudaStream_t st, int *nl) {
-  const int npts = W.npts;
+static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStream_t st, int *nl) {
+  const int nch = W.PP / MX_CH, NN = M.npnp;
+  const MxParams P = W.prm;
+  const MxScalPtrs s = Launch{M, W, st}.sp();
+  double *rho[2] = {s.rho0, s.rho1}, *pq[2] = {s.pq0, s.pq1};
+  const size_t sm32 = 3 * NN * MX_CH * sizeof(float), sm64 = 3 * NN * MX_CH * sizeof(double);
   *nl = 0;
   for (int it = 0; it < n_inner; it++) {
-    float *pold = (it & 1) ? W.pA.p : W.pB.p;  // p_{it-1} lives in buffer (it-1)&1
-    float *pcur = (it & 1) ? W.pB.p : W.pA.p;  // p_it in buffer it&1
-    if (it == 0) pold = W.pA.p;                // p_0 written by the restart
-    SX_NP_SWITCH_M(M.np, (k_mx_op32<N_><<<dim3(M.nel, P), 128, 0, st>>>(
-                             M, W.dplanes.p, W.r32.p, pold, pcur, W.q32.p, W.Yb32.p, W.scal.p, it, W.partA.p,
-                             W.cntA.p, W.maxblk)));
-    k_mx_upd<<<dim3((npts + 255) / 256, P), 256, 0, st>>>(M, W.dplanes.p, pcur, W.q32.p, W.Yb32.p, W.d32.p,
-                                                          W.r32.p, W.x64.p, W.scal.p, it,
-                                                          it == n_inner - 1 ? 1 : 0, W.partA.p, W.cntA.p,
-                                                          W.maxblk);
+    // p_it lives in buffer it&1 (p_0 written by the restart into pA)
+    float *pold = (it == 0) ? W.pA.p : ((it & 1) ? W.pA.p : W.pB.p);
+    float *pcur = (it & 1) ? W.pB.p : W.pA.p;
+    SX_NP_SWITCH_M(M.np, (k_x_op32<N_><<<dim3(M.nel, nch), 256, sm32, st>>>(
+                             M, P, W.r32.p, pold, pcur, W.q32.p, W.Yb32.p, rho[it & 1], rho[(it + 1) & 1],
+                             pq[it & 1], it, W.part.p, W.cnt.p)));
+    k_x_upd<<<dim3(W.G, nch), 256, 0, st>>>(M, P, pcur, W.q32.p, W.Yb32.p, W.d32.p, W.r32.p, W.x64.p,
+                                            rho[it & 1], pq[it & 1], rho[(it + 1) & 1],
+                                            it == n_inner - 1 ? 1 : 0, W.part.p, W.cnt.p);
     *nl += 2;
   }
-  SX_NP_SWITCH_M(M.np, (k_mx_op64<N_><<<dim3(M.nel, P), 128, 0, st>>>(M, W.dplanes.p, W.x64.p, W.Ye64.p)));
-  k_mx_res<<<dim3((npts + 255) / 256, P), 256, 0, st>>>(M, W.dplanes.p, W.Ye64.p, W.b64.p, W.r32.p, W.d32.p,
-                                                        W.pA.p, W.scal.p, W.partA.p, W.cntA.p, W.maxblk);
+  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<dim3(M.nel, nch), 256, sm64, st>>>(M, P, W.x64.p, W.Ye64.p)));
+  k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r32.p, W.d32.p, W.pA.p, s.r2, s.rho0,
+                                          W.part.p, W.cnt.p);
   *nl += 2;
   SX_CUDA(cudaGetLastError());
   return SX_OK;
@@ -483,40 +677,129 @@ static int capture(cudaStream_t st, cudaGraphExec_t *out, const std::function<in
   return SX_OK;
 }
 
-int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxPlane> &planes, bool rebuild,
-                double tol_rel, int max_refine, int n_inner, cudaStream_t st, sx_solve_stats *stats) {
-  const int P = (int)planes.size();
-  if (P == 0) return SX_OK;
+// Interleaved preconditioner PCi[g*M + m] from the per-mode systems.
+__global__ void k_x_pc(int npts, int M, const float *const *pcs, float *out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= npts) return;
+  for (int m = 0; m < M; m++) out[(size_t)g * M + m] = pcs[m][g];
+}
+
+static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int nyq,
+                 int num_modes, cudaStream_t st) {
+  const int npts = M.nglobal + M.nel * M.nint;
+  const int PP = ((nz + MX_CH - 1) / MX_CH) * MX_CH;
+  const int Mc = std::max(1, num_modes);
+  {
+    // grow-only: a workspace is reused across solves of different sizes
+    auto need = [](auto &b, size_t n) { return b.n < n ? b.alloc(n) : SX_OK; };
+    const size_t n = (size_t)PP * npts;
+    W.G = grid_nodes(npts);
+    SX_TRY(need(W.b64, n));
+    SX_TRY(need(W.x64, n));
+    SX_TRY(need(W.Ye64, (size_t)PP * M.nel * M.npnp));
+    SX_TRY(need(W.r32, n));
+    SX_TRY(need(W.d32, n));
+    SX_TRY(need(W.pA, n));
+    SX_TRY(need(W.pB, n));
+    SX_TRY(need(W.q32, n));
+    SX_TRY(need(W.Yb32, (size_t)PP * M.nel * M.next));
+    SX_TRY(need(W.scal, (size_t)6 * PP));
+    SX_TRY(need(W.hcon, (size_t)PP));
+    SX_TRY(need(W.gess, (size_t)PP * M.nglobal));
+    SX_TRY(need(W.nsolve, (size_t)PP));
+    SX_TRY(need(W.pcf, (size_t)npts * Mc));
+    SX_TRY(need(W.part, (size_t)PP * std::max(W.G, M.nel) * 2));
+    if (W.cnt.n < (size_t)(PP / MX_CH)) {
+      SX_TRY(W.cnt.alloc(PP / MX_CH));
+      SX_TRY(W.cnt.zero(st));
+    }
+    W.hscal.assign((size_t)6 * PP, 0.0);
+    W.PP = PP;
+    W.npts = npts;
+    W.M = Mc;
+  }
+  // per-plane constants; planes without a system (Nyquist, padding) borrow
+  // the first group's
+  std::vector<double> hc(PP, groups[0].sys->betak2 + groups[0].sys->lambda2);
+  std::vector<int> ns(PP, groups[0].sys->nsolve);
+  std::vector<const float *> pcs(Mc, groups[0].sys->pcf.p);
+  for (const MxGroup &g : groups) {
+    for (int q = 0; q < g.P; q++) {
+      hc[g.plane0 + q] = g.sys->betak2 + g.sys->lambda2;
+      ns[g.plane0 + q] = g.sys->nsolve;
+    }
+    if (g.mode < Mc) pcs[g.mode] = g.sys->pcf.p;
+  }
+  SX_CUDA(cudaMemcpyAsync(W.hcon.p, hc.data(), sizeof(double) * PP, cudaMemcpyHostToDevice, st));
+  SX_CUDA(cudaMemcpyAsync(W.nsolve.p, ns.data(), sizeof(int) * PP, cudaMemcpyHostToDevice, st));
+  DBuf<const float *> dp;
+  SX_TRY(dp.upload_on(pcs.data(), pcs.size(), st));
+  k_x_pc<<<(npts + 255) / 256, 256, 0, st>>>(npts, Mc, dp.p, W.pcf.p);
+  SX_CUDA(cudaGetLastError());
+  SX_CUDA(cudaStreamSynchronize(st));
+  (void)nyq;
+  return SX_OK;
+}
+
+int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int nyq,
+                int num_modes, double *d_u, double *d_f, const double *d_bc, long long stride,
+                bool rebuild, double tol_rel, int max_refine, int n_inner, bool graphs, cudaStream_t st,
+                sx_solve_stats *stats) {
+  if (groups.empty()) return SX_OK;
   if (M.mixed) {
     set_error("mixed-precision form does not take Robin (mixed) boundary conditions");
     return SX_ERR_UNSUPPORTED;
   }
-  SX_TRY(reserve(M, W, P));
-  bool any_bc = false;
-  for (const MxPlane &p : planes) any_bc |= p.bc != nullptr;
-  if (rebuild || !W.g_init || W.n_inner != n_inner) {
+  SX_TRY(ensure_constD());
+  if (rebuild || !graphs || !W.g_init || W.n_inner != n_inner) {
     if (W.g_init) cudaGraphExecDestroy(W.g_init);
     if (W.g_round) cudaGraphExecDestroy(W.g_round);
     W.g_init = W.g_round = nullptr;
-    if (W.dplanes.n < (size_t)P) SX_TRY(W.dplanes.alloc(P));
-    SX_CUDA(cudaMemcpy(W.dplanes.p, planes.data(), sizeof(MxPlane) * P, cudaMemcpyHostToDevice));
-    SX_TRY(capture(st, &W.g_init, [&]() { return enqueue_init(M, W, P, any_bc, st, &W.launches_init); }));
-    SX_TRY(capture(st, &W.g_round, [&]() { return enqueue_round(M, W, P, n_inner, st, &W.launches_round); }));
+    SX_TRY(setup(M, W, groups, nz, nyq, num_modes, st));
+    int attr_rc = SX_OK;
+    SX_NP_SWITCH_M(M.np, (attr_rc = set_smem_attrs<N_>()));
+    SX_TRY(attr_rc);
+    MxParams &P = W.prm;
+    P.PP = W.PP;
+    P.nz = nz;
+    P.nyq = nyq;
+    P.M = W.M;
+    P.hcon = W.hcon.p;
+    P.nsolve = W.nsolve.p;
+    P.pcf = W.pcf.p;
+    P.f = d_f;
+    P.u = d_u;
+    P.stride = stride;
+    P.bc = d_bc;
+    P.bcstride = (long long)std::max(M.nbound, 1) * M.np;
+    P.gess = W.gess.p;
+    if (graphs) {
+      const bool any_bc = d_bc != nullptr;
+      SX_TRY(capture(st, &W.g_init, [&]() { return enqueue_init(M, W, any_bc, st, &W.launches_init); }));
+      SX_TRY(capture(st, &W.g_round, [&]() { return enqueue_round(M, W, n_inner, st, &W.launches_round); }));
+    }
     W.n_inner = n_inner;
   }
-  // essential values: zeroed, then set from the BC lines inside g_init
-  for (const MxPlane &p : planes) SX_CUDA(cudaMemsetAsync(p.gess, 0, sizeof(double) * M.nglobal, st));
-  SX_CUDA(cudaGraphLaunch(W.g_init, st));
-  int rounds = 0, launches = W.launches_init;
+  // essential values: zeroed here, set from the BC lines inside g_init
+  SX_CUDA(cudaMemsetAsync(W.gess.p, 0, sizeof(double) * (size_t)W.PP * M.nglobal, st));
+  if (graphs)
+    SX_CUDA(cudaGraphLaunch(W.g_init, st));
+  else
+    SX_TRY(enqueue_init(M, W, d_bc != nullptr, st, &W.launches_init));
+  int rounds = 0, launches = W.launches_init + 1;
   double worst = 0.0;
+  const int PP = W.PP;
   for (rounds = 1; rounds <= max_refine; rounds++) {
-    SX_CUDA(cudaGraphLaunch(W.g_round, st));
+    if (graphs)
+      SX_CUDA(cudaGraphLaunch(W.g_round, st));
+    else
+      SX_TRY(enqueue_round(M, W, n_inner, st, &W.launches_round));
     launches += W.launches_round;
-    SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(MxScal) * P, cudaMemcpyDeviceToHost, st));
+    SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(double) * 6 * PP, cudaMemcpyDeviceToHost, st));
     SX_CUDA(cudaStreamSynchronize(st));
     worst = 0.0;
-    for (int i = 0; i < P; i++) {
-      const double b2 = W.hscal[i].b2, r2 = W.hscal[i].r2;
+    for (int p = 0; p < PP; p++) {
+      const double r2 = W.hscal[4 * PP + p], b2 = W.hscal[5 * PP + p];
       const double rel = b2 > 0.0 ? std::sqrt(std::max(r2, 0.0) / b2) : 0.0;
       if (!(rel == rel)) worst = INFINITY;  // NaN
       worst = std::max(worst, rel);
@@ -524,15 +807,16 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxPlane> &pla
     if (worst <= tol_rel) break;
   }
   if (rounds > max_refine) rounds = max_refine;
-  k_mx_unpack<<<dim3(M.nel, P), 128, 0, st>>>(M, W.dplanes.p, W.x64.p);
-  launches += 1;
+  SX_NP_SWITCH_M(M.np, (k_x_unpack<N_><<<dim3(M.nel, PP / MX_CH), 256, 0, st>>>(M, W.prm, W.x64.p)));
   SX_CUDA(cudaGetLastError());
+  int solved = 0;
+  for (const MxGroup &g : groups) solved += g.P;
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
-    stats->planes_solved = P;
+    stats->planes_solved = solved;
     stats->refinements = rounds;
     stats->iterations_max = rounds * n_inner;
-    stats->iterations_total = rounds * n_inner * P;
+    stats->iterations_total = rounds * n_inner * solved;
     stats->final_rel_residual = worst;
     stats->kernel_launches = launches;
   }

@@ -1,0 +1,97 @@
+"""GPU tests of the serving loop (sx_server_*).
+
+* Requests of different meshes, orders and mode counts, submitted together
+  and run concurrently, give bitwise the same results as each solved alone
+  through ModalMatrixSys.solve_batched_host (same kernels, same schedule).
+* Results match the oracle's FP64 direct solve within 1e-10.
+* Geometry and systems are reused across requests (cache hits).
+* A request larger than the memory budget is refused with SX_ERR_CAPACITY.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def sx():
+    import semtex_b200
+    return semtex_b200
+
+
+def _requests():
+    from semtex_b200.mesh import rect_mesh
+    from semtex_b200.workloads import fourier_forcing
+    rng = np.random.default_rng(42)
+    out = []
+    for i, (nx, ny, np_, nm, lam) in enumerate([(3, 3, 5, 2, 1e3), (4, 2, 7, 1, 50.0),
+                                                (5, 4, 6, 3, 1e4), (2, 2, 9, 2, 300.0),
+                                                (3, 3, 5, 2, 1e3), (6, 3, 8, 4, 2e3)]):
+        m = rect_mesh(nx, ny, np_, 0.0, 1.0 + 0.1 * i, 0.0, 1.0)
+        nz = 1 if nm == 1 else 2 * nm
+        lamv = np.full(nm, lam)
+        bk2 = np.arange(nm, dtype=np.float64) ** 2
+        out.append((m, lamv, bk2, fourier_forcing(m, nz, rng)))
+    return out
+
+
+def _alone(sx, m, lam, bk2, f):
+    S = sx.ModalMatrixSys(sx.Mesh(m), num_modes=len(lam), method=sx.JACPCG, lambda2_modes=lam,
+                          betak2_modes=bk2)
+    return S.solve_batched_host(f, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30)
+
+
+def test_mix_equals_alone_and_oracle(sx):
+    reqs = _requests()
+    alone = [_alone(sx, *r) for r in reqs]
+    srv = sx.Server(slots=3, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30, inner_iters=12)
+    try:
+        ids = [srv.submit(*r) for r in reqs]
+        res = [srv.wait(i, timeout_s=120.0) for i in ids]
+        stats = srv.stats()
+    finally:
+        srv.close()
+    for (status, lat, u), a in zip(res, alone):
+        assert status in (sx.OK, sx.WARN_STEP_LIMIT)
+        assert lat > 0.0
+        assert np.array_equal(u, a)
+    assert stats["completed"] == len(reqs)
+    assert stats["mesh_hits"] >= 1          # requests 0 and 4 share a mesh
+    assert stats["p99_ms"] >= stats["p50_ms"] > 0.0
+    # one request against the oracle
+    from oracle.oracle import OracleMesh, solve_planes
+    m, lam, bk2, f = reqs[2]
+    uo, _ = solve_planes(OracleMesh(m), 0.0, 1.0, f, None, lambda2_per_mode=lam)
+    sp = [0] + list(range(2, f.shape[0]))
+    u = res[2][2]
+    assert np.linalg.norm(u[sp] - uo[sp]) <= TOL * np.linalg.norm(uo[sp])
+
+
+def test_fp64_direct_server_matches_oracle(sx):
+    reqs = _requests()[:3]
+    srv = sx.Server(slots=2, precision=sx.FP64)
+    try:
+        ids = [srv.submit(*r) for r in reqs]
+        res = [srv.wait(i, timeout_s=120.0) for i in ids]
+    finally:
+        srv.close()
+    from oracle.oracle import OracleMesh, solve_planes
+    for (m, lam, bk2, f), (status, _, u) in zip(reqs, res):
+        assert status == sx.OK
+        uo, _ = solve_planes(OracleMesh(m), 0.0, 1.0, f, None, lambda2_per_mode=lam)
+        sp = [0] + list(range(2, f.shape[0])) if f.shape[0] > 1 else [0]
+        assert np.linalg.norm(u[sp] - uo[sp]) <= 1e-12 * np.linalg.norm(uo[sp])
+
+
+def test_capacity_rejection(sx):
+    m, lam, bk2, f = _requests()[5]
+    srv = sx.Server(slots=1, hbm_budget=1 << 16)
+    try:
+        with pytest.raises(sx.SolverError) as ei:
+            srv.submit(m, lam, bk2, f)
+        assert ei.value.status == 11  # SX_ERR_CAPACITY
+        assert srv.stats()["rejected"] == 1
+    finally:
+        srv.close()
