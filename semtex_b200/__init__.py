@@ -266,7 +266,7 @@ class ModalMatrixSys:
         qm = self.mesh.qm
         f = np.ascontiguousarray(forcing, dtype=np.float64)
         nz = f.shape[0]
-        u = out if out is not None else np.empty_like(f)
+        u = out if out is not None else np.zeros_like(f)  # the Nyquist plane is left as passed
         b = self._bc_array(bc, nz)
         st = SolveStats()
         rc = lib.sx_field_solve_batched_host(self.h, _dptr(u), _dptr(f),

@@ -502,9 +502,23 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
   const int rc = solve_batched_on(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride, precision,
                                   tol_rel, max_refine, st, stats);
   if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
-  SX_CUDA(cudaMemcpyAsync(u, s->hu.p, n * 8, cudaMemcpyDeviceToHost, st));
+  SX_TRY(copy_solved_planes(u, s->hu.p, nz, plane_stride, s->base_mode, st));
   SX_TRY(take_status(s, true, st, false));
   return rc;
+}
+
+int sx::copy_solved_planes(double *h_u, const double *d_u, int nz, int plane_stride, int base_mode,
+                           cudaStream_t st) {
+  const size_t ps = (size_t)plane_stride;
+  if (nz > 1 && base_mode == 0) {
+    SX_CUDA(cudaMemcpyAsync(h_u, d_u, ps * 8, cudaMemcpyDeviceToHost, st));
+    if (nz > 2)
+      SX_CUDA(cudaMemcpyAsync(h_u + 2 * ps, d_u + 2 * ps, (size_t)(nz - 2) * ps * 8, cudaMemcpyDeviceToHost,
+                              st));
+  } else {
+    SX_CUDA(cudaMemcpyAsync(h_u, d_u, (size_t)nz * ps * 8, cudaMemcpyDeviceToHost, st));
+  }
+  return SX_OK;
 }
 
 extern "C" int sx_profile_band_sweeps(sx_modal s, int reps, void *stream) {

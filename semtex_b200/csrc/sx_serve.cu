@@ -272,11 +272,15 @@ int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &d
     SX_TRY(ws.dstatus.zero(stream));
   }
   sx_solve_stats sst{};
-  const int rc = solve_batched_on(&ws, du.p, df.p, r->bc.empty() ? nullptr : dbc.p, r->nz, r->stride,
-                                  cfg.precision, cfg.tol_rel, cfg.max_refine, stream, &sst);
+  int rc = solve_batched_on(&ws, du.p, df.p, r->bc.empty() ? nullptr : dbc.p, r->nz, r->stride,
+                            cfg.precision, cfg.tol_rel, cfg.max_refine, stream, &sst);
   if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
-    SX_CUDA(cudaMemcpyAsync(r->u, du.p, n * 8, cudaMemcpyDeviceToHost, stream));
-    SX_CUDA(cudaStreamSynchronize(stream));
+    int c = copy_solved_planes(r->u, du.p, r->nz, r->stride, r->base_mode, stream);
+    if (c == SX_OK && cudaStreamSynchronize(stream) != cudaSuccess) {
+      set_error("serving: device -> host copy of a result failed");
+      c = SX_ERR_CUDA;
+    }
+    if (c != SX_OK) rc = c;
   }
   {
     std::lock_guard<std::mutex> lk(mu);
