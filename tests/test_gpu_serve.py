@@ -29,7 +29,7 @@ def _requests():
     for i, (nx, ny, np_, nm, lam) in enumerate([(3, 3, 5, 2, 1e3), (4, 2, 7, 1, 50.0),
                                                 (5, 4, 6, 3, 1e4), (2, 2, 9, 2, 300.0),
                                                 (3, 3, 5, 2, 1e3), (6, 3, 8, 4, 2e3)]):
-        m = rect_mesh(nx, ny, np_, 0.0, 1.0 + 0.1 * i, 0.0, 1.0)
+        m = rect_mesh(nx, ny, np_, 0.0, 1.0 + 0.1 * (i % 4), 0.0, 1.0)  # 0 and 4: one mesh
         nz = 1 if nm == 1 else 2 * nm
         lamv = np.full(nm, lam)
         bk2 = np.arange(nm, dtype=np.float64) ** 2
@@ -60,6 +60,7 @@ def test_mix_equals_alone_and_oracle(sx):
         assert not bad, f"planes {bad} differ (max {np.max(np.abs(u - a)):.3e})"
     assert stats["completed"] == len(reqs)
     assert stats["mesh_hits"] >= 1          # requests 0 and 4 share a mesh
+    assert stats["system_hits"] >= 2        # ... and both of their systems
     assert stats["p99_ms"] >= stats["p50_ms"] > 0.0
     # one request against the oracle
     from oracle.oracle import OracleMesh, solve_planes
