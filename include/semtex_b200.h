@@ -155,6 +155,27 @@ SX_API int sx_field_solve_device(sx_modal modal, double *d_u, double *d_f, const
                           int plane_stride, double tol_rel, int step_max, void *stream,
                           sx_solve_stats *stats);
 
+/* ---- no-allocation direct solve (no reference counterpart) ---------------
+ * sx_field_solve_device on DIRECT systems, with its per-call scratch (job
+ * record, condensed right-hand sides, element boundary forcing, essential
+ * values) in one file-scope device array of SX_STATIC_SCRATCH_BYTES instead
+ * of the modal system's grow-only workspace: no cudaMalloc, cudaFree or other
+ * device allocation in any call.  For callers that cannot allocate: loops
+ * whose device memory is already held by another allocator (cudaMalloc would
+ * fail) and latency-bound loops (cudaFree synchronises the device).
+ *   - The first call on each device looks up the array's address with
+ *     cudaGetSymbolAddress (with that device current), which can load the
+ *     module; make that first call before any stream capture.
+ *   - SX_ERR_CAPACITY when one mode needs more than SX_STATIC_SCRATCH_BYTES
+ *     (sx_last_error() gives the bytes needed); SX_ERR_UNSUPPORTED when a
+ *     mode's system is not DIRECT.
+ *   - The array is shared by all calls on a device: calls that overlap in
+ *     time (two threads or two streams) race on it; serialise them.
+ *   - Results equal sx_field_solve_device's bit for bit (same kernels). */
+#define SX_STATIC_SCRATCH_BYTES (4u << 20)
+SX_API int sx_field_solve_device_static(sx_modal modal, double *d_u, double *d_f, const double *d_bc, int nz,
+                                        int plane_stride, void *stream, sx_solve_stats *stats);
+
 /* ---- batched form (no reference counterpart: extends Field::solve) --------
  * All modes of the system in one captured CUDA graph, every mode's planes
  * processed together.  precision = SX_FP64 (same answer as the plain form

@@ -30,6 +30,7 @@ DIRECT, JACPCG, MIXED_SOLVER = 0, 1, 2
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
 TUNE_INNER_ITERS, TUNE_BAND_CLUSTER = 1, 2
+STATIC_SCRATCH_BYTES = 4 << 20  # SX_STATIC_SCRATCH_BYTES
 
 
 class SolverError(RuntimeError):
@@ -104,6 +105,7 @@ def _load():
     L.sx_modal_band.argtypes = [vp, ip, P(dp), P(ip), P(ip)]
     L.sx_field_solve.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, dp, ip, P(SolveStats)]
     L.sx_field_solve_device.argtypes = [vp, vp, vp, vp, ip, ip, dp, ip, vp, P(SolveStats)]
+    L.sx_field_solve_device_static.argtypes = [vp, vp, vp, vp, ip, ip, vp, P(SolveStats)]
     L.sx_field_solve_batched.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(SolveStats)]
     L.sx_field_solve_batched_host.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, ip, dp, ip,
                                               P(SolveStats)]
@@ -249,6 +251,15 @@ class ModalMatrixSys:
         rc = lib.sx_field_solve_device(self.h, d_u, d_f, d_bc, nz, stride, tol_rel, step_max,
                                        stream, C.byref(st))
         _check(rc, "sx_field_solve_device", allow=(OK, WARN_STEP_LIMIT))
+        return st.as_dict()
+
+    def solve_device_static(self, d_u, d_f, d_bc, nz, stride, stream=0):
+        """solve_device for DIRECT systems with no device allocation: scratch
+        is a fixed device array of STATIC_SCRATCH_BYTES shared by all calls
+        on a device (overlapping calls race; serialise them)."""
+        st = SolveStats()
+        rc = lib.sx_field_solve_device_static(self.h, d_u, d_f, d_bc, nz, stride, stream, C.byref(st))
+        _check(rc, "sx_field_solve_device_static")
         return st.as_dict()
 
     def solve_batched(self, d_u, d_f, d_bc, nz, stride, precision=FP64, tol_rel=1e-12,
