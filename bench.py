@@ -183,6 +183,23 @@ def rel_err(a, b):
             float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)))
 
 
+def _ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload, from
+    the committed ncu summary profiles/<kernel>_*.md (its line
+    `dram_bytes_per_launch: N`); None when there is none."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for name in sorted(os.listdir(d)):
+        if not (name.startswith(kernel + "_") and name.endswith(".md")):
+            continue
+        with open(os.path.join(d, name)) as fh:
+            for line in fh:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1].strip().split()[0])
+    return None
+
+
 def run_ours(args, rank, world):
     import torch
     import semtex_b200 as sx
@@ -216,29 +233,36 @@ def run_ours(args, rank, world):
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
 
+    def restore():
+        f_work.copy_(f_src)  # the solve overwrites its forcing (src/field.cpp:525-526)
+
     def step_batched():
-        f_work.copy_(f_src)
         S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride, sx.FP64, stream=sptr)
 
     def step_plain():
-        f_work.copy_(f_src)
         S.solve_device(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride, stream=sptr)
+
+    # 256 MB written between timed steps: evicts the 126 MB L2
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
 
     def timed(fn, k, wu):
         for _ in range(wu):
+            restore()
             fn()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        for e0, e1 in ev:
+            restore()
+            flush.zero_()
+            e0.record(stream)
             fn()
-        e1.record(stream)
+            e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / k
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / k
         if dist is not None:
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -246,31 +270,34 @@ def run_ours(args, rank, world):
         return ms
 
     # plain FP64, mode by mode (reference-compatible form)
+    restore()
     step_plain()
     torch.cuda.synchronize()
     u_plain = u_dev.cpu().numpy().copy()
     ms_plain = timed(step_plain, max(1, min(args.steps, 3)), 1)
 
-    # batched FP64 (headline for now)
+    # batched FP64
     clk = ClockSampler(dev.index)
+    restore()
     step_batched()
     torch.cuda.synchronize()
     u_batched = u_dev.cpu().numpy().copy()
     clk.start()
     ms_batched = timed(step_batched, args.steps, args.warmup)
 
+    restore()
     st_b = S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride, sx.FP64, stream=sptr)
     launches_fp64 = int(st_b["kernel_launches"])
 
-    # batched mixed precision: FP32 PCG inner iterations, FP64 refinement
+    # batched mixed precision: FP32 CG inner iterations, FP64 refinement
     mixed_stats = {}
 
     def step_mixed():
-        f_work.copy_(f_src)
         mixed_stats.update(S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride,
                                            sx.MIXED_FP32, tol_rel=args.tol, max_refine=20,
                                            stream=sptr))
 
+    restore()
     step_mixed()
     torch.cuda.synchronize()
     u_mixed = u_dev.cpu().numpy().copy()
@@ -289,29 +316,51 @@ def run_ours(args, rank, world):
     ms_head = ms_mixed if use_mixed else ms_batched
     launches_per_step = int(mixed_stats.get("kernel_launches", 0)) if use_mixed else launches_fp64
 
-    # dominant kernel: the banded sweeps, timed on their own stream
+    def kernel_ms(replay, reps):
+        """Average duration of one replayed launch, CUDA events on its stream."""
+        replay(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        replay(reps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    hbm, peak_kind = _peaks()
     reps = max(3, args.steps)
-    S.profile_band_sweeps(1, sptr)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    S.profile_band_sweeps(reps, sptr)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    sweep_ms = e0.elapsed_time(e1) / reps
-    # algorithmic bytes per launch: the band factor read by each sweep
-    # (forward and backward) + each sweep's RHS read and write
+    # batched FP64's dominant kernel: the banded sweeps.  Algorithmic bytes
+    # per launch: the band factor read by each sweep (forward and backward)
+    # + each sweep's RHS read and write.
+    restore()
+    S.solve_batched(u_dev.data_ptr(), f_work.data_ptr(), 0, nz, stride, sx.FP64, stream=sptr)
+    sweep_ms = kernel_ms(lambda r: S.profile_band_sweeps(r, sptr), reps)
     band_bytes = 0
     for mode in range(nmodes):
         P = 1 if (base + mode) == 0 else 2
         band_bytes += 2 * m.nsolve * m.nband * 8 + 2 * 2 * P * m.nsolve * 8
-    hbm, peak_kind = _peaks()
-    achieved = band_bytes / (sweep_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_band_sweep", "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_launch": band_bytes,
-                "launch_ms": sweep_ms}
+    band_gbs = band_bytes / (sweep_ms * 1e-3) / 1e9
+    roof_band = {"bound": "hbm", "kernel": "k_band_sweep", "achieved": band_gbs, "peak": hbm,
+                 "unit": "GB/s", "frac": band_gbs / hbm, "peak_kind": peak_kind,
+                 "traffic": _ncu_traffic("k_band_sweep"), "algorithmic_bytes_per_launch": band_bytes,
+                 "launch_ms": sweep_ms}
+    # the mixed form's dominant kernel: one fused FP32 CG iteration (k_cg)
+    # over every plane.  Algorithmic bytes per launch: r, s, p, d read and
+    # written at every node, A u (element boundary slots + interior nodes)
+    # read and written, per plane solved; + the preconditioner columns and the
+    # FP32 geometry read once.
+    restore()
+    step_mixed()
+    cg_ms = kernel_ms(lambda r: S.profile_mixed_iterations(r, sptr), reps)
+    nn = m.np * m.np
+    npts = m.nglobal + m.nel * (m.np - 2) ** 2
+    cg_bytes = 4 * planes_solved * (8 * npts + 2 * m.nel * nn) + 4 * npts * nmodes + 16 * m.nel * nn
+    cg_gbs = cg_bytes / (cg_ms * 1e-3) / 1e9
+    roof_cg = {"bound": "hbm", "kernel": "k_cg", "achieved": cg_gbs, "peak": hbm, "unit": "GB/s",
+               "frac": cg_gbs / hbm, "peak_kind": peak_kind, "traffic": _ncu_traffic("k_cg"),
+               "algorithmic_bytes_per_launch": cg_bytes, "launch_ms": cg_ms}
+    roofline = roof_cg if use_mixed else roof_band
 
     # end to end through the host-pointer C-ABI call, pinned buffers
     f_host = torch.tensor(w.forcing).pin_memory()
@@ -356,6 +405,7 @@ def run_ours(args, rank, world):
         "speedup_mixed_vs_plain": ms_plain / ms_mixed,
         "setup_s": setup_s,
         "roofline": roofline,
+        "roofline_other_form": roof_band if use_mixed else roof_cg,
         "e2e": {"value": total_dofs / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": int(fh.nbytes), "d2h_bytes_per_step": int(uh.nbytes),
                 "ms_per_step": e2e_s * 1e3, "call": "sx_field_solve_batched_host (pinned)"},

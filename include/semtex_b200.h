@@ -53,8 +53,11 @@ enum {
   SX_ERR_NOT_FOUND = 12     /* serving: unknown request id                        */
 };
 
-/* Solver kinds: femlib/cfemdef.h:43-47 (SolverKind). */
-enum { SX_DIRECT = 0, SX_JACPCG = 1, SX_MIXED = 2 };
+/* Solver kinds: femlib/cfemdef.h:43-47 (SolverKind).  SX_AUTO has no
+ * reference counterpart: each mode is DIRECT when the band Cholesky streams
+ * fewer bytes than Jacobi-PCG would for its conditioning (the routing rule
+ * of SX_TUNE_MIXED_ROUTE), JACPCG otherwise. */
+enum { SX_DIRECT = 0, SX_JACPCG = 1, SX_MIXED = 2, SX_AUTO = 3 };
 
 /* Boundary-condition kinds (src/condition.h: Essential, Natural, Mixed). */
 enum { SX_BC_ESSENTIAL = 0, SX_BC_NATURAL = 1, SX_BC_MIXED = 2 };
@@ -94,6 +97,7 @@ typedef struct {
   int refinements;      /* mixed precision: outer refinement steps taken        */
   double final_rel_residual; /* mixed precision / PCG: max ||r||/||b||          */
   int kernel_launches;  /* kernels this call enqueued (graph nodes included)    */
+  int planes_direct;    /* mixed precision: planes routed to the FP64 band solve */
 } sx_solve_stats;
 
 /* ---- library ------------------------------------------------------------ */
@@ -195,8 +199,14 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
 /* Schedule knobs of the batched forms (no reference counterpart), set by
  * the autotuner or by hand; value <= 0 restores the default.
  *   SX_TUNE_INNER_ITERS   FP32 PCG iterations per refinement round (12)
- *   SX_TUNE_BAND_CLUSTER  CTAs per cluster in the band sweeps (auto)     */
-enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2 };
+ *   SX_TUNE_BAND_CLUSTER  CTAs per cluster in the band sweeps (auto)
+ *   SX_TUNE_MIXED_ROUTE   how SX_MIXED_FP32 solves each mode: 0 = by cost
+ *                         (default: modes whose Jacobi-CG would stream more
+ *                         bytes than three band solves go to the FP64 band
+ *                         Cholesky, when the mode is factored), 1 = FP32 CG
+ *                         for every mode, 2 = band Cholesky for every
+ *                         factored mode                                   */
+enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3 };
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 
 /* Profiling hook (no reference counterpart): re-launch only the banded
@@ -204,6 +214,11 @@ SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
  * `stream`, so the dominant kernel can be timed on its own.  The RHS
  * workspace is overwritten; call after sx_field_solve_batched. */
 SX_API int sx_profile_band_sweeps(sx_modal modal, int reps, void *stream);
+/* Same for the mixed-precision form: `reps` launches of one inner FP32
+ * iteration (the fused k_cg kernel) on the workspace of the last mixed
+ * solve (which needs >= 2 inner iterations).  The iterates are overwritten;
+ * the next solve starts afresh. */
+SX_API int sx_profile_mixed_iterations(sx_modal modal, int reps, void *stream);
 
 /* ---- serving loop (no reference counterpart) -----------------------------
  * A request loop for Helmholtz solves of different meshes, orders and mode

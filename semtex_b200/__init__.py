@@ -26,10 +26,11 @@ from .mesh import (ESSENTIAL, MIXED, NATURAL, Boundary, QuadMesh, gll_points,  #
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsemtex_b200.so")
 
-DIRECT, JACPCG, MIXED_SOLVER = 0, 1, 2
+DIRECT, JACPCG, MIXED_SOLVER, AUTO = 0, 1, 2, 3
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
-TUNE_INNER_ITERS, TUNE_BAND_CLUSTER = 1, 2
+TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE = 1, 2, 3
+ROUTE_AUTO, ROUTE_CG, ROUTE_BAND = 0, 1, 2
 STATIC_SCRATCH_BYTES = 4 << 20  # SX_STATIC_SCRATCH_BYTES
 
 
@@ -53,7 +54,8 @@ class MeshDesc(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("planes_solved", C.c_int), ("iterations_max", C.c_int),
                 ("iterations_total", C.c_int), ("refinements", C.c_int),
-                ("final_rel_residual", C.c_double), ("kernel_launches", C.c_int)]
+                ("final_rel_residual", C.c_double), ("kernel_launches", C.c_int),
+                ("planes_direct", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -110,6 +112,7 @@ def _load():
     L.sx_field_solve_batched_host.argtypes = [vp, P(dp), P(dp), P(dp), ip, ip, ip, dp, ip,
                                               P(SolveStats)]
     L.sx_profile_band_sweeps.argtypes = [vp, ip, vp]
+    L.sx_profile_mixed_iterations.argtypes = [vp, ip, vp]
     L.sx_modal_status.argtypes = [vp]
     L.sx_modal_tune.argtypes = [vp, ip, ip]
     L.sx_server_create.argtypes = [P(ServerConfig), P(vp)]
@@ -287,16 +290,23 @@ class ModalMatrixSys:
         self.last_stats = st.as_dict()
         return u
 
-    def tune(self, inner_iters=None, band_cluster=None):
+    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None):
         """Schedule knobs of the batched forms (None leaves a knob alone, 0
-        restores its default)."""
+        restores its default).  mixed_route: ROUTE_AUTO (by cost), ROUTE_CG
+        (FP32 CG for every mode), ROUTE_BAND (band Cholesky for every
+        factored mode)."""
         if inner_iters is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_INNER_ITERS, int(inner_iters)), "sx_modal_tune")
         if band_cluster is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_BAND_CLUSTER, int(band_cluster)), "sx_modal_tune")
+        if mixed_route is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_MIXED_ROUTE, int(mixed_route)), "sx_modal_tune")
 
     def profile_band_sweeps(self, reps, stream=0):
         _check(lib.sx_profile_band_sweeps(self.h, reps, stream), "sx_profile_band_sweeps")
+
+    def profile_mixed_iterations(self, reps, stream=0):
+        _check(lib.sx_profile_mixed_iterations(self.h, reps, stream), "sx_profile_mixed_iterations")
 
     def status(self):
         return _check(lib.sx_modal_status(self.h), "sx_modal_status")

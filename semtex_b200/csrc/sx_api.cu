@@ -35,16 +35,19 @@ void sx_modal_s::rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vecto
   uniq.clear();
   for (auto &x : sys)
     if (std::find(uniq.begin(), uniq.end(), x) == uniq.end()) uniq.push_back(x);
-  if (gexec) cudaGraphExecDestroy(gexec);
-  gexec = nullptr;
-  gkey[0] = gkey[1] = gkey[2] = nullptr;
+  fp64.reset();
+  hyb.reset();
   mkey[0] = mkey[1] = mkey[2] = nullptr;
-  gjobs.clear();
+  mmodes.clear();
   cluster_for.clear();
 }
 
 sx_modal_s::~sx_modal_s() {
-  if (gexec) cudaGraphExecDestroy(gexec);
+  fp64.reset();
+  hyb.reset();
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
+  if (aux) cudaStreamDestroy(aux);
   if (own && !own_stream_external) cudaStreamDestroy(own);
 }
 
@@ -93,6 +96,13 @@ int modal_populate(sx_modal_s &M, const double *lam, const double *bk2, const Sy
     const int mode = M.base_mode + l;
     int kind = M.method;
     if (M.method == SX_MIXED) kind = (mode == 0) ? SX_DIRECT : SX_JACPCG;  // src/matrix.cpp:93-96
+    if (M.method == SX_AUTO) {
+      const sx_mesh_s &Mh = *M.mesh;
+      kind = band_cheaper(Mh.np, Mh.nel, Mh.nglobal, Mh.nsolve, Mh.nband, Mh.kratio, lam[l] + bk2[l], M.n_inner,
+                          1e-12)
+                 ? SX_DIRECT
+                 : SX_JACPCG;
+    }
     std::shared_ptr<System> found;
     for (auto &s : M.uniq)
       if (same_constants(*s, lam[l], bk2[l], kind)) {
@@ -138,7 +148,7 @@ int modal_populate(sx_modal_s &M, const double *lam, const double *bk2, const Sy
 
 static int modal_build(sx_mesh m, int base_mode, int num_modes, const double *lam, const double *bk2,
                        int method, sx_modal *out) {
-  if (!m || !out || num_modes <= 0 || base_mode < 0 || method < SX_DIRECT || method > SX_MIXED)
+  if (!m || !out || num_modes <= 0 || base_mode < 0 || method < SX_DIRECT || method > SX_AUTO)
     return SX_ERR_ARG;
   *out = nullptr;
   std::unique_ptr<sx_modal_s> M(new sx_modal_s());
@@ -212,10 +222,12 @@ extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
     case SX_TUNE_BAND_CLUSTER:
       if (value > 16) return SX_ERR_ARG;
       s->forced_cluster = value > 0 ? value : 0;
-      if (s->gexec) {  // the captured batched graph bakes in the cluster size
-        cudaGraphExecDestroy(s->gexec);
-        s->gexec = nullptr;
-      }
+      s->fp64.reset();  // the captured graphs bake in the cluster size
+      s->hyb.reset();
+      return SX_OK;
+    case SX_TUNE_MIXED_ROUTE:
+      if (value < 0 || value > 2) return SX_ERR_ARG;
+      s->mixed_route = value;
       return SX_OK;
     default:
       return SX_ERR_ARG;
@@ -371,8 +383,100 @@ extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc
   return rc;
 }
 
-// Mixed-precision batched form: every solved plane of every mode in one
-// FP32-PCG / FP64-refinement iteration (sx_mixed.cu).
+// Batched FP64 direct solve of `groups` (DIRECT systems) on stream st: one
+// job per group in every kernel; the sequence is captured once into B's
+// graph and replayed while the arguments, the RHS workspace and the set of
+// modes stay the same.
+static int direct_batched(sx_modal_s *s, DirectBatch &B, const std::vector<Group> &groups, double *d_u,
+                          double *d_f, const double *d_bc, int nz, int plane_stride, cudaStream_t st) {
+  for (auto &g : groups)
+    if (s->sys[g.mode]->method != SX_DIRECT) {
+      set_error("the batched band solve needs DIRECT systems (local mode %d is not)", g.mode);
+      return SX_ERR_UNSUPPORTED;
+    }
+  int planes = 0;
+  std::vector<int> modes;
+  for (auto &g : groups) {
+    planes += g.P;
+    modes.push_back(g.mode);
+  }
+  SX_TRY(reserve_ws(*s, planes));
+  const bool same = B.exec && B.key[0] == d_u && B.key[1] == d_f && B.key[2] == d_bc && B.key[3] == s->rhs.p &&
+                    B.key[4] == s->Fb.p && B.key[5] == s->gess.p && B.nz == nz && B.stride == plane_stride &&
+                    B.modes == modes;
+  const MeshView M = s->mesh->view();
+  if (!same || !s->use_graphs) {
+    B.reset();
+    const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
+    std::vector<Job> jobs;
+    int slot = 0;
+    for (auto &g : groups) {
+      jobs.push_back(make_job(*s, g, slot, d_u, d_f, d_bc, plane_stride, bcstride));
+      slot += g.P;
+    }
+    if (B.djobs.n < jobs.size()) SX_TRY(B.djobs.alloc(jobs.size()));
+    SX_CUDA(cudaMemcpyAsync(B.djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
+    SX_CUDA(cudaStreamSynchronize(st));
+    SX_TRY(prepare_direct_kernels(M));
+    B.C = s->cluster((int)jobs.size());
+    B.jobs = jobs;
+    B.modes = modes;
+    if (!s->use_graphs) return direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches);
+    cudaGraph_t g = nullptr;
+    SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches);
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (rc != SX_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    SX_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&B.exec, g, 0);
+    cudaGraphDestroy(g);
+    SX_CUDA(ie);
+    B.key[0] = d_u;
+    B.key[1] = d_f;
+    B.key[2] = d_bc;
+    B.key[3] = s->rhs.p;
+    B.key[4] = s->Fb.p;
+    B.key[5] = s->gess.p;
+    B.nz = nz;
+    B.stride = plane_stride;
+  }
+  SX_CUDA(cudaGraphLaunch(B.exec, st));
+  return SX_OK;
+}
+
+bool sx::band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon,
+                      int n_inner, double tol_rel) {
+  if (!(hcon > 0.0)) return true;
+  const int nn = np * np, next = 4 * (np - 1), nint = nn - next;
+  const double per_round = std::max((double)n_inner, 5.3 * std::sqrt(1.0 + kratio / hcon));
+  const double rounds = std::max(1.0, std::ceil(std::log(std::max(tol_rel, 1e-15)) / std::log(1e-7)));
+  const double npts = nglobal + (double)nel * nint;
+  const double cg = per_round * rounds * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn);
+  const double band =
+      (2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0) /
+      2.0;
+  return cg > 3.0 * band;
+}
+
+// Route of a mode in the mixed-precision form: true = the FP64 band
+// Cholesky (the mode must be factored), false = FP32 CG inside FP64
+// refinement.
+static bool route_direct(const sx_modal_s &s, const System &S, double tol_rel) {
+  if (S.method != SX_DIRECT || !S.tiles.p) return false;
+  if (s.mixed_route == 1) return false;
+  if (s.mixed_route == 2) return true;
+  const sx_mesh_s &M = *s.mesh;
+  return band_cheaper(M.np, M.nel, M.nglobal, S.nsolve, M.nband, M.kratio, S.lambda2 + S.betak2, s.n_inner,
+                      tol_rel);
+}
+
+// Mixed-precision batched form (sx_mixed.cu): the modes routed to the FP32
+// iterations run as one FP32-CG / FP64-refinement solve of all their planes;
+// the modes routed to the band Cholesky run as one batched FP64 direct solve
+// on a second stream at the same time.
 static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
                                int plane_stride, double tol_rel, int max_refine, cudaStream_t st,
                                sx_solve_stats *stats) {
@@ -380,20 +484,54 @@ static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const doubl
   SX_TRY(plane_groups(*s, nz, groups));
   for (auto &u : s->uniq)
     if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, st));
+  std::vector<Group> gd;
   std::vector<MxGroup> mg;
-  for (auto &g : groups) mg.push_back({g.mode, g.plane0, g.P, s->sys[g.mode].get()});
-  const int nyq = (nz > 1 && s->base_mode == 0) ? 1 : -1;
-  const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
-                         s->mstride == plane_stride && s->mixed.n_inner == s->n_inner);
-  const MeshView M = s->mesh->view();
-  const int rc = mixed_solve(M, s->mixed, mg, nz, nyq, s->num_modes, d_u, d_f, d_bc, plane_stride, rebuild,
-                             tol_rel, max_refine, s->n_inner, s->use_graphs, st, stats);
+  std::vector<int> jmodes;
+  for (auto &g : groups) {
+    const System *S = s->sys[g.mode].get();
+    if (route_direct(*s, *S, tol_rel)) {
+      gd.push_back(g);
+    } else {
+      mg.push_back({g.mode, g.plane0, g.P, S});
+      jmodes.push_back(g.mode);
+    }
+  }
+  int dplanes = 0;
+  for (auto &g : gd) dplanes += g.P;
+  if (!gd.empty()) {
+    if (!s->aux) SX_CUDA(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    if (!s->ev_fork) SX_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    if (!s->ev_join) SX_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    SX_CUDA(cudaEventRecord(s->ev_fork, st));
+    SX_CUDA(cudaStreamWaitEvent(s->aux, s->ev_fork, 0));
+    SX_TRY(direct_batched(s, s->hyb, gd, d_u, d_f, d_bc, nz, plane_stride, s->aux));
+    SX_CUDA(cudaEventRecord(s->ev_join, s->aux));
+  }
+  sx_solve_stats loc{};
+  int rc = SX_OK;
+  if (!mg.empty()) {
+    const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
+                           s->mstride == plane_stride && s->mixed.n_inner == s->n_inner && s->mmodes == jmodes);
+    const MeshView M = s->mesh->view();
+    rc = mixed_solve(M, s->mixed, mg, nz, s->num_modes, d_u, d_f, d_bc, plane_stride, rebuild, tol_rel,
+                     max_refine, s->n_inner, s->use_graphs, st, &loc);
+    if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
+      s->mkey[0] = d_u;
+      s->mkey[1] = d_f;
+      s->mkey[2] = d_bc;
+      s->mnz = nz;
+      s->mstride = plane_stride;
+      s->mmodes = jmodes;
+    }
+  }
+  if (!gd.empty()) SX_CUDA(cudaStreamWaitEvent(st, s->ev_join, 0));
   if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
-  s->mkey[0] = d_u;
-  s->mkey[1] = d_f;
-  s->mkey[2] = d_bc;
-  s->mnz = nz;
-  s->mstride = plane_stride;
+  if (stats) {
+    *stats = loc;
+    stats->planes_solved += dplanes;
+    stats->planes_direct = dplanes;
+    if (!gd.empty()) stats->kernel_launches += s->hyb.launches;
+  }
   return rc;
 }
 
@@ -406,64 +544,11 @@ int solve_batched_on(sx_modal_s *s, double *d_u, double *d_f, const double *d_bc
     return mixed_solve_batched(s, d_u, d_f, d_bc, nz, plane_stride, tol_rel, max_refine, st, stats);
   std::vector<Group> groups;
   SX_TRY(plane_groups(*s, nz, groups));
-  for (auto &g : groups)
-    if (s->sys[g.mode]->method != SX_DIRECT) {
-      set_error("batched FP64 form needs DIRECT systems");
-      return SX_ERR_UNSUPPORTED;
-    }
-  int planes = 0;
-  for (auto &g : groups) planes += g.P;
-  SX_TRY(reserve_ws(*s, planes));
-  const bool same = s->gexec && s->gkey[0] == d_u && s->gkey[1] == d_f && s->gkey[2] == d_bc &&
-                    s->gnz == nz && s->gstride == plane_stride && s->gprec == precision;
-  const MeshView M = s->mesh->view();
-  if (!same || !s->use_graphs) {
-    if (s->gexec) {
-      cudaGraphExecDestroy(s->gexec);
-      s->gexec = nullptr;
-    }
-    const long long bcstride = (long long)std::max(s->mesh->nbound, 1) * s->mesh->np;
-    std::vector<Job> jobs;
-    int slot = 0;
-    for (auto &g : groups) {
-      jobs.push_back(make_job(*s, g, slot, d_u, d_f, d_bc, plane_stride, bcstride));
-      slot += g.P;
-    }
-    if (s->bjobs.n < jobs.size()) SX_TRY(s->bjobs.alloc(jobs.size()));
-    SX_CUDA(cudaMemcpyAsync(s->bjobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
-    SX_CUDA(cudaStreamSynchronize(st));
-    SX_TRY(prepare_direct_kernels(M));
-    const int C = s->cluster((int)jobs.size());
-    s->gjobs = jobs;
-    s->gC = C;
-    if (!s->use_graphs) {
-      SX_TRY(direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches));
-    } else {
-      cudaGraph_t g = nullptr;
-      SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const int rc = direct_solve_jobs(M, s->bjobs.p, jobs, st, C, &s->glaunches);
-      const cudaError_t ce = cudaStreamEndCapture(st, &g);
-      if (rc != SX_OK) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-      }
-      SX_CUDA(ce);
-      const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
-      cudaGraphDestroy(g);
-      SX_CUDA(ie);
-      s->gkey[0] = d_u;
-      s->gkey[1] = d_f;
-      s->gkey[2] = d_bc;
-      s->gnz = nz;
-      s->gstride = plane_stride;
-      s->gprec = precision;
-    }
-  }
-  if (s->use_graphs) SX_CUDA(cudaGraphLaunch(s->gexec, st));
+  SX_TRY(direct_batched(s, s->fp64, groups, d_u, d_f, d_bc, nz, plane_stride, st));
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
-    stats->planes_solved = planes;
-    stats->kernel_launches = s->glaunches;
+    for (auto &g : groups) stats->planes_solved += g.P;
+    stats->kernel_launches = s->fp64.launches;
   }
   return SX_OK;
 }
@@ -522,8 +607,13 @@ int sx::copy_solved_planes(double *h_u, const double *d_u, int nz, int plane_str
 }
 
 extern "C" int sx_profile_band_sweeps(sx_modal s, int reps, void *stream) {
-  if (!s || reps <= 0 || s->gjobs.empty()) return SX_ERR_ARG;
+  if (!s || reps <= 0 || s->fp64.jobs.empty()) return SX_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  for (int r = 0; r < reps; r++) SX_TRY(band_sweep_jobs(s->bjobs.p, s->gjobs, s->gC, st));
+  for (int r = 0; r < reps; r++) SX_TRY(band_sweep_jobs(s->fp64.djobs.p, s->fp64.jobs, s->fp64.C, st));
   return SX_OK;
+}
+
+extern "C" int sx_profile_mixed_iterations(sx_modal s, int reps, void *stream) {
+  if (!s) return SX_ERR_ARG;
+  return mixed_profile_iterations(s->mesh->view(), s->mixed, reps, (cudaStream_t)stream);
 }

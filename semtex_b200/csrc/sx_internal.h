@@ -138,6 +138,9 @@ struct MeshView {
   const int *g2e_last;                   // nglobal: last (e*next+i) writing node (local2global)
   const int4 *g2e4;                      // nglobal: first 4 CSR entries, -1 padded, .w = -2 if more
   const unsigned long long *owner;       // nel: bit a set when element e is node btog[e][a]'s last writer
+  const int4 *e2w4;                      // nel*next: g2e4 of node btog[e][a] (the gather list per slot)
+  const float4 *Gf;                      // nel*npnp: (Q1, Q2, Q3, Q4) in FP32, tensor order
+  const int *pmap;                       // npnp: edge-map slot of tensor node t (inverse of emap)
   int nbound;
   const int *b_elmt, *b_side, *b_kind;
   const double *b_K, *b_C, *b_area;      // b_area: nbound*np
@@ -167,9 +170,15 @@ struct sx_mesh_s {
   sx::DBuf<double> dD, dQ1, dQ2, dQ3, dQ4, dQ8, dK, dC, darea;
   sx::DBuf<float> dQ1f, dQ2f, dQ3f, dQ4f, dDf;
   sx::DBuf<unsigned char> dhasQ3;
+  sx::DBuf<int> dpmap;
   sx::DBuf<int> demap, dbtog, dbmask, demask, dg2e_ptr, dg2e_idx, dg2e_last, dbe, dbs, dbk;
   sx::DBuf<int> dnat_ptr, dnat_idx, dcolour_elmt;
-  sx::DBuf<int4> dg2e4;
+  sx::DBuf<int4> dg2e4, de2w4;
+  sx::DBuf<float4> dGf;
+  // max over nodes of the assembled stiffness diagonal over the assembled
+  // mass diagonal: the Jacobi-scaled operator's condition number is about
+  // 1 + kratio / hCon
+  double kratio = 0.0;
   sx::DBuf<unsigned long long> downer;
   sx::MeshView view() const;
 };
@@ -199,6 +208,19 @@ int system_build_direct(System &S, cudaStream_t st);
 int system_build_jacobi(System &S, cudaStream_t st);
 int system_build_jacobi_diag(System &S, cudaStream_t st);
 int system_band_export(const System &S, double *ab);  // LAPACK band, host
+
+// sx_mesh_s::kratio of a mesh description, from host geometry alone.
+int mesh_kratio(const sx_mesh_desc *d, double *out);
+
+// Whether the FP64 band Cholesky is the cheaper route, in streamed bytes,
+// for a mode with Helmholtz constant hcon solved to tol_rel: Jacobi-CG takes
+// about 5.3 sqrt(1 + kratio / hcon) iterations per 1e-7 of residual
+// (measured with the oracle over lambda2 = 1..1e6 at N = 8 and 10), each
+// streaming 4 (8 npts + 2 nel np^2) bytes per plane; the band solve streams
+// its factor twice plus the condensation matrices, at about a third of the
+// CG kernel's bandwidth (its sweeps are latency-bound), hence the factor 3.
+bool band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon, int n_inner,
+                  double tol_rel);
 
 // Solve workspace for up to `planes` planes of one system.
 struct Work {

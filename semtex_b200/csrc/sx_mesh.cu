@@ -196,6 +196,7 @@ sx::MeshView sx_mesh_s::view() const {
   v.btog = dbtog.p; v.bmask = dbmask.p; v.emask = demask.p;
   v.g2e_ptr = dg2e_ptr.p; v.g2e_idx = dg2e_idx.p; v.g2e_last = dg2e_last.p;
   v.g2e4 = dg2e4.p; v.owner = downer.p;
+  v.e2w4 = de2w4.p; v.Gf = dGf.p; v.pmap = dpmap.p;
   v.nbound = nbound; v.b_elmt = dbe.p; v.b_side = dbs.p; v.b_kind = dbk.p;
   v.b_K = dK.p; v.b_C = dC.p; v.b_area = darea.p;
   v.nat_ptr = dnat_ptr.p; v.nat_idx = dnat_idx.p;
@@ -214,6 +215,62 @@ static int bnd_node(const sx_mesh_s &M, int b, int i) {
   if (i < nm) return bmap[side * nm + i];
   return side == 3 ? bmap[0] : bmap[side * nm + nm];
 }
+
+// max over nodes of diag(K)_g / diag(M)_g from the host geometry, Q3 cross
+// terms left out.  The stiffness part of Element::HelmholtzDiag
+// (src/element.cpp:1512-1561) at tensor node (i, j) is
+//   sum_k D(k, i)^2 Q2(k, j) + sum_k Q1(i, k) D(k, j)^2
+// and the mass part Q4(i, j); boundary nodes are summed over their elements.
+static double stiffness_mass_ratio(const sx_mesh_s &M) {
+  const int np = M.np, nn = M.npnp, next = M.next, nint = M.nint;
+  std::vector<double> K((size_t)M.nglobal + (size_t)M.nel * nint, 0.0), Mm(K.size(), 0.0);
+  for (int e = 0; e < M.nel; e++) {
+    const double *Q1 = &M.Q1[(size_t)e * nn], *Q2 = &M.Q2[(size_t)e * nn], *Q4 = &M.Q4[(size_t)e * nn];
+    for (int i = 0; i < np; i++)
+      for (int j = 0; j < np; j++) {
+        double k = 0.0;
+        for (int m = 0; m < np; m++) {
+          const double di = M.D[m * np + i], dj = M.D[m * np + j];
+          k += di * di * Q2[m * np + j] + Q1[i * np + m] * dj * dj;
+        }
+        const int t = i * np + j, a = M.pmap[t];
+        const size_t g = a < next ? (size_t)M.btog[(size_t)e * next + a]
+                                  : (size_t)M.nglobal + (size_t)e * nint + (a - next);
+        K[g] += k;
+        Mm[g] += Q4[t];
+      }
+  }
+  double r = 0.0;
+  for (size_t g = 0; g < K.size(); g++)
+    if (Mm[g] > 0.0) r = std::max(r, K[g] / Mm[g]);
+  return r;
+}
+
+namespace sx {
+
+int mesh_kratio(const sx_mesh_desc *d, double *out) {
+  if (!d || !out || d->np < NP_MIN || d->np > NP_MAX || d->nel <= 0 || !d->x || !d->y || !d->btog ||
+      d->nglobal <= 0)
+    return SX_ERR_ARG;
+  sx_mesh_s T;  // host geometry only
+  const int np = d->np, nn = np * np, next = 4 * (np - 1), nel = d->nel;
+  T.np = np; T.npnp = nn; T.next = next; T.nint = nn - next; T.nel = nel; T.nglobal = d->nglobal;
+  gll_tables(np, T.z, T.w, T.D);
+  edge_maps(np, T.emap, T.pmap);
+  const size_t tot = (size_t)nel * nn, tb = (size_t)nel * next;
+  T.Q1.assign(tot, 0.0); T.Q2.assign(tot, 0.0); T.Q3.assign(tot, 0.0);
+  T.Q4.assign(tot, 0.0); T.Q8.assign(tot, 0.0);
+  T.hasQ3.assign(nel, 0);
+  for (int e = 0; e < nel; e++)
+    SX_TRY(element_geometry(T, e, d->x + (size_t)e * nn, d->y + (size_t)e * nn));
+  T.btog.assign(d->btog, d->btog + tb);
+  for (size_t i = 0; i < tb; i++)
+    if (T.btog[i] < 0 || T.btog[i] >= d->nglobal) return SX_ERR_ARG;
+  *out = stiffness_mass_ratio(T);
+  return SX_OK;
+}
+
+}  // namespace sx
 
 extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   if (!d || !out) return SX_ERR_ARG;
@@ -354,6 +411,13 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   SX_TRY(M->dQ2f.upload(f2.data(), tot));
   SX_TRY(M->dQ3f.upload(f3.data(), tot));
   SX_TRY(M->dQ4f.upload(f4.data(), tot));
+  {
+    std::vector<float4> gf(tot);
+    for (size_t i = 0; i < tot; i++) gf[i] = make_float4(f1[i], f2[i], f3[i], f4[i]);
+    SX_TRY(M->dGf.upload(gf.data(), tot));
+  }
+  SX_TRY(M->dpmap.upload(M->pmap.data(), nn));
+  M->kratio = stiffness_mass_ratio(*M);
   std::vector<float> df(M->D.begin(), M->D.end());
   SX_TRY(M->dDf.upload(df.data(), df.size()));
   SX_TRY(M->dhasQ3.upload(M->hasQ3.data(), nel));
@@ -373,6 +437,9 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       g4[g] = make_int4(v[0], v[1], v[2], v[3]);
     }
     SX_TRY(M->dg2e4.upload(g4.data(), g4.size()));
+    std::vector<int4> e4((size_t)nel * next);
+    for (size_t k = 0; k < e4.size(); k++) e4[k] = g4[M->btog[k]];
+    SX_TRY(M->de2w4.upload(e4.data(), e4.size()));
     std::vector<unsigned long long> own(nel, 0ull);
     for (int e = 0; e < nel; e++)
       for (int a = 0; a < next; a++)

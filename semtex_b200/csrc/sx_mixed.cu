@@ -17,18 +17,17 @@
 // loaded once for all planes.  Thread mapping everywhere: lane = plane
 // within a chunk of 32 (blockIdx.y = chunk), warp = node row.
 //
-// One inner iteration is two kernels, each with its reduction fused in:
-//   k_x_op32  p <- z + beta p (z = PC r) on the fly, element operator
-//             q_e = A_e p_e (FP32 sum factorisation), interior q stored,
-//             boundary contributions to an element-local buffer, and
-//             p.q = sum_e p_e . q_e (the assembled dot: p vanishes on
-//             essential nodes)
-//   k_x_upd   direct-stiffness gather of q (element order), d += alpha p,
-//             r -= alpha q, rho = r.(PC r)
+// One inner iteration is one kernel, k_cg: the Chronopoulos-Gear form of
+// PCG (one global reduction per iteration), element by element --
+//   gather w = A u of the previous launch (direct-stiffness sum of the
+//   element boundary slots, in element order), the vector updates at the
+//   element's nodes (every element computes its shared nodes, the owner
+//   writes them), u = PC r, the element operator A_e u_e, and the two dots
+//   (r, u) and (A u, u) = sum_e u_e . A_e u_e.
 // Reductions are two-level and deterministic: per-block partials per plane,
-// the last block of a chunk sums them in index order.  Each refinement round
-// is one captured CUDA graph; the host reads the residual norms between
-// rounds.
+// the last block of a chunk sums them in index order and computes the next
+// iteration's scalars.  Each refinement round is one captured CUDA graph;
+// the host reads the residual norms between rounds.
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -46,7 +45,7 @@ __device__ __forceinline__ int gidx(const MeshView &M, int e, int a) {
   return a < M.next ? M.btog[(size_t)e * M.next + a] : M.nglobal + e * M.nint + (a - M.next);
 }
 
-__device__ __forceinline__ bool real_plane(const MxParams &P, int p) { return p < P.nz && p != P.nyq; }
+__device__ __forceinline__ bool real_plane(const MxParams &P, int p) { return P.active[p] != 0; }
 
 // Direct-stiffness sum of element-local boundary values at global node g,
 // in element order (the CSR order): up to four loads issued together.
@@ -136,6 +135,65 @@ __device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, 
     if (outB) outB[p] = fb;
   }
   if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
+}
+
+// chunk_reduce2 for a block of ROWS warps that leaves the per-plane totals
+// to the caller: returns true in warp 0 of the chunk's last block, with the
+// sums of a and b over the chunk's blocks in fa, fb.
+template <int ROWS>
+__device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsigned *cnt, int G, double &fa,
+                                          double &fb) {
+  __shared__ double sa[ROWS][MX_CH], sb[ROWS][MX_CH];
+  __shared__ int last;
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.y * MX_CH + lane, PPc = gridDim.y * MX_CH;
+  sa[row][lane] = a;
+  sb[row][lane] = b;
+  __syncthreads();
+  if (row == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int r = 0; r < ROWS; r++) {
+      ta += sa[r][lane];
+      tb += sb[r][lane];
+    }
+    reinterpret_cast<double2 *>(part)[(size_t)blockIdx.x * PPc + p] = make_double2(ta, tb);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&cnt[blockIdx.y], 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double ta = 0.0, tb = 0.0;
+  const double2 *pp = reinterpret_cast<const double2 *>(part) + p;
+  int bx = row;
+#pragma unroll 1
+  for (; bx + 3 * ROWS < G; bx += 4 * ROWS) {
+    const double2 v0 = __ldcg(&pp[(size_t)bx * PPc]);
+    const double2 v1 = __ldcg(&pp[(size_t)(bx + ROWS) * PPc]);
+    const double2 v2 = __ldcg(&pp[(size_t)(bx + 2 * ROWS) * PPc]);
+    const double2 v3 = __ldcg(&pp[(size_t)(bx + 3 * ROWS) * PPc]);
+    ta += v0.x; tb += v0.y;
+    ta += v1.x; tb += v1.y;
+    ta += v2.x; tb += v2.y;
+    ta += v3.x; tb += v3.y;
+  }
+  for (; bx < G; bx += ROWS) {
+    const double2 v = __ldcg(&pp[(size_t)bx * PPc]);
+    ta += v.x;
+    tb += v.y;
+  }
+  sa[row][lane] = ta;
+  sb[row][lane] = tb;
+  __syncthreads();
+  if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
+  if (row != 0) return false;
+  fa = fb = 0.0;
+  for (int r = 0; r < ROWS; r++) {
+    fa += sa[r][lane];
+    fb += sb[r][lane];
+  }
+  return true;
 }
 
 // GLL derivative matrices for np = 3..12, FP32 and FP64, in constant memory:
@@ -298,17 +356,16 @@ __global__ void __launch_bounds__(256) k_x_constrain(MeshView M, MxParams P, dou
   for (int a = row; a < NN; a += MX_ROWS) Ye[ye_index(M, e, a, P.PP) + p] = -F[emap[a] * MX_CH + lane];
 }
 
-// b = DSS(Ye) + <h,w>, essential tail zero; x = 0, d = 0, r = b (FP32),
-// p_0 = PC r; per-plane ||b||^2 and rho_0.
+// b = DSS(Ye) + <h,w>, essential tail zero; x = 0, r = b (FP32); per-plane
+// ||b||^2.
 __global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const double *__restrict__ Ye, double *b64,
-                                               double *x64, float *r32, float *d32, float *p0, double *b2,
-                                               double *rho0, double *part, unsigned *cnt) {
+                                               double *x64, float *r32, double *b2, double *part, unsigned *cnt) {
   const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
-  const int ns = P.nsolve[p], c = pc_col(P, p);
+  const int ns = P.nsolve[p];
   const bool rp = real_plane(P, p);
-  double bb = 0.0, rz = 0.0;
+  double bb = 0.0;
   for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
     double s = 0.0;
     if (g < M.nglobal) {
@@ -329,144 +386,257 @@ __global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const dou
     const size_t o = (size_t)g * PP + p;
     b64[o] = s;
     x64[o] = 0.0;
-    const float rf = (float)s;
-    r32[o] = rf;
-    d32[o] = 0.0f;
-    const float z = P.pcf[(size_t)g * P.M + c] * rf;
-    p0[o] = z;
+    r32[o] = (float)s;
     bb += s * s;
-    rz += (double)rf * (double)z;
   }
-  chunk_reduce2(bb, rz, part, cnt, gridDim.x, b2, rho0);
+  chunk_reduce2(bb, 0.0, part, cnt, gridDim.x, b2, nullptr);
 }
 
 // ---------------------------------------------------------------------------
-// inner FP32 PCG iteration
+// inner FP32 PCG iteration (Chronopoulos-Gear)
 // ---------------------------------------------------------------------------
+//
+// Chronopoulos & Gear (J. Comput. Appl. Math. 25 (1989) 153-168) carry
+// s = A p beside p, so both inner products of an iteration come from the
+// same vectors and share one reduction:
+//   init  u0 = PC r0, w0 = A u0, gamma0 = (r0,u0), delta0 = (w0,u0),
+//         alpha0 = gamma0 / delta0, beta0 = 0
+//   it i  p = u + beta p, s = w + beta s, d += alpha p, r -= alpha s,
+//         u = PC r, w = A u, gamma' = (r,u), delta = (w,u),
+//         beta' = gamma' / gamma, alpha' = gamma' / (delta - beta' gamma' / alpha)
+// In exact arithmetic these are the iterates of the Jacobi-PCG loop of
+// src/field.cpp:672-704.
+
+enum { CG_INIT = 0, CG_ITER = 1, CG_LAST = 2 };
+
+// Direct-stiffness sum at global node g from its gather list q (the first
+// four CSR entries, or .w == -2 to walk the CSR), in element order.
+__device__ __forceinline__ float gather_w(const MeshView &M, const float *__restrict__ W, int4 q, int g, int PP,
+                                          int p) {
+  if (q.w == -2) {
+    float s = 0.0f;
+    for (int k = M.g2e_ptr[g]; k < M.g2e_ptr[g + 1]; k++) s += W[(size_t)M.g2e_idx[k] * PP + p];
+    return s;
+  }
+  const float v0 = W[(size_t)q.x * PP + p];
+  const float v1 = q.y >= 0 ? W[(size_t)q.y * PP + p] : 0.0f;
+  const float v2 = q.z >= 0 ? W[(size_t)q.z * PP + p] : 0.0f;
+  const float v3 = q.w >= 0 ? W[(size_t)q.w * PP + p] : 0.0f;
+  return ((v0 + v1) + v2) + v3;
+}
+
+// One launch = one iteration for every plane: block (element e, chunk of 32
+// planes), NP warps.  Phase A walks the element's nodes in edge-map order
+// (warp w takes slots w, w + NP, ...: the boundary slots spread evenly);
+// the operator then runs on tensor lines: warp w owns row w for the
+// x-derivative terms and column w for the y-derivative terms, the derivative
+// matrix is read from constant memory with compile-time subscripts, and
+// shared memory is touched about five times per node.
+// mode CG_INIT: u = PC r from r[0], w -> W[0]; scalars -> slot 0.
+// mode CG_ITER: iteration `it` (slots it & 1 in, (it + 1) & 1 out).
+// mode CG_LAST: only the owners' d update, folded into x64; no operator.
+// Resident blocks per SM the register budget is set for: the kernel is
+// latency-bound (dependent gathers), so occupancy pays more than registers.
+constexpr int cg_min_blocks(int np) { return np <= 10 ? 3 : 2; }
 
 template <int NP>
-__global__ void __launch_bounds__(256) k_x_op32(MeshView M, MxParams P, const float *__restrict__ r32,
-                                                const float *__restrict__ pold, float *__restrict__ pnew,
-                                                float *__restrict__ q32, float *__restrict__ Yb,
-                                                const double *rho_i, const double *rho_im1, double *pq_out, int it,
-                                                double *part, unsigned *cnt) {
-  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
-  constexpr int NA = (NN + MX_ROWS - 1) / MX_ROWS;  // nodes per warp row
-  extern __shared__ __align__(16) float smf[];
-  float *U = smf, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
-  __shared__ float D[NN], Q[4][NN];
-  __shared__ int emap[NN], gtab[NN];
-  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+__global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
+    k_cg(MeshView M, MxParams P, CgVecs V, int it, int mode, double *part,
+                                                unsigned *cnt) {
+  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, DO = DOff<NP>::v;
+  // two [NN][32] exchange buffers: B0 holds u, B1 the column results (and on
+  // curved elements both carry r and s once)
+  extern __shared__ __align__(16) float smc[];
+  float *B0 = smc, *B1 = smc + NN * MX_CH;
+  __shared__ int gtab[NN], emt[NN], tsl[NN];
+  __shared__ int4 w4[NE];
+  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
-  const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 256) {
-    D[i] = M.Df[i];
-    Q[0][i] = M.Q1f[eo + i];
-    Q[1][i] = M.Q2f[eo + i];
-    Q[2][i] = M.Q3f[eo + i];
-    Q[3][i] = M.Q4f[eo + i];
-    emap[i] = M.emap[i];
-    gtab[i] = (i < NE) ? M.btog[(size_t)e * NE + i] : M.nglobal + e * NI + (i - NE);
+  for (int a = threadIdx.x; a < NN; a += NP * 32) {
+    gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
+    emt[a] = M.emap[a];
+    tsl[a] = M.pmap[a];
+    if (a < NE) w4[a] = M.e2w4[(size_t)e * NE + a];
   }
-  float beta = 0.0f;
-  if (it > 0) {
-    const double rn = rho_i[p], ro = rho_im1[p];
-    beta = (ro != 0.0) ? (float)(rn / ro) : 0.0f;
+  const bool init = mode == CG_INIT, last = mode == CG_LAST;
+  const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
+  const bool warm = !init && it > 0;  // s, p, d hold previous iterates
+  // buffers of this launch, selected without indexing the parameter arrays
+  const float *__restrict__ rin = cur ? V.r[1] : V.r[0];
+  float *__restrict__ rout = nxt ? V.r[1] : V.r[0];
+  const float *__restrict__ sin = nxt ? V.s[1] : V.s[0];
+  float *__restrict__ sout = cur ? V.s[1] : V.s[0];
+  const float *__restrict__ Win = cur ? V.W[1] : V.W[0];
+  float *__restrict__ Wout = nxt ? V.W[1] : V.W[0];
+  const double *gam_in = cur ? V.gam[1] : V.gam[0], *alpha_in = cur ? V.alpha[1] : V.alpha[0];
+  const double *beta_in = cur ? V.beta[1] : V.beta[0];
+  double *gam_out = nxt ? V.gam[1] : V.gam[0], *alpha_out = nxt ? V.alpha[1] : V.alpha[0];
+  double *beta_out = nxt ? V.beta[1] : V.beta[0];
+  const int ns = P.nsolve[p], c = pc_col(P, p);
+  float alpha = 0.0f, beta = 0.0f;
+  if (!init) {
+    alpha = (float)alpha_in[p];
+    beta = (float)beta_in[p];
   }
-  const int c = pc_col(P, p);
-  // one writer per global node: the last element that touches it
   const unsigned long long own = M.owner[e];
   __syncthreads();
-  // gather: every load of this thread issued before any is used
-  float pv[NA], rv[NA], cv[NA];
-#pragma unroll
-  for (int t = 0; t < NA; t++) {
-    const int a = row + t * MX_ROWS;
-    if (a < NN) {
-      const int g = gtab[a];
-      const size_t o = (size_t)g * PP + p;
-      pv[t] = pold[o];
-      if (it > 0) {
-        rv[t] = r32[o];
-        cv[t] = P.pcf[(size_t)g * P.M + c];
-      }
-    }
-  }
-#pragma unroll
-  for (int t = 0; t < NA; t++) {
-    const int a = row + t * MX_ROWS;
-    if (a < NN) {
-      float v = pv[t];
-      if (it > 0) {
-        v = cv[t] * rv[t] + beta * v;
-        if (a >= NE || ((own >> a) & 1ull)) pnew[(size_t)gtab[a] * PP + p] = v;
-      }
-      U[emap[a] * MX_CH + lane] = v;
-    }
-  }
-  __syncthreads();
-  op_stage1<NP, float>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
-  __syncthreads();
-  const float hc = (float)P.hcon[p];
-  double pq = 0.0;
-  for (int a = row; a < NN; a += MX_ROWS) {
-    const int idx = emap[a];
-    const float t = op_stage2<NP, float>(D, Q[3], hc, U, R, S, idx);
-    pq += (double)(U[idx * MX_CH + lane] * t);
-    if (a < NE)
-      Yb[((size_t)e * NE + a) * PP + p] = t;
-    else
-      q32[(size_t)gtab[a] * PP + p] = t;
-  }
-  chunk_reduce2(pq, 0.0, part, cnt, gridDim.x, pq_out, nullptr);
-}
 
-__global__ void __launch_bounds__(256) k_x_upd(MeshView M, MxParams P, const float *__restrict__ pcur,
-                                               const float *__restrict__ q32, const float *__restrict__ Yb,
-                                               float *d32, float *r32, double *x64, const double *rho_i,
-                                               const double *pq_i, double *rho_next, int last, double *part,
-                                               unsigned *cnt) {
-  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
-  const int npts = M.nglobal + M.nel * M.nint;
-  const int ns = P.nsolve[p], c = pc_col(P, p);
-  const double pq = pq_i[p];
-  const float alpha = (pq > 0.0) ? (float)(rho_i[p] / pq) : 0.0f;
-  double rz = 0.0;
-  constexpr int UNR = 4;  // nodes per thread per pass, loads issued together
-  const int stride = gridDim.x * MX_ROWS;
-  for (int base = blockIdx.x * MX_ROWS + row; base < npts; base += stride * UNR) {
-    float qv[UNR], pv[UNR], dv[UNR], rv[UNR], cv[UNR];
+  // ---- phase A: vector updates at the element's nodes, u = PC r -> U, in
+  // two batches of slots, each batch's loads issued before any is used
+  constexpr int KB = (NP + 1) / 2;
+  double gam = 0.0;
 #pragma unroll
-    for (int u = 0; u < UNR; u++) {
-      const int g = base + u * stride;
-      if (g < npts) {
+  for (int k0 = 0; k0 < NP; k0 += KB) {
+    float rv[KB], cv[KB], wv[KB], sv[KB], pv[KB], dv[KB];
+#pragma unroll
+    for (int kk = 0; kk < KB; kk++) {
+      rv[kk] = cv[kk] = wv[kk] = sv[kk] = pv[kk] = dv[kk] = 0.0f;
+      if (k0 + kk >= NP) continue;
+      const int a = w + (k0 + kk) * NP;
+      const int g = gtab[a];
+      const bool solve = a >= NE || g < ns;
+      const bool mine = a >= NE || ((own >> a) & 1ull);
+      if (solve && (!last || mine)) {
         const size_t o = (size_t)g * PP + p;
-        pv[u] = pcur[o];
-        dv[u] = d32[o];
-        rv[u] = r32[o];
-        cv[u] = P.pcf[(size_t)g * P.M + c];
-        qv[u] = (g >= M.nglobal) ? q32[o] : (g < ns ? dss_gather(M, Yb, g, PP, p) : 0.0f);
+        rv[kk] = rin[o];
+        cv[kk] = P.pcf[(size_t)g * P.M + c];
+        if (!init && !last) {
+          wv[kk] = a >= NE ? V.wi[o] : gather_w(M, Win, w4[a], g, PP, p);
+          if (warm) sv[kk] = sin[o];
+        }
+        if (warm && mine) {
+          pv[kk] = V.p[o];
+          dv[kk] = V.d[o];
+        }
       }
     }
 #pragma unroll
-    for (int u = 0; u < UNR; u++) {
-      const int g = base + u * stride;
-      if (g < npts) {
-        const size_t o = (size_t)g * PP + p;
-        const float d = dv[u] + alpha * pv[u];
-        const float r = rv[u] - alpha * qv[u];
-        r32[o] = r;
-        if (last)
-          x64[o] += (double)d;
-        else
-          d32[o] = d;
-        const float z = cv[u] * r;
-        rz += (double)r * (double)z;
+    for (int kk = 0; kk < KB; kk++) {
+      if (k0 + kk >= NP) continue;
+      const int a = w + (k0 + kk) * NP;
+      const int g = gtab[a];
+      const bool solve = a >= NE || g < ns;
+      const bool mine = a >= NE || ((own >> a) & 1ull);
+      const size_t o = (size_t)g * PP + p;
+      float un = 0.0f;
+      if (init) {
+        un = cv[kk] * rv[kk];
+        if (solve && mine) gam += (double)rv[kk] * (double)un;
+      } else if (solve) {
+        const float uo = cv[kk] * rv[kk];
+        const float pp = warm ? uo + beta * pv[kk] : uo;
+        const float dd = warm ? dv[kk] + alpha * pp : alpha * pp;
+        if (last) {
+          if (mine) V.x64[o] += (double)dd;
+        } else {
+          const float s = warm ? wv[kk] + beta * sv[kk] : wv[kk];
+          const float rn = rv[kk] - alpha * s;
+          un = cv[kk] * rn;
+          if (mine) {
+            sout[o] = s;
+            rout[o] = rn;
+            V.p[o] = pp;
+            V.d[o] = dd;
+            gam += (double)rn * (double)un;
+          }
+        }
       }
+      if (!last) B0[emt[a] * MX_CH + lane] = un;
     }
   }
-  chunk_reduce2(rz, 0.0, part, cnt, gridDim.x, rho_next, nullptr);
+  if (last) return;  // block-uniform
+  __syncthreads();
+
+  // ---- operator: out = hc Q4 u + D^T S + R D on tensor lines
+  float ur[NP], R[NP], S[NP];
+  {
+    float uc[NP];
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      ur[j] = B0[(w * NP + j) * MX_CH + lane];  // row w
+      uc[j] = B0[(j * NP + w) * MX_CH + lane];  // column w
+    }
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      float r = 0.0f, s = 0.0f;
+#pragma unroll
+      for (int k = 0; k < NP; k++) {
+        r += ur[k] * c_Df[DO + j * NP + k];  // r(w, j) = sum_k u(w, k) D(j, k)
+        s += c_Df[DO + j * NP + k] * uc[k];  // s(j, w) = sum_k D(j, k) u(k, w)
+      }
+      R[j] = r;
+      S[j] = s;
+    }
+  }
+  const float4 *G = M.Gf + (size_t)e * NN;
+  if (M.hasQ3[e]) {
+    // curved: R = Q1 r + Q3 s, S = Q2 s + Q3 r need both at every node
+    __syncthreads();  // every warp has its u lines: B0 is free
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      B1[(w * NP + j) * MX_CH + lane] = R[j];
+      B0[(j * NP + w) * MX_CH + lane] = S[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      const float4 gr = G[w * NP + j], gc = G[j * NP + w];
+      const float s_wj = B0[(w * NP + j) * MX_CH + lane], r_jw = B1[(j * NP + w) * MX_CH + lane];
+      R[j] = gr.x * R[j] + gr.z * s_wj;
+      S[j] = gc.y * S[j] + gc.z * r_jw;
+    }
+    __syncthreads();  // B1 is free for the column results
+  } else {
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      R[j] *= G[w * NP + j].x;
+      S[j] *= G[j * NP + w].y;
+    }
+  }
+  // column w: a(i, w) = sum_k D(k, i) S(k, w), handed to the row owners
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    float a = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NP; k++) a += c_Df[DO + k * NP + i] * S[k];
+    B1[(i * NP + w) * MX_CH + lane] = a;
+  }
+  __syncthreads();
+  // row w: out(w, j) = hc Q4 u + a(w, j) + sum_k R(w, k) D(k, j)
+  const float hc = (float)P.hcon[p];
+  double del = 0.0;
+#pragma unroll
+  for (int j = 0; j < NP; j++) {
+    float b = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NP; k++) b += R[k] * c_Df[DO + k * NP + j];
+    const int t = w * NP + j, a = tsl[t];
+    const float out = G[t].w * hc * ur[j] + B1[t * MX_CH + lane] + b;
+    if (a < NE)
+      Wout[((size_t)e * NE + a) * PP + p] = out;
+    else
+      V.wi[(size_t)gtab[a] * PP + p] = out;
+    del += (double)ur[j] * (double)out;
+  }
+
+  // ---- gamma = (r, u), delta = (A u, u); the chunk's last block forms the
+  // next iteration's scalars
+  double gn, dn;
+  if (chunk_sum<NP>(gam, del, part, cnt, gridDim.x, gn, dn)) {
+    double an, bn;
+    if (init) {
+      bn = 0.0;
+      an = dn > 0.0 ? gn / dn : 0.0;
+    } else {
+      const double go = gam_in[p], ao = alpha_in[p];
+      bn = go > 0.0 ? gn / go : 0.0;
+      const double den = ao > 0.0 ? dn - bn * gn / ao : dn;
+      an = (gn > 0.0 && den > 0.0) ? gn / den : 0.0;
+    }
+    gam_out[p] = gn;
+    alpha_out[p] = an;
+    beta_out[p] = bn;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -502,16 +672,17 @@ __global__ void __launch_bounds__(256) k_x_op64(MeshView M, MxParams P, const do
     Ye[ye_index(M, e, a, PP) + p] = op_stage2<NP, double>(D, Q[3], hc, U, R, S, emap[a]);
 }
 
-// r = b - A x (FP64), essential tail zero; restart the inner solve:
-// r32 = r, d = 0, p_0 = PC r; per-plane ||r||^2 and rho_0.
+// r = b - A x (FP64), essential tail zero; the next round's inner solve
+// starts from r32 = r (and d = 0, which its first iteration assumes);
+// per-plane ||r||^2.
 __global__ void __launch_bounds__(256) k_x_res(MeshView M, MxParams P, const double *__restrict__ Ye,
-                                               const double *__restrict__ b64, float *r32, float *d32, float *p0,
-                                               double *r2, double *rho0, double *part, unsigned *cnt) {
+                                               const double *__restrict__ b64, float *r32, double *r2, double *part,
+                                               unsigned *cnt) {
   const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
-  const int ns = P.nsolve[p], c = pc_col(P, p);
-  double rr = 0.0, rz = 0.0;
+  const int ns = P.nsolve[p];
+  double rr = 0.0;
   for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
     double ax = 0.0;
     bool solve = true;
@@ -523,15 +694,10 @@ __global__ void __launch_bounds__(256) k_x_res(MeshView M, MxParams P, const dou
     }
     const size_t o = (size_t)g * PP + p;
     const double r = solve ? b64[o] - ax : 0.0;
-    const float rf = (float)r;
-    r32[o] = rf;
-    d32[o] = 0.0f;
-    const float z = P.pcf[(size_t)g * P.M + c] * rf;
-    p0[o] = z;
+    r32[o] = (float)r;
     rr += r * r;
-    rz += (double)rf * (double)z;
   }
-  chunk_reduce2(rr, rz, part, cnt, gridDim.x, r2, rho0);
+  chunk_reduce2(rr, 0.0, part, cnt, gridDim.x, r2, nullptr);
 }
 
 // u = x at element nodes, essential values from gess (global2local +
@@ -598,27 +764,50 @@ static int set_smem_attrs() {
                                (int)(4 * NN * MX_CH * sizeof(double))));
   SX_CUDA(cudaFuncSetAttribute(k_x_op64<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(3 * NN * MX_CH * sizeof(double))));
-  SX_CUDA(cudaFuncSetAttribute(k_x_op32<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(3 * NN * MX_CH * sizeof(float))));
+  SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(2 * NN * MX_CH * sizeof(float))));
   return SX_OK;
 }
 
-struct Launch {
-  const MeshView &M;
-  MixedWork &W;
-  cudaStream_t st;
-  int chunks() const { return W.PP / MX_CH; }
-  MxScalPtrs sp() const {
-    double *s = W.scal.p;
-    const int PP = W.PP;
-    return {s, s + PP, s + 2 * PP, s + 3 * PP, s + 4 * PP, s + 5 * PP};
+static MxScalPtrs scal_ptrs(const MixedWork &W) {
+  double *s = W.scal.p;
+  const size_t PP = W.PP;
+  MxScalPtrs r;
+  r.r2 = s;
+  r.b2 = s + PP;
+  for (int k = 0; k < 2; k++) {
+    r.gam[k] = s + (2 + k) * PP;
+    r.alpha[k] = s + (4 + k) * PP;
+    r.beta[k] = s + (6 + k) * PP;
   }
-};
+  return r;
+}
+
+static CgVecs cg_vecs(MixedWork &W) {
+  const MxScalPtrs s = scal_ptrs(W);
+  CgVecs v;
+  v.r[0] = W.r0.p;
+  v.r[1] = W.r1.p;
+  v.s[0] = W.s0.p;
+  v.s[1] = W.s1.p;
+  v.W[0] = W.W0.p;
+  v.W[1] = W.W1.p;
+  v.wi = W.wi.p;
+  v.p = W.p.p;
+  v.d = W.d.p;
+  v.x64 = W.x64.p;
+  for (int k = 0; k < 2; k++) {
+    v.gam[k] = s.gam[k];
+    v.alpha[k] = s.alpha[k];
+    v.beta[k] = s.beta[k];
+  }
+  return v;
+}
 
 static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream_t st, int *nl) {
-  const int npts = W.npts, nch = W.PP / MX_CH, NN = M.npnp;
+  const int nch = W.PP / MX_CH, NN = M.npnp;
   const MxParams P = W.prm;
-  const MxScalPtrs s = Launch{M, W, st}.sp();
+  const MxScalPtrs s = scal_ptrs(W);
   *nl = 0;
   if (any_bc) {
     k_x_ess<<<W.PP, 32, 0, st>>>(M, P);
@@ -626,37 +815,43 @@ static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream
   }
   const size_t sm64x4 = 4 * NN * MX_CH * sizeof(double);
   SX_NP_SWITCH_M(M.np, (k_x_constrain<N_><<<dim3(M.nel, nch), 256, sm64x4, st>>>(M, P, W.Ye64.p)));
-  k_x_rhs<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.x64.p, W.r32.p, W.d32.p, W.pA.p, s.b2,
-                                          s.rho0, W.part.p, W.cnt.p);
+  k_x_rhs<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.x64.p, W.r0.p, s.b2, W.part.p, W.cnt.p);
   *nl += 2;
-  (void)npts;
   SX_CUDA(cudaGetLastError());
   return SX_OK;
 }
 
+// One refinement round: the inner solve from r (r0 buffer, d = 0), x += d,
+// then the FP64 residual into r0 for the next round.
 static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStream_t st, int *nl) {
   const int nch = W.PP / MX_CH, NN = M.npnp;
   const MxParams P = W.prm;
-  const MxScalPtrs s = Launch{M, W, st}.sp();
-  double *rho[2] = {s.rho0, s.rho1}, *pq[2] = {s.pq0, s.pq1};
-  const size_t sm32 = 3 * NN * MX_CH * sizeof(float), sm64 = 3 * NN * MX_CH * sizeof(double);
+  const MxScalPtrs s = scal_ptrs(W);
+  const CgVecs V = cg_vecs(W);
+  const size_t smcg = 2 * NN * MX_CH * sizeof(float), sm64 = 3 * NN * MX_CH * sizeof(double);
+  const dim3 eg(M.nel, nch);
   *nl = 0;
+  SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, smcg, st>>>(M, P, V, 0, CG_INIT, W.part.p, W.cnt.p)));
   for (int it = 0; it < n_inner; it++) {
-    // p_it lives in buffer it&1 (p_0 written by the restart into pA)
-    float *pold = (it == 0) ? W.pA.p : ((it & 1) ? W.pA.p : W.pB.p);
-    float *pcur = (it & 1) ? W.pB.p : W.pA.p;
-    SX_NP_SWITCH_M(M.np, (k_x_op32<N_><<<dim3(M.nel, nch), 256, sm32, st>>>(
-                             M, P, W.r32.p, pold, pcur, W.q32.p, W.Yb32.p, rho[it & 1], rho[(it + 1) & 1],
-                             pq[it & 1], it, W.part.p, W.cnt.p)));
-    k_x_upd<<<dim3(W.G, nch), 256, 0, st>>>(M, P, pcur, W.q32.p, W.Yb32.p, W.d32.p, W.r32.p, W.x64.p,
-                                            rho[it & 1], pq[it & 1], rho[(it + 1) & 1],
-                                            it == n_inner - 1 ? 1 : 0, W.part.p, W.cnt.p);
-    *nl += 2;
+    const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
+    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, smcg, st>>>(M, P, V, it, mode, W.part.p, W.cnt.p)));
   }
-  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<dim3(M.nel, nch), 256, sm64, st>>>(M, P, W.x64.p, W.Ye64.p)));
-  k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r32.p, W.d32.p, W.pA.p, s.r2, s.rho0,
-                                          W.part.p, W.cnt.p);
-  *nl += 2;
+  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, 256, sm64, st>>>(M, P, W.x64.p, W.Ye64.p)));
+  k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r0.p, s.r2, W.part.p, W.cnt.p);
+  *nl = n_inner + 3;
+  SX_CUDA(cudaGetLastError());
+  return SX_OK;
+}
+
+int mixed_profile_iterations(const MeshView &M, MixedWork &W, int reps, cudaStream_t st) {
+  // iteration 1 reads what iteration 0 of the last round wrote
+  if (W.PP == 0 || W.n_inner < 2 || reps <= 0) return SX_ERR_ARG;
+  const int nch = W.PP / MX_CH, NN = M.npnp;
+  const CgVecs V = cg_vecs(W);
+  const size_t smcg = 2 * NN * MX_CH * sizeof(float);
+  for (int r = 0; r < reps; r++)
+    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, nch), N_ * 32, smcg, st>>>(M, W.prm, V, 1, CG_ITER, W.part.p,
+                                                                             W.cnt.p)));
   SX_CUDA(cudaGetLastError());
   return SX_OK;
 }
@@ -684,8 +879,8 @@ __global__ void k_x_pc(int npts, int M, const float *const *pcs, float *out) {
   for (int m = 0; m < M; m++) out[(size_t)g * M + m] = pcs[m][g];
 }
 
-static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int nyq,
-                 int num_modes, cudaStream_t st) {
+static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
+                 cudaStream_t st) {
   const int npts = M.nglobal + M.nel * M.nint;
   const int PP = ((nz + MX_CH - 1) / MX_CH) * MX_CH;
   const int Mc = std::max(1, num_modes);
@@ -697,54 +892,58 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
     SX_TRY(need(W.b64, n));
     SX_TRY(need(W.x64, n));
     SX_TRY(need(W.Ye64, (size_t)PP * M.nel * M.npnp));
-    SX_TRY(need(W.r32, n));
-    SX_TRY(need(W.d32, n));
-    SX_TRY(need(W.pA, n));
-    SX_TRY(need(W.pB, n));
-    SX_TRY(need(W.q32, n));
-    SX_TRY(need(W.Yb32, (size_t)PP * M.nel * M.next));
-    SX_TRY(need(W.scal, (size_t)6 * PP));
+    SX_TRY(need(W.r0, n));
+    SX_TRY(need(W.r1, n));
+    SX_TRY(need(W.s0, n));
+    SX_TRY(need(W.s1, n));
+    SX_TRY(need(W.p, n));
+    SX_TRY(need(W.d, n));
+    SX_TRY(need(W.wi, n));
+    SX_TRY(need(W.W0, (size_t)PP * M.nel * M.next));
+    SX_TRY(need(W.W1, (size_t)PP * M.nel * M.next));
+    SX_TRY(need(W.scal, (size_t)MX_NSCAL * PP));
     SX_TRY(need(W.hcon, (size_t)PP));
     SX_TRY(need(W.gess, (size_t)PP * M.nglobal));
     SX_TRY(need(W.nsolve, (size_t)PP));
+    SX_TRY(need(W.active, (size_t)PP));
     SX_TRY(need(W.pcf, (size_t)npts * Mc));
     SX_TRY(need(W.part, (size_t)PP * std::max(W.G, M.nel) * 2));
     if (W.cnt.n < (size_t)(PP / MX_CH)) {
       SX_TRY(W.cnt.alloc(PP / MX_CH));
       SX_TRY(W.cnt.zero(st));
     }
-    W.hscal.assign((size_t)6 * PP, 0.0);
+    W.hscal.assign((size_t)2 * PP, 0.0);
     W.PP = PP;
     W.npts = npts;
     W.M = Mc;
   }
-  // per-plane constants; planes without a system (Nyquist, padding) borrow
-  // the first group's
+  // per-plane constants; planes without a system here (Nyquist, padding,
+  // planes of other groups) are inactive and borrow the first group's
   std::vector<double> hc(PP, groups[0].sys->betak2 + groups[0].sys->lambda2);
-  std::vector<int> ns(PP, groups[0].sys->nsolve);
+  std::vector<int> ns(PP, groups[0].sys->nsolve), act(PP, 0);
   std::vector<const float *> pcs(Mc, groups[0].sys->pcf.p);
   for (const MxGroup &g : groups) {
     for (int q = 0; q < g.P; q++) {
       hc[g.plane0 + q] = g.sys->betak2 + g.sys->lambda2;
       ns[g.plane0 + q] = g.sys->nsolve;
+      act[g.plane0 + q] = 1;
     }
     if (g.mode < Mc) pcs[g.mode] = g.sys->pcf.p;
   }
   SX_CUDA(cudaMemcpyAsync(W.hcon.p, hc.data(), sizeof(double) * PP, cudaMemcpyHostToDevice, st));
   SX_CUDA(cudaMemcpyAsync(W.nsolve.p, ns.data(), sizeof(int) * PP, cudaMemcpyHostToDevice, st));
+  SX_CUDA(cudaMemcpyAsync(W.active.p, act.data(), sizeof(int) * PP, cudaMemcpyHostToDevice, st));
   DBuf<const float *> dp;
   SX_TRY(dp.upload_on(pcs.data(), pcs.size(), st));
   k_x_pc<<<(npts + 255) / 256, 256, 0, st>>>(npts, Mc, dp.p, W.pcf.p);
   SX_CUDA(cudaGetLastError());
   SX_CUDA(cudaStreamSynchronize(st));
-  (void)nyq;
   return SX_OK;
 }
 
-int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int nyq,
-                int num_modes, double *d_u, double *d_f, const double *d_bc, long long stride,
-                bool rebuild, double tol_rel, int max_refine, int n_inner, bool graphs, cudaStream_t st,
-                sx_solve_stats *stats) {
+int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
+                double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild, double tol_rel,
+                int max_refine, int n_inner, bool graphs, cudaStream_t st, sx_solve_stats *stats) {
   if (groups.empty()) return SX_OK;
   if (M.mixed) {
     set_error("mixed-precision form does not take Robin (mixed) boundary conditions");
@@ -755,14 +954,14 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     if (W.g_init) cudaGraphExecDestroy(W.g_init);
     if (W.g_round) cudaGraphExecDestroy(W.g_round);
     W.g_init = W.g_round = nullptr;
-    SX_TRY(setup(M, W, groups, nz, nyq, num_modes, st));
+    SX_TRY(setup(M, W, groups, nz, num_modes, st));
     int attr_rc = SX_OK;
     SX_NP_SWITCH_M(M.np, (attr_rc = set_smem_attrs<N_>()));
     SX_TRY(attr_rc);
     MxParams &P = W.prm;
     P.PP = W.PP;
     P.nz = nz;
-    P.nyq = nyq;
+    P.active = W.active.p;
     P.M = W.M;
     P.hcon = W.hcon.p;
     P.nsolve = W.nsolve.p;
@@ -795,11 +994,12 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     else
       SX_TRY(enqueue_round(M, W, n_inner, st, &W.launches_round));
     launches += W.launches_round;
-    SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(double) * 6 * PP, cudaMemcpyDeviceToHost, st));
+    // r2 and b2 lead the scalar block
+    SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(double) * 2 * PP, cudaMemcpyDeviceToHost, st));
     SX_CUDA(cudaStreamSynchronize(st));
     worst = 0.0;
     for (int p = 0; p < PP; p++) {
-      const double r2 = W.hscal[4 * PP + p], b2 = W.hscal[5 * PP + p];
+      const double r2 = W.hscal[p], b2 = W.hscal[PP + p];
       const double rel = b2 > 0.0 ? std::sqrt(std::max(r2, 0.0) / b2) : 0.0;
       if (!(rel == rel)) worst = INFINITY;  // NaN
       worst = std::max(worst, rel);

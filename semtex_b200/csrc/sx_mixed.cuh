@@ -13,7 +13,8 @@ constexpr int MX_CH = 32;  // planes per block chunk (one warp lane per plane)
 struct MxParams {
   int PP;               // padded plane count (multiple of MX_CH)
   int nz;               // real planes in the caller's arrays
-  int nyq;              // Nyquist plane (not solved) or -1
+  const int *active;    // [PP] 1 for planes this form solves (not the Nyquist
+                        // plane, padding, or planes routed to the direct path)
   int M;                // columns of the interleaved preconditioner (local modes)
   const double *hcon;   // [PP] lambda2 + betak2 of the plane's mode
   const int *nsolve;    // [PP]
@@ -26,17 +27,33 @@ struct MxParams {
   double *gess;         // [PP * nglobal] essential values, plane-major
 };
 
-// Per-plane scalars, each an array of PP doubles.
+// Per-plane scalars, each an array of PP doubles: residual and RHS norms
+// (read by the host between rounds), then the inner iteration's gamma,
+// alpha, beta in two slots (iteration parity).
+constexpr int MX_NSCAL = 8;
 struct MxScalPtrs {
-  double *rho0, *rho1, *pq0, *pq1, *r2, *b2;
+  double *r2, *b2, *gam[2], *alpha[2], *beta[2];
+};
+
+// Vectors of the FP32 inner iteration, plane-interleaved [npts][PP] unless
+// noted.  r and s alternate between two buffers by iteration parity (other
+// elements still read the old value of a shared node while its owner writes
+// the new one); p and d are read only by the node's owner and stay in place.
+struct CgVecs {
+  float *r[2], *s[2];
+  float *W[2];     // element boundary slots of A u, [nel][next][PP]
+  float *wi;       // A u at interior nodes, by global node
+  float *p, *d;
+  double *x64;
+  double *gam[2], *alpha[2], *beta[2];
 };
 
 struct MixedWork {
   int PP = 0, npts = 0, n_inner = 0, M = 0, G = 0;
   DBuf<double> hcon, b64, x64, Ye64, scal, part, gess;
-  DBuf<int> nsolve;
+  DBuf<int> nsolve, active;
   DBuf<unsigned> cnt;
-  DBuf<float> pcf, r32, d32, pA, pB, q32, Yb32;
+  DBuf<float> pcf, r0, r1, s0, s1, p, d, wi, W0, W1;
   cudaGraphExec_t g_init = nullptr, g_round = nullptr;
   int launches_init = 0, launches_round = 0;
   std::vector<double> hscal;
@@ -54,12 +71,18 @@ struct MxGroup {
   const System *sys;
 };
 
-// Run the batched mixed-precision solve of planes 0..nz-1 (plane 1 is the
-// Nyquist datum when nyq == 1).  Stops when every plane's FP64 relative
-// residual ||b - A x|| / ||b|| <= tol_rel or after max_refine rounds.
-int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int nyq,
-                int num_modes, double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild,
-                double tol_rel, int max_refine, int n_inner, bool graphs, cudaStream_t st,
-                sx_solve_stats *stats);
+// Run the batched mixed-precision solve of the planes of `groups` (nz
+// planes in the caller's arrays; the others -- the Nyquist plane, planes
+// solved by another path -- are neither read nor written).  Stops when every
+// plane's FP64 relative residual ||b - A x|| / ||b|| <= tol_rel or after
+// max_refine rounds.
+int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
+                double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild, double tol_rel,
+                int max_refine, int n_inner, bool graphs, cudaStream_t st, sx_solve_stats *stats);
+
+// Enqueue `reps` inner-iteration launches (k_cg, iteration 1) on the
+// workspace of the last mixed solve, for timing the kernel on its own.  The
+// workspace's iterates are left meaningless; the next solve starts afresh.
+int mixed_profile_iterations(const MeshView &M, MixedWork &W, int reps, cudaStream_t st);
 
 }  // namespace sx

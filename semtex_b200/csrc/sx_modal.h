@@ -12,6 +12,32 @@
 #include "sx_pcg.cuh"
 #include "sx_solve.cuh"
 
+namespace sx {
+
+// A batched FP64 direct solve of a set of plane groups: the job table, and
+// the kernel sequence captured once as a CUDA graph and replayed while the
+// arguments it was captured for stay the same.
+struct DirectBatch {
+  cudaGraphExec_t exec = nullptr;
+  const void *key[6] = {};  // u, f, bc, and the workspace buffers rhs, Fb, gess
+  int nz = 0, stride = 0;
+  std::vector<int> modes;  // local mode of each group, in job order
+  DBuf<Job> djobs;
+  std::vector<Job> jobs;   // host copy of the captured jobs
+  int C = 1, launches = 0; // band-sweep cluster size, kernels per solve
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    jobs.clear();
+    modes.clear();
+  }
+  ~DirectBatch() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+}  // namespace sx
+
 struct sx_modal_s {
   sx_mesh_s *mesh = nullptr;
   int base_mode = 0, num_modes = 0, method = SX_DIRECT;
@@ -24,21 +50,21 @@ struct sx_modal_s {
   size_t npad_max = 0;
   // host-pointer entries: device staging
   sx::DBuf<double> hu, hf, hbc;
-  // batched form: captured graph and the arguments it was captured for
+  // batched forms
   cudaStream_t own = nullptr;
   bool own_stream_external = false;
-  cudaGraphExec_t gexec = nullptr;
-  const void *gkey[3] = {nullptr, nullptr, nullptr};
-  int gnz = 0, gstride = 0, gprec = -1;
-  sx::DBuf<sx::Job> bjobs;
-  std::vector<sx::Job> gjobs;        // host copy of the captured jobs
-  int gC = 1, glaunches = 0;         // their band-sweep cluster size, kernel count
+  sx::DirectBatch fp64;              // SX_FP64: every mode
+  sx::DirectBatch hyb;               // SX_MIXED_FP32: the modes routed to the band solve
+  cudaStream_t aux = nullptr;        // runs `hyb` beside the FP32 iterations
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   sx::DBuf<int> dstatus;             // device status bits of the last solves
   // mixed-precision batched form
   sx::MixedWork mixed;
   const void *mkey[3] = {nullptr, nullptr, nullptr};
   int mnz = 0, mstride = 0;
+  std::vector<int> mmodes;           // local modes the FP32 iterations solve
   int n_inner = 12;                  // FP32 PCG iterations per refinement round
+  int mixed_route = 0;               // 0 auto, 1 FP32 CG only, 2 band solve where factored
   bool use_graphs = true;
   std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
   int forced_cluster = 0;

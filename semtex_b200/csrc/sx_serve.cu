@@ -42,6 +42,7 @@ uint64_t fnv(uint64_t h, const void *p, size_t n) {
 
 struct MeshCopy {
   int np = 0, nel = 0, nglobal = 0, nsolve = 0, nband = 0, nbound = 0;
+  double kratio = 0.0;  // stiffness / mass diagonal ratio (routes the mixed form)
   std::vector<double> x, y, bK, bC;
   std::vector<int> btog, bmask, be, bs, bk;
   uint64_t key = 0;
@@ -86,7 +87,8 @@ struct SysEntry {
 
 size_t mesh_estimate(const MeshCopy &m) {
   const size_t nn = (size_t)m.np * m.np, next = 4 * (m.np - 1);
-  return (size_t)m.nel * nn * (5 * 8 + 4 * 4 + 1) + (size_t)m.nel * next * 4 * 3 + (size_t)m.nglobal * 32 +
+  return (size_t)m.nel * nn * (5 * 8 + 4 * 4 + 16 + 1) + (size_t)m.nel * next * (4 * 3 + 16) +
+         (size_t)m.nglobal * 32 +
          (size_t)m.nbound * m.np * 8 + 4096;
 }
 
@@ -107,7 +109,7 @@ size_t work_estimate(const MeshCopy &m, int nz, int precision) {
   const size_t PP = ((nz + MX_CH - 1) / MX_CH) * MX_CH;
   size_t b = 2 * (size_t)nz * m.nel * nn * 8 + (size_t)nz * std::max(m.nbound, 1) * m.np * 8;  // I/O
   if (precision == SX_MIXED_FP32)
-    b += PP * npts * (2 * 8 + 6 * 4) + PP * m.nel * nn * 8 + PP * m.nel * next * 4 + PP * m.nglobal * 8 +
+    b += PP * npts * (2 * 8 + 9 * 4) + PP * m.nel * nn * 8 + 2 * PP * m.nel * next * 4 + PP * m.nglobal * 8 +
          npts * (nz / 2 + 1) * 4;
   else
     b += (size_t)nz * ((m.nsolve + NB) * 8 + (size_t)m.nel * next * 8 + (size_t)m.nglobal * 8);
@@ -134,6 +136,16 @@ struct sx_server_s {
   std::vector<double> latencies;
   sx_server_stats st{};
 
+  // System kind of one mode: SX_DIRECT for SX_FP64; for SX_MIXED_FP32 the
+  // FP32 iterations (SX_JACPCG) unless the band Cholesky is the cheaper
+  // route for this conditioning (then the mode is factored and solved by it).
+  int mode_kind(const MeshCopy &m, double lam, double bk2) const {
+    if (cfg.precision == SX_FP64) return SX_DIRECT;
+    return band_cheaper(m.np, m.nel, m.nglobal, m.nsolve, m.nband, m.kratio, lam + bk2, cfg.inner_iters,
+                        cfg.tol_rel)
+               ? SX_DIRECT
+               : SX_JACPCG;
+  }
   bool admissible(Req *r, size_t &need);
   void evict_for(size_t need, uint64_t keep_mesh);
   void worker(int slot);
@@ -142,10 +154,10 @@ struct sx_server_s {
 
 // Memory this request still needs beyond what is cached (caller holds mu).
 bool sx_server_s::admissible(Req *r, size_t &need) {
-  const int kind = cfg.precision == SX_FP64 ? SX_DIRECT : SX_JACPCG;
   need = work_estimate(r->mesh, r->nz, cfg.precision);
   if (!meshes.count(r->mesh.key)) need += mesh_estimate(r->mesh);
   for (int l = 0; l < r->num_modes; l++) {
+    const int kind = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
     uint64_t a, b;
     std::memcpy(&a, &r->lam[l], 8);
     std::memcpy(&b, &r->bk2[l], 8);
@@ -185,7 +197,6 @@ void sx_server_s::evict_for(size_t need, uint64_t keep_mesh) {
 
 int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &df, DBuf<double> &dbc,
                        cudaStream_t stream) {
-  const int kind = cfg.precision == SX_FP64 ? SX_DIRECT : SX_JACPCG;
   sx_mesh_s *mesh = nullptr;
   std::vector<std::shared_ptr<System>> sys(r->num_modes);
   std::vector<std::tuple<uint64_t, uint64_t, uint64_t, int>> keys(r->num_modes);
@@ -218,6 +229,7 @@ int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &d
     }
     std::vector<System *> to_factor;
     for (int l = 0; l < r->num_modes; l++) {
+      const int kind = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
       uint64_t a, b;
       std::memcpy(&a, &r->lam[l], 8);
       std::memcpy(&b, &r->bk2[l], 8);
@@ -258,8 +270,7 @@ int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &d
     }
     SX_TRY(factor_batch(to_factor, stream));
   }
-  const int method = kind;
-  ws.rebind(mesh, r->base_mode, r->num_modes, method, sys);
+  ws.rebind(mesh, r->base_mode, r->num_modes, cfg.precision == SX_FP64 ? SX_DIRECT : SX_MIXED, sys);
   ws.n_inner = cfg.inner_iters;
   const size_t n = (size_t)r->nz * r->stride;
   if (du.n < n) SX_TRY(du.alloc(n));
@@ -413,6 +424,10 @@ extern "C" int sx_server_submit(sx_server s, const sx_request *q, unsigned long 
   h = fnv(h, m.bK.data(), m.bK.size() * 8);
   h = fnv(h, m.bC.data(), m.bC.size() * 8);
   m.key = h;
+  {
+    const int rk = mesh_kratio(&d, &m.kratio);
+    if (rk != SX_OK) return rk;
+  }
   r->base_mode = q->base_mode;
   r->num_modes = q->num_modes;
   r->nz = q->nz;
@@ -424,9 +439,8 @@ extern "C" int sx_server_submit(sx_server s, const sx_request *q, unsigned long 
   r->u = q->u;
   r->t_submit = Clock::now();
   // a request that cannot fit even in an empty device is refused up front
-  const int kind = s->cfg.precision == SX_FP64 ? SX_DIRECT : SX_JACPCG;
-  const size_t alone = work_estimate(m, r->nz, s->cfg.precision) + mesh_estimate(m) +
-                       (size_t)r->num_modes * system_estimate(m, kind);
+  size_t alone = work_estimate(m, r->nz, s->cfg.precision) + mesh_estimate(m);
+  for (int l = 0; l < r->num_modes; l++) alone += system_estimate(m, s->mode_kind(m, r->lam[l], r->bk2[l]));
   std::lock_guard<std::mutex> lk(s->mu);
   s->st.submitted++;
   if (alone > s->cfg.hbm_budget) {

@@ -83,8 +83,9 @@ def test_mixed_matches_oracle(sx, torch, lam, inner):
     from semtex_b200.workloads import small_channel
     w = small_channel(nx=6, ny=5, np_=9, nz=6, lam=lam, seed=5)
     _, S = _setup(sx, w)
-    S.tune(inner_iters=inner)
+    S.tune(inner_iters=inner, mixed_route=sx.ROUTE_CG)
     um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32, tol=1e-12)
+    assert st["planes_direct"] == 0
     assert st["final_rel_residual"] <= 1e-12
     uo, _ = solve_planes(OracleMesh(w.mesh), 0.0, 1.0, w.forcing, None,
                          lambda2_per_mode=w.lambda2)
@@ -99,7 +100,7 @@ def test_mixed_regress_goldens(sx, torch, name):
     from semtex_b200.workloads import Workload
     w = Workload(name, m, 1, 0.0, np.array([p["lambda2"]]), np.array([0.0]), f)
     _, S = _setup(sx, w)
-    S.tune(inner_iters=200)
+    S.tune(inner_iters=200, mixed_route=sx.ROUTE_CG)
     um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32, tol=1e-13, bc=bc)
     uo, _ = solve_planes(OracleMesh(m), p["lambda2"], 0.0, f, bc)
     l2, mx = rel_errs(um, uo)
@@ -113,9 +114,45 @@ def test_mixed_deterministic(sx, torch):
     from semtex_b200.workloads import small_channel
     w = small_channel(nx=6, ny=6, np_=7, nz=8, lam=1e5, seed=9)
     _, S = _setup(sx, w)
+    S.tune(mixed_route=sx.ROUTE_CG)
     a, _ = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
     b, _ = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
     assert np.array_equal(a, b)
+
+
+def test_mixed_route_band_equals_fp64(sx, torch):
+    """Modes routed to the band Cholesky run the batched FP64 form's kernels:
+    their planes equal the FP64 form's bit for bit."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=8, ny=8, np_=9, nz=12, lam=1e6, seed=11)
+    _, S = _setup(sx, w)
+    ub, _ = _run_device(torch, S, w, batched=True)
+    S.tune(mixed_route=sx.ROUTE_BAND)
+    um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
+    sp = solved_planes(w.nz)
+    assert st["planes_direct"] == len(sp) == st["planes_solved"]
+    assert np.array_equal(um[sp], ub[sp])
+
+
+@pytest.mark.parametrize("method", ["direct", "auto"])
+def test_mixed_hybrid_route_vs_oracle(sx, torch, method):
+    """lambda2 from 1e-2 to 1e6 across the modes: the ill-conditioned modes
+    go to the FP64 band Cholesky, the others to the FP32 iterations, both in
+    one call; every plane meets the 1e-10 bar against the oracle."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=10, ny=8, np_=9, nz=16, lam=1e6, seed=13)
+    w.lambda2 = np.logspace(-2, 6, w.num_modes)
+    mesh = sx.Mesh(w.mesh)
+    S = sx.ModalMatrixSys(mesh, num_modes=w.num_modes, method=sx.DIRECT if method == "direct" else sx.AUTO,
+                          lambda2_modes=w.lambda2, betak2_modes=w.betak2)
+    um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32, tol=1e-12)
+    sp = solved_planes(w.nz)
+    assert 0 < st["planes_direct"] < len(sp), st
+    assert st["planes_solved"] == len(sp)
+    uo, _ = solve_planes(OracleMesh(w.mesh), 0.0, 1.0, w.forcing, None, lambda2_per_mode=w.lambda2)
+    for p in sp:
+        l2, mx = rel_errs(um[p], uo[p])
+        assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (p, l2, mx, st)
 
 
 def test_batched_host_entry(sx, torch):

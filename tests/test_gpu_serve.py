@@ -37,16 +37,28 @@ def _requests():
     return out
 
 
+CFG = dict(precision=None, tol_rel=1e-12, max_refine=30, inner_iters=12)
+
+
+def _cfg(sx):
+    return dict(CFG, precision=sx.MIXED_FP32)
+
+
 def _alone(sx, m, lam, bk2, f):
-    S = sx.ModalMatrixSys(sx.Mesh(m), num_modes=len(lam), method=sx.JACPCG, lambda2_modes=lam,
-                          betak2_modes=bk2)
-    return S.solve_batched_host(f, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30)
+    """The request served by itself: a fresh one-slot server, same settings."""
+    srv = sx.Server(slots=1, **_cfg(sx))
+    try:
+        status, _, u = srv.wait(srv.submit(m, lam, bk2, f), timeout_s=120.0)
+    finally:
+        srv.close()
+    assert status in (sx.OK, sx.WARN_STEP_LIMIT)
+    return u
 
 
 def test_mix_equals_alone_and_oracle(sx):
     reqs = _requests()
     alone = [_alone(sx, *r) for r in reqs]
-    srv = sx.Server(slots=3, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30, inner_iters=12)
+    srv = sx.Server(slots=3, **_cfg(sx))
     try:
         ids = [srv.submit(*r) for r in reqs]
         res = [srv.wait(i, timeout_s=120.0) for i in ids]
@@ -97,3 +109,24 @@ def test_capacity_rejection(sx):
         assert srv.stats()["rejected"] == 1
     finally:
         srv.close()
+
+
+def test_mixed_server_routes_ill_conditioned_modes(sx):
+    """A near-Poisson request (lambda2 = 1e-2): the mixed server factors it
+    and solves it by the FP64 band Cholesky, within 1e-10 of the oracle."""
+    from semtex_b200.mesh import rect_mesh
+    from semtex_b200.workloads import fourier_forcing
+    from oracle.oracle import OracleMesh, solve_planes
+    m = rect_mesh(6, 5, 8, 0.0, 1.0, 0.0, 1.0)
+    lam = np.array([1e-2, 1e-2])
+    bk2 = np.array([0.0, 1.0])
+    f = fourier_forcing(m, 4, np.random.default_rng(7))
+    srv = sx.Server(slots=1, **_cfg(sx))
+    try:
+        status, _, u = srv.wait(srv.submit(m, lam, bk2, f), timeout_s=120.0)
+    finally:
+        srv.close()
+    assert status == sx.OK
+    uo, _ = solve_planes(OracleMesh(m), 0.0, 1.0, f, None, lambda2_per_mode=lam)
+    for p in (0, 2, 3):
+        assert np.linalg.norm(u[p] - uo[p]) <= TOL * np.linalg.norm(uo[p])
