@@ -421,8 +421,57 @@ def run_ours(args, rank, world):
         l2a, mxa = rel_err(u_batched[2], sols[0])
         l2b, mxb = rel_err(u_batched[3], sols[1])
         line["batched_fp64"]["rel_err_vs_oracle_mode1"] = [max(l2a, l2b), max(mxa, mxb)]
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_serving(n_requests, check_oracle=True):
+    """The serving loop on a bounded sample of the mixed-size request stream
+    (config 4): requests are submitted at their Poisson arrival times
+    (2000/s) to a mixed-precision server with 4 slots; latency is submit to
+    result on the host, as the server measures it.  The smallest requests
+    are checked against the oracle's FP64 direct solve."""
+    import semtex_b200 as sx
+    from semtex_b200.workloads import serving_trace
+    t0 = time.perf_counter()
+    trace = serving_trace(n_requests)
+    prep_s = time.perf_counter() - t0
+    srv = sx.Server(slots=4, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30, inner_iters=12)
+    try:
+        ids = []
+        start = time.perf_counter()
+        for r in trace:
+            while time.perf_counter() - start < r.t_arrival:
+                pass
+            ids.append(srv.submit(r.mesh, r.lambda2, r.betak2, r.forcing))
+        res = [srv.wait(i, timeout_s=600.0) for i in ids]
+        makespan = time.perf_counter() - start
+        st = srv.stats()
+    finally:
+        srv.close()
+    lat = np.array([lt for _, lt, _ in res])
+    ok = sum(1 for s, _, _ in res if s == sx.OK)
+    dofs = sum(r.dof_solves for r in trace)
+    out = {"requests": n_requests, "trace": "cfg4: E_x,E_y~U[2,64], N~U{4..10}, modes~U[1,64], "
+                                            "lambda2~logU[1e-2,1e4], Poisson 2000/s, seed 4",
+           "slots": 4, "precision": "mixed (FP32 CG / FP64 band per mode, FP64 refinement)",
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "mean_ms": float(lat.mean()), "makespan_s": makespan,
+           "throughput_dof_solves_per_s": dofs / makespan, "requests_per_s": n_requests / makespan,
+           "converged_to_1e-12": ok, "mesh_hits": st["mesh_hits"], "system_misses": st["system_misses"],
+           "evictions": st["evictions"], "host_prep_s_untimed": prep_s}
+    if check_oracle:
+        from oracle.oracle import OracleMesh, solve_planes
+        worst = 0.0
+        for k in sorted(range(n_requests), key=lambda k: trace[k].dof_solves)[:3]:
+            r, u = trace[k], res[k][2]
+            uo, _ = solve_planes(OracleMesh(r.mesh), 0.0, 1.0, r.forcing, None, lambda2_per_mode=r.lambda2)
+            sp = [0] + list(range(2, r.nz)) if r.nz > 1 else [0]
+            worst = max(worst, rel_err(u[sp], uo[sp])[0])
+        out["rel_err_vs_oracle_3_smallest"] = worst
+    return out
 
 
 def run_profile(args):
@@ -471,6 +520,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--serve-requests", type=int, default=32,
+                    help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
     ap.add_argument("--profile", choices=["band", "mixed"], default=None,

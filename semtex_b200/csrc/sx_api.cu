@@ -97,9 +97,12 @@ int modal_populate(sx_modal_s &M, const double *lam, const double *bk2, const Sy
     int kind = M.method;
     if (M.method == SX_MIXED) kind = (mode == 0) ? SX_DIRECT : SX_JACPCG;  // src/matrix.cpp:93-96
     if (M.method == SX_AUTO) {
+      // a modal system is built to be solved many times (a DNS run solves
+      // it every timestep): the factorisation is charged over 100 solves;
+      // 1e-12 in at most 20 rounds is the batched form's default target
       const sx_mesh_s &Mh = *M.mesh;
       kind = band_cheaper(Mh.np, Mh.nel, Mh.nglobal, Mh.nsolve, Mh.nband, Mh.kratio, lam[l] + bk2[l], M.n_inner,
-                          1e-12)
+                          1e-12, 20, 100.0)
                  ? SX_DIRECT
                  : SX_JACPCG;
     }
@@ -448,29 +451,35 @@ static int direct_batched(sx_modal_s *s, DirectBatch &B, const std::vector<Group
 }
 
 bool sx::band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon,
-                      int n_inner, double tol_rel) {
+                      int n_inner, double tol_rel, int max_refine, double reuse) {
   if (!(hcon > 0.0)) return true;
   const int nn = np * np, next = 4 * (np - 1), nint = nn - next;
-  const double per_round = std::max((double)n_inner, 5.3 * std::sqrt(1.0 + kratio / hcon));
-  const double rounds = std::max(1.0, std::ceil(std::log(std::max(tol_rel, 1e-15)) / std::log(1e-7)));
+  n_inner = std::max(n_inner, 1);
+  const double decades = std::max(1.0, std::log(std::max(tol_rel, 1e-15)) / std::log(1e-7));
+  const double iters = 5.3 * std::sqrt(1.0 + kratio / hcon) * decades;
+  const double rounds = std::max(std::ceil(decades), std::ceil(iters / n_inner));
+  if (rounds > max_refine) return true;
   const double npts = nglobal + (double)nel * nint;
-  const double cg = per_round * rounds * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn);
-  const double band =
-      (2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0) /
-      2.0;
-  return cg > 3.0 * band;
+  const double cg_s =
+      rounds * n_inner * std::max(2.0 * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn) / 2.1e12, 12e-6);
+  const double band_bytes =
+      2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0;
+  const double nblk = std::ceil(nsolve / (double)NB);
+  const double band_s = std::max(band_bytes / 1.9e12, 2.0 * nblk * 7.7e-6);
+  const double factor_s = reuse > 0.0 ? nsolve * (double)nband * nband / 3.9e12 / reuse : 0.0;
+  return cg_s > band_s + factor_s;
 }
 
 // Route of a mode in the mixed-precision form: true = the FP64 band
 // Cholesky (the mode must be factored), false = FP32 CG inside FP64
 // refinement.
-static bool route_direct(const sx_modal_s &s, const System &S, double tol_rel) {
+static bool route_direct(const sx_modal_s &s, const System &S, double tol_rel, int max_refine) {
   if (S.method != SX_DIRECT || !S.tiles.p) return false;
   if (s.mixed_route == 1) return false;
   if (s.mixed_route == 2) return true;
   const sx_mesh_s &M = *s.mesh;
   return band_cheaper(M.np, M.nel, M.nglobal, S.nsolve, M.nband, M.kratio, S.lambda2 + S.betak2, s.n_inner,
-                      tol_rel);
+                      tol_rel, max_refine, 0.0);
 }
 
 // Mixed-precision batched form (sx_mixed.cu): the modes routed to the FP32
@@ -489,7 +498,7 @@ static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const doubl
   std::vector<int> jmodes;
   for (auto &g : groups) {
     const System *S = s->sys[g.mode].get();
-    if (route_direct(*s, *S, tol_rel)) {
+    if (route_direct(*s, *S, tol_rel, max_refine)) {
       gd.push_back(g);
     } else {
       mg.push_back({g.mode, g.plane0, g.P, S});

@@ -212,15 +212,23 @@ int system_band_export(const System &S, double *ab);  // LAPACK band, host
 // sx_mesh_s::kratio of a mesh description, from host geometry alone.
 int mesh_kratio(const sx_mesh_desc *d, double *out);
 
-// Whether the FP64 band Cholesky is the cheaper route, in streamed bytes,
-// for a mode with Helmholtz constant hcon solved to tol_rel: Jacobi-CG takes
-// about 5.3 sqrt(1 + kratio / hcon) iterations per 1e-7 of residual
-// (measured with the oracle over lambda2 = 1..1e6 at N = 8 and 10), each
-// streaming 4 (8 npts + 2 nel np^2) bytes per plane; the band solve streams
-// its factor twice plus the condensation matrices, at about a third of the
-// CG kernel's bandwidth (its sweeps are latency-bound), hence the factor 3.
+// Whether the FP64 band Cholesky is the better route for one mode (two
+// planes) of the mixed-precision form with Helmholtz constant hcon, solved
+// to tol_rel with n_inner FP32 iterations per refinement round and at most
+// max_refine rounds.  Predicted times on B200:
+//   CG:     Jacobi-CG takes about 5.3 sqrt(1 + kratio / hcon) iterations per
+//           1e-7 of residual (measured with the oracle over lambda2 = 1..1e6,
+//           N = 8 and 10); each iteration streams 4 (8 npts + 2 nel np^2)
+//           bytes per plane at 2.1 TB/s (k_cg, measured), 12 us at least
+//   band:   the factor twice plus hbi/hii at 1.9 TB/s (k_band_sweep with 32
+//           systems, measured), or 2 nblk block steps of 7.7 us each when
+//           few systems run (its serial chain), whichever is longer
+//   factor: nsolve nband^2 flops at 3.9 TFLOP/s (config-2 set-up,
+//           measured), divided by `reuse`, the solves expected per factored
+//           system (0: already factored, no cost).
+// A mode whose CG would need more than max_refine rounds goes to the band.
 bool band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon, int n_inner,
-                  double tol_rel);
+                  double tol_rel, int max_refine, double reuse);
 
 // Solve workspace for up to `planes` planes of one system.
 struct Work {

@@ -62,6 +62,7 @@ struct Req {
   MeshCopy mesh;
   int base_mode = 0, num_modes = 0, nz = 0, stride = 0;
   std::vector<double> lam, bk2, f, bc;
+  std::vector<int> kinds;  // per mode: system kind, fixed when admitted
   double *u = nullptr;
   Clock::time_point t_submit;
   size_t reserve = 0;  // bytes reserved while in flight
@@ -136,13 +137,19 @@ struct sx_server_s {
   std::vector<double> latencies;
   sx_server_stats st{};
 
-  // System kind of one mode: SX_DIRECT for SX_FP64; for SX_MIXED_FP32 the
-  // FP32 iterations (SX_JACPCG) unless the band Cholesky is the cheaper
-  // route for this conditioning (then the mode is factored and solved by it).
+  // System kind of one mode (caller holds mu): SX_DIRECT for SX_FP64.  For
+  // SX_MIXED_FP32 a cached factor is used when there is one; otherwise the
+  // mode is factored only when the band Cholesky, with its factorisation
+  // charged to this request alone, beats the FP32 iterations (or when those
+  // would not converge within max_refine rounds).
   int mode_kind(const MeshCopy &m, double lam, double bk2) const {
     if (cfg.precision == SX_FP64) return SX_DIRECT;
+    uint64_t a, b;
+    std::memcpy(&a, &lam, 8);
+    std::memcpy(&b, &bk2, 8);
+    if (systems.count(std::make_tuple(m.key, a, b, (int)SX_DIRECT))) return SX_DIRECT;
     return band_cheaper(m.np, m.nel, m.nglobal, m.nsolve, m.nband, m.kratio, lam + bk2, cfg.inner_iters,
-                        cfg.tol_rel)
+                        cfg.tol_rel, cfg.max_refine, 1.0)
                ? SX_DIRECT
                : SX_JACPCG;
   }
@@ -156,8 +163,9 @@ struct sx_server_s {
 bool sx_server_s::admissible(Req *r, size_t &need) {
   need = work_estimate(r->mesh, r->nz, cfg.precision);
   if (!meshes.count(r->mesh.key)) need += mesh_estimate(r->mesh);
+  r->kinds.resize(r->num_modes);
   for (int l = 0; l < r->num_modes; l++) {
-    const int kind = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
+    const int kind = r->kinds[l] = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
     uint64_t a, b;
     std::memcpy(&a, &r->lam[l], 8);
     std::memcpy(&b, &r->bk2[l], 8);
@@ -229,7 +237,7 @@ int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &d
     }
     std::vector<System *> to_factor;
     for (int l = 0; l < r->num_modes; l++) {
-      const int kind = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
+      const int kind = r->kinds[l];
       uint64_t a, b;
       std::memcpy(&a, &r->lam[l], 8);
       std::memcpy(&b, &r->bk2[l], 8);
@@ -439,9 +447,9 @@ extern "C" int sx_server_submit(sx_server s, const sx_request *q, unsigned long 
   r->u = q->u;
   r->t_submit = Clock::now();
   // a request that cannot fit even in an empty device is refused up front
+  std::lock_guard<std::mutex> lk(s->mu);
   size_t alone = work_estimate(m, r->nz, s->cfg.precision) + mesh_estimate(m);
   for (int l = 0; l < r->num_modes; l++) alone += system_estimate(m, s->mode_kind(m, r->lam[l], r->bk2[l]));
-  std::lock_guard<std::mutex> lk(s->mu);
   s->st.submitted++;
   if (alone > s->cfg.hbm_budget) {
     s->st.rejected++;

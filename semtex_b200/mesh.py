@@ -93,26 +93,26 @@ def element_nodes(np_: int, z: np.ndarray, vx, vy):
         sp = z if s < 2 else -z[::-1]
         px = x1 + (x2 - x1) * 0.5 * (sp + 1.0)
         py = y1 + (y2 - y1) * 0.5 * (sp + 1.0)
-        for i in range(nm):
-            if s == 0:
-                idx = (0, i)
-            elif s == 1:
-                idx = (i, nm)
-            elif s == 2:
-                idx = (nm, nm - i)
-            else:
-                idx = (nm - i, 0)
-            x[idx], y[idx] = px[i], py[i]
-    zr = zs = z
-    for i in range(1, nm):
-        for j in range(1, nm):
-            for a in (x, y):
-                a[i, j] = (0.50 * ((1.0 - zr[j]) * a[i, 0] + (1.0 + zr[j]) * a[i, nm]
-                                   + (1.0 - zs[i]) * a[0, j] + (1.0 + zs[i]) * a[nm, j])
-                           - 0.25 * ((1.0 - zr[j]) * (1.0 - zs[i]) * a[0, 0]
-                                     + (1.0 - zr[j]) * (1.0 + zs[i]) * a[nm, 0]
-                                     + (1.0 - zs[i]) * (1.0 + zr[j]) * a[0, nm]
-                                     + (1.0 + zs[i]) * (1.0 + zr[j]) * a[nm, nm]))
+        # side s's first nm points, CCW from its start vertex
+        if s == 0:
+            idx = (0, slice(0, nm))
+        elif s == 1:
+            idx = (slice(0, nm), nm)
+        elif s == 2:
+            idx = (nm, slice(nm, 0, -1))
+        else:
+            idx = (slice(nm, 0, -1), 0)
+        x[idx], y[idx] = px[:nm], py[:nm]
+    # Coons interior, node by node the same arithmetic as a scalar loop
+    zr = z[None, 1:nm]  # along j
+    zs = z[1:nm, None]  # along i
+    for a in (x, y):
+        a[1:nm, 1:nm] = (0.50 * ((1.0 - zr) * a[1:nm, 0:1] + (1.0 + zr) * a[1:nm, nm:nm + 1]
+                                 + (1.0 - zs) * a[0:1, 1:nm] + (1.0 + zs) * a[nm:nm + 1, 1:nm])
+                         - 0.25 * ((1.0 - zr) * (1.0 - zs) * a[0, 0]
+                                   + (1.0 - zr) * (1.0 + zs) * a[nm, 0]
+                                   + (1.0 - zs) * (1.0 + zr) * a[0, nm]
+                                   + (1.0 + zs) * (1.0 + zr) * a[nm, nm]))
     return x, y
 
 

@@ -126,6 +126,47 @@ def config3(nx=64, ny=64, np_=11, nz=128, seed=3):
                     seed=seed, info={"jitter": 0.20})
 
 
+@dataclass
+class ServeRequest:
+    t_arrival: float             # seconds after the first arrival
+    mesh: QuadMesh
+    lambda2: np.ndarray          # per mode
+    betak2: np.ndarray           # per mode, k^2
+    forcing: np.ndarray          # (nz, nplane)
+
+    @property
+    def nz(self):
+        return self.forcing.shape[0]
+
+    @property
+    def dof_solves(self):
+        """Unique nodes per plane x planes solved (Nyquist excluded)."""
+        return self.mesh.n_unique * (1 if self.nz == 1 else self.nz - 1)
+
+
+def serving_trace(n_requests, seed=4, rate=2000.0):
+    """Mixed-size request stream (config 4): Poisson arrivals at `rate`/s;
+    each request a straight-sided E_x x E_y quad mesh of [0,1]^2 with E_x,
+    E_y uniform in [2, 64], order N uniform in {4..10}, a mode count uniform
+    in [1, 64], lambda2 log-uniform in [1e-2, 1e4] (plus k^2 per mode, beta =
+    1), seeded Gaussian Fourier forcing, Dirichlet on every side.  The first
+    `n_requests` requests of the seeded stream."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(n_requests):
+        ex, ey = (int(v) for v in rng.integers(2, 65, size=2))
+        order = int(rng.integers(4, 11))
+        modes = int(rng.integers(1, 65))
+        lam = float(np.exp(rng.uniform(np.log(1e-2), np.log(1e4))))
+        m = rect_mesh(ex, ey, order + 1, 0.0, 1.0, 0.0, 1.0)
+        nz = 1 if modes == 1 else 2 * modes
+        f = fourier_forcing(m, nz, rng)
+        out.append(ServeRequest(t, m, np.full(modes, lam), np.arange(modes, dtype=np.float64) ** 2, f))
+        t += float(rng.exponential(1.0 / rate))
+    return out
+
+
 def small_channel(nx=8, ny=6, np_=9, nz=16, lam=1e6, seed=7, jitter=0.15):
     """Small config-2-shaped case for parity tests."""
     m = _jittered_channel(nx, ny, np_, jitter, seed)
