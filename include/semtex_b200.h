@@ -198,7 +198,9 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
 
 /* Schedule knobs of the batched forms (no reference counterpart), set by
  * the autotuner or by hand; value <= 0 restores the default.
- *   SX_TUNE_INNER_ITERS   FP32 PCG iterations per refinement round (12)
+ *   SX_TUNE_INNER_ITERS   FP32 PCG iterations per refinement round, at
+ *                         least (12); raised per call to what the
+ *                         worst-conditioned FP32-routed mode needs
  *   SX_TUNE_BAND_CLUSTER  CTAs per cluster in the band sweeps (auto)
  *   SX_TUNE_MIXED_ROUTE   how SX_MIXED_FP32 solves each mode: 0 = by cost
  *                         (default: modes whose Jacobi-CG would stream more

@@ -450,22 +450,24 @@ static int direct_batched(sx_modal_s *s, DirectBatch &B, const std::vector<Group
   return SX_OK;
 }
 
+int sx::cg_round_iters(double kratio, double hcon) {
+  if (!(hcon > 0.0)) return CG_ROUND_CAP + 1;
+  const double n = std::ceil(4.5 * std::sqrt(1.0 + kratio / hcon));
+  return n > CG_ROUND_CAP ? CG_ROUND_CAP + 1 : (int)n;
+}
+
 bool sx::band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon,
                       int n_inner, double tol_rel, int max_refine, double reuse) {
-  if (!(hcon > 0.0)) return true;
+  const int per_round = std::max(std::max(n_inner, 1), cg_round_iters(kratio, hcon));
+  if (per_round > CG_ROUND_CAP) return true;
   const int nn = np * np, next = 4 * (np - 1), nint = nn - next;
-  n_inner = std::max(n_inner, 1);
-  const double decades = std::max(1.0, std::log(std::max(tol_rel, 1e-15)) / std::log(1e-7));
-  const double iters = 5.3 * std::sqrt(1.0 + kratio / hcon) * decades;
-  const double rounds = std::max(std::ceil(decades), std::ceil(iters / n_inner));
+  const double rounds = std::max(1.0, std::ceil(-std::log10(std::max(tol_rel, 1e-15)) / 6.0));
   if (rounds > max_refine) return true;
   const double npts = nglobal + (double)nel * nint;
-  const double cg_s =
-      rounds * n_inner * std::max(2.0 * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn) / 2.1e12, 12e-6);
-  const double band_bytes =
-      2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0;
-  const double nblk = std::ceil(nsolve / (double)NB);
-  const double band_s = std::max(band_bytes / 1.9e12, 2.0 * nblk * 7.7e-6);
+  const double cg_s = rounds * per_round * 2.0 * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn) / 2.1e12;
+  const double band_s =
+      (2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0) /
+      1.9e12;
   const double factor_s = reuse > 0.0 ? nsolve * (double)nband * nband / 3.9e12 / reuse : 0.0;
   return cg_s > band_s + factor_s;
 }
@@ -519,11 +521,20 @@ static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const doubl
   sx_solve_stats loc{};
   int rc = SX_OK;
   if (!mg.empty()) {
+    // iterations per round: the knob, raised to what the worst-conditioned
+    // mode needs for a 1e-6 cut per round (a restarted CG round that stops
+    // short stalls the refinement)
+    int n_inner = std::max(s->n_inner, 1);
+    for (const MxGroup &g : mg)
+      n_inner = std::max(n_inner, std::min(CG_ROUND_CAP, cg_round_iters(s->mesh->kratio,
+                                                                         g.sys->lambda2 + g.sys->betak2)));
     const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
-                           s->mstride == plane_stride && s->mixed.n_inner == s->n_inner && s->mmodes == jmodes);
+                           s->mstride == plane_stride && s->mixed.n_inner == n_inner && s->mmodes == jmodes &&
+                           s->mixed.status == s->dstatus.p);
+    s->mixed.status = s->dstatus.p;
     const MeshView M = s->mesh->view();
     rc = mixed_solve(M, s->mixed, mg, nz, s->num_modes, d_u, d_f, d_bc, plane_stride, rebuild, tol_rel,
-                     max_refine, s->n_inner, s->use_graphs, st, &loc);
+                     max_refine, n_inner, s->use_graphs, st, &loc);
     if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
       s->mkey[0] = d_u;
       s->mkey[1] = d_f;

@@ -138,7 +138,9 @@ struct MeshView {
   const int *g2e_last;                   // nglobal: last (e*next+i) writing node (local2global)
   const int4 *g2e4;                      // nglobal: first 4 CSR entries, -1 padded, .w = -2 if more
   const unsigned long long *owner;       // nel: bit a set when element e is node btog[e][a]'s last writer
-  const int4 *e2w4;                      // nel*next: g2e4 of node btog[e][a] (the gather list per slot)
+  const int4 *e2w4;                      // nel*next: gather list of node btog[e][a], in CSR order, as
+                                         // (element << 8 | tensor node) of its first four holders,
+                                         // -1 padded, .w = -2 when it has more (walk the CSR)
   const float4 *Gf;                      // nel*npnp: (Q1, Q2, Q3, Q4) in FP32, tensor order
   const int *pmap;                       // npnp: edge-map slot of tensor node t (inverse of emap)
   int nbound;
@@ -212,21 +214,30 @@ int system_band_export(const System &S, double *ab);  // LAPACK band, host
 // sx_mesh_s::kratio of a mesh description, from host geometry alone.
 int mesh_kratio(const sx_mesh_desc *d, double *out);
 
+// FP32 CG iterations one refinement round needs to cut its residual by
+// 1e-6, about what FP32 arithmetic allows: Jacobi-CG takes about
+// 5.3 sqrt(1 + kratio / hcon) iterations per 1e-7 (measured with the oracle
+// over lambda2 = 1..1e6, N = 4..10, square and 1:4 elements: within +-40 %).
+// Above CG_ROUND_CAP (or for hcon <= 0) the FP32 iterations are not used.
+constexpr int CG_ROUND_CAP = 400;
+int cg_round_iters(double kratio, double hcon);
+
 // Whether the FP64 band Cholesky is the better route for one mode (two
 // planes) of the mixed-precision form with Helmholtz constant hcon, solved
-// to tol_rel with n_inner FP32 iterations per refinement round and at most
-// max_refine rounds.  Predicted times on B200:
-//   CG:     Jacobi-CG takes about 5.3 sqrt(1 + kratio / hcon) iterations per
-//           1e-7 of residual (measured with the oracle over lambda2 = 1..1e6,
-//           N = 8 and 10); each iteration streams 4 (8 npts + 2 nel np^2)
-//           bytes per plane at 2.1 TB/s (k_cg, measured), 12 us at least
+// to tol_rel with at least n_inner FP32 iterations per refinement round and
+// at most max_refine rounds.  Predicted streaming times on B200 (the
+// per-launch latencies are shared by all modes of a batched launch, so a
+// mode is charged only for its bytes):
+//   CG:     rounds of max(n_inner, cg_round_iters) iterations, one round per
+//           1e-6 of tol_rel; each iteration streams 4 (8 npts + 2 nel np^2)
+//           bytes per plane at 2.1 TB/s (k_cg, measured)
 //   band:   the factor twice plus hbi/hii at 1.9 TB/s (k_band_sweep with 32
-//           systems, measured), or 2 nblk block steps of 7.7 us each when
-//           few systems run (its serial chain), whichever is longer
+//           systems, measured)
 //   factor: nsolve nband^2 flops at 3.9 TFLOP/s (config-2 set-up,
 //           measured), divided by `reuse`, the solves expected per factored
 //           system (0: already factored, no cost).
-// A mode whose CG would need more than max_refine rounds goes to the band.
+// A mode whose rounds would exceed CG_ROUND_CAP iterations, or whose CG would
+// need more than max_refine rounds, goes to the band.
 bool band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon, int n_inner,
                   double tol_rel, int max_refine, double reuse);
 

@@ -437,8 +437,18 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       g4[g] = make_int4(v[0], v[1], v[2], v[3]);
     }
     SX_TRY(M->dg2e4.upload(g4.data(), g4.size()));
+    // per element slot: the holders of its node as (element << 8 | tensor
+    // node), the element-layout address of their A u (nel < 2^23, np^2 < 256)
+    if (nel >= (1 << 23)) {
+      set_error("%d elements: the element-layout gather tables hold at most 2^23", nel);
+      return SX_ERR_UNSUPPORTED;
+    }
+    auto pack = [&](int ei) { return ei < 0 ? ei : ((ei / next) << 8) | M->emap[ei % next]; };
     std::vector<int4> e4((size_t)nel * next);
-    for (size_t k = 0; k < e4.size(); k++) e4[k] = g4[M->btog[k]];
+    for (size_t k = 0; k < e4.size(); k++) {
+      const int4 q = g4[M->btog[k]];
+      e4[k] = make_int4(pack(q.x), pack(q.y), pack(q.z), q.w == -2 ? -2 : pack(q.w));
+    }
     SX_TRY(M->de2w4.upload(e4.data(), e4.size()));
     std::vector<unsigned long long> own(nel, 0ull);
     for (int e = 0; e < nel; e++)

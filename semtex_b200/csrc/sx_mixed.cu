@@ -35,6 +35,7 @@
 
 #include "sx_kernels.cuh"
 #include "sx_mixed.cuh"
+#include "sx_ptx.cuh"
 #include "sx_solve.cuh"
 
 namespace sx {
@@ -409,70 +410,111 @@ __global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const dou
 
 enum { CG_INIT = 0, CG_ITER = 1, CG_LAST = 2 };
 
-// Direct-stiffness sum at global node g from its gather list q (the first
-// four CSR entries, or .w == -2 to walk the CSR), in element order.
-__device__ __forceinline__ float gather_w(const MeshView &M, const float *__restrict__ W, int4 q, int g, int PP,
-                                          int p) {
+// Element-layout address of (element e, plane chunk y, tensor node t, lane l).
+template <int NN>
+__device__ __forceinline__ size_t eidx(int e, int nch, int y, int t, int l) {
+  return (((size_t)e * nch + y) * NN + t) * MX_CH + l;
+}
+
+// Direct-stiffness sum of the element-layout W at global node g, in element
+// (CSR) order, from its gather list q (holders packed as element << 8 |
+// tensor node; .w == -2: walk the CSR, whose entries are element * next +
+// slot, slot -> tensor node through emt).  Every holder of g forms the same
+// sum in the same order.
+template <int NN>
+__device__ __forceinline__ float gather_we(const MeshView &M, const float *__restrict__ W, int4 q, int g, int nch,
+                                           int y, int l, const int *emt) {
   if (q.w == -2) {
     float s = 0.0f;
-    for (int k = M.g2e_ptr[g]; k < M.g2e_ptr[g + 1]; k++) s += W[(size_t)M.g2e_idx[k] * PP + p];
+    for (int k = M.g2e_ptr[g]; k < M.g2e_ptr[g + 1]; k++) {
+      const int ei = M.g2e_idx[k], eh = ei / M.next;
+      s += W[eidx<NN>(eh, nch, y, emt[ei - eh * M.next], l)];
+    }
     return s;
   }
-  const float v0 = W[(size_t)q.x * PP + p];
-  const float v1 = q.y >= 0 ? W[(size_t)q.y * PP + p] : 0.0f;
-  const float v2 = q.z >= 0 ? W[(size_t)q.z * PP + p] : 0.0f;
-  const float v3 = q.w >= 0 ? W[(size_t)q.w * PP + p] : 0.0f;
+  const float v0 = W[eidx<NN>(q.x >> 8, nch, y, q.x & 255, l)];
+  const float v1 = q.y >= 0 ? W[eidx<NN>(q.y >> 8, nch, y, q.y & 255, l)] : 0.0f;
+  const float v2 = q.z >= 0 ? W[eidx<NN>(q.z >> 8, nch, y, q.z & 255, l)] : 0.0f;
+  const float v3 = q.w >= 0 ? W[eidx<NN>(q.w >> 8, nch, y, q.w & 255, l)] : 0.0f;
   return ((v0 + v1) + v2) + v3;
 }
 
-// One launch = one iteration for every plane: block (element e, chunk of 32
-// planes), NP warps.  Phase A walks the element's nodes in edge-map order
-// (warp w takes slots w, w + NP, ...: the boundary slots spread evenly);
-// the operator then runs on tensor lines: warp w owns row w for the
+// One launch = one iteration for every plane: block (element e, chunk y of
+// 32 planes), NP warps.  Thread 0 stages the element's spans of r, s, p, d,
+// its own A u and the preconditioner into shared memory with TMA bulk copies
+// on one mbarrier while the block loads its tables.  Phase A walks the
+// element's nodes in edge-map order (warp w takes slots w, w + NP, ...: the
+// boundary slots spread evenly), gathers A u of the previous launch at the
+// boundary nodes, updates its copies of s, r, p, d in shared memory and
+// writes u = PC r; thread 0 streams the updated spans back with bulk stores
+// while the operator runs on tensor lines (warp w owns row w for the
 // x-derivative terms and column w for the y-derivative terms, the derivative
-// matrix is read from constant memory with compile-time subscripts, and
-// shared memory is touched about five times per node.
-// mode CG_INIT: u = PC r from r[0], w -> W[0]; scalars -> slot 0.
-// mode CG_ITER: iteration `it` (slots it & 1 in, (it + 1) & 1 out).
+// matrix in constant memory with compile-time subscripts); A u is staged in
+// shared memory and bulk-stored as well.
+// mode CG_INIT: r gathered from the residual's global vector, u = PC r;
+//               writes r and A u (W[0]); scalars -> slot 0.
+// mode CG_ITER: iteration `it` (W and scalar slots it & 1 in, (it + 1) & 1 out).
 // mode CG_LAST: only the owners' d update, folded into x64; no operator.
-// Resident blocks per SM the register budget is set for: the kernel is
-// latency-bound (dependent gathers), so occupancy pays more than registers.
-constexpr int cg_min_blocks(int np) { return np <= 10 ? 3 : 2; }
+// Resident blocks per SM that the register budget is set for (shared memory
+// allows 3 at np <= 9 and 2 at np <= 11).
+constexpr int cg_min_blocks(int np) { return np <= 9 ? 3 : (np <= 11 ? 2 : 1); }
+constexpr long long CG_WAIT_LIMIT = 2000000000LL;  // clock cycles: about a second
+
+// Dynamic shared memory of k_cg: six [NN][32] spans and the [NN][16]
+// preconditioner pairs.
+constexpr size_t cg_smem(int np) { return (size_t)np * np * (6 * MX_CH + 16) * sizeof(float); }
 
 template <int NP>
 __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
-    k_cg(MeshView M, MxParams P, CgVecs V, int it, int mode, double *part,
-                                                unsigned *cnt) {
+    k_cg(MeshView M, MxParams P, CgVecs V, int it, int mode, double *part, unsigned *cnt) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, DO = DOff<NP>::v;
-  // two [NN][32] exchange buffers: B0 holds u, B1 the column results (and on
-  // curved elements both carry r and s once)
-  extern __shared__ __align__(16) float smc[];
-  float *B0 = smc, *B1 = smc + NN * MX_CH;
+  constexpr uint32_t SPAN = NN * MX_CH * sizeof(float), PSPAN = NN * 16 * sizeof(float);
+  // shared spans, NN * 32 floats each: r, s, p, d (updated in place); B1 =
+  // the element's own A u, then the column results (and r on curved
+  // elements); B0 = u, then s on curved elements, then the A u to store;
+  // then the preconditioner pairs [NN][16]
+  extern __shared__ __align__(128) float smc[];
+  float *Rs = smc, *Ss = Rs + NN * MX_CH, *Ps = Ss + NN * MX_CH, *Ds = Ps + NN * MX_CH;
+  float *B1 = Ds + NN * MX_CH, *B0 = B1 + NN * MX_CH, *PCs = B0 + NN * MX_CH;
   __shared__ int gtab[NN], emt[NN], tsl[NN];
   __shared__ int4 w4[NE];
-  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int staged;
+  const int e = blockIdx.x, y = blockIdx.y, nch = gridDim.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = y * MX_CH + lane, PP = P.PP;
+  const bool init = mode == CG_INIT, last = mode == CG_LAST;
+  const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
+  const bool warm = !init && it > 0;  // s, p, d hold previous iterates
+  const size_t base = eidx<NN>(e, nch, y, 0, 0), pbase = ((size_t)e * nch + y) * NN * 16;
+  // buffers of this launch, selected without indexing the parameter arrays
+  const float *__restrict__ Win = cur ? V.WE[1] : V.WE[0];
+  float *__restrict__ Wout = nxt ? V.WE[1] : V.WE[0];
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init_cluster();
+    const uint32_t bytes =
+        PSPAN + (init ? 0u : SPAN) + (!init && !last ? SPAN : 0u) + (warm ? (last ? 2u : 3u) * SPAN : 0u);
+    mbar_arrive_expect_tx(&bar, bytes);
+    bulk_g2s(PCs, V.pcE + pbase, PSPAN, &bar);
+    if (!init) bulk_g2s(Rs, V.rE + base, SPAN, &bar);
+    if (!init && !last) bulk_g2s(B1, Win + base, SPAN, &bar);
+    if (warm) {
+      bulk_g2s(Ps, V.pE + base, SPAN, &bar);
+      bulk_g2s(Ds, V.dE + base, SPAN, &bar);
+      if (!last) bulk_g2s(Ss, V.sE + base, SPAN, &bar);
+    }
+  }
   for (int a = threadIdx.x; a < NN; a += NP * 32) {
     gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
     emt[a] = M.emap[a];
     tsl[a] = M.pmap[a];
     if (a < NE) w4[a] = M.e2w4[(size_t)e * NE + a];
   }
-  const bool init = mode == CG_INIT, last = mode == CG_LAST;
-  const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
-  const bool warm = !init && it > 0;  // s, p, d hold previous iterates
-  // buffers of this launch, selected without indexing the parameter arrays
-  const float *__restrict__ rin = cur ? V.r[1] : V.r[0];
-  float *__restrict__ rout = nxt ? V.r[1] : V.r[0];
-  const float *__restrict__ sin = nxt ? V.s[1] : V.s[0];
-  float *__restrict__ sout = cur ? V.s[1] : V.s[0];
-  const float *__restrict__ Win = cur ? V.W[1] : V.W[0];
-  float *__restrict__ Wout = nxt ? V.W[1] : V.W[0];
   const double *gam_in = cur ? V.gam[1] : V.gam[0], *alpha_in = cur ? V.alpha[1] : V.alpha[0];
   const double *beta_in = cur ? V.beta[1] : V.beta[0];
   double *gam_out = nxt ? V.gam[1] : V.gam[0], *alpha_out = nxt ? V.alpha[1] : V.alpha[0];
   double *beta_out = nxt ? V.beta[1] : V.beta[0];
-  const int ns = P.nsolve[p], c = pc_col(P, p);
+  const int ns = P.nsolve[p];
   float alpha = 0.0f, beta = 0.0f;
   if (!init) {
     alpha = (float)alpha_in[p];
@@ -480,72 +522,80 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
   }
   const unsigned long long own = M.owner[e];
   __syncthreads();
+  // the staged spans: thread 0 waits (bounded) and tells the block; the
+  // others then pass the completed phase, which orders the TMA writes for them
+  if (threadIdx.x == 0) {
+    bool ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);
+    if (!ok) {
+      atomicOr(V.status, 1 << SX_ERR_TIMEOUT);
+      ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);  // let the copies land before leaving
+    }
+    staged = ok;
+  }
+  __syncthreads();
+  if (!staged) return;  // block-uniform
+  if (threadIdx.x != 0) mbar_wait(&bar, 0, CG_WAIT_LIMIT);
 
-  // ---- phase A: vector updates at the element's nodes, u = PC r -> U, in
-  // two batches of slots, each batch's loads issued before any is used
-  constexpr int KB = (NP + 1) / 2;
+  // ---- phase A: vector updates at the element's nodes, u = PC r -> B0.
+  // Global loads first (the boundary gathers, or r at INIT), all in flight
+  // together; then the updates on the staged spans.
+  float gv[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    const int a = w + k * NP, g = gtab[a];
+    gv[k] = 0.0f;
+    if (!(a >= NE || g < ns)) continue;
+    if (init)
+      gv[k] = V.r0[(size_t)g * PP + p];
+    else if (!last && a < NE)
+      gv[k] = gather_we<NN>(M, Win, w4[a], g, nch, y, lane, emt);
+  }
   double gam = 0.0;
 #pragma unroll
-  for (int k0 = 0; k0 < NP; k0 += KB) {
-    float rv[KB], cv[KB], wv[KB], sv[KB], pv[KB], dv[KB];
-#pragma unroll
-    for (int kk = 0; kk < KB; kk++) {
-      rv[kk] = cv[kk] = wv[kk] = sv[kk] = pv[kk] = dv[kk] = 0.0f;
-      if (k0 + kk >= NP) continue;
-      const int a = w + (k0 + kk) * NP;
-      const int g = gtab[a];
-      const bool solve = a >= NE || g < ns;
-      const bool mine = a >= NE || ((own >> a) & 1ull);
-      if (solve && (!last || mine)) {
-        const size_t o = (size_t)g * PP + p;
-        rv[kk] = rin[o];
-        cv[kk] = P.pcf[(size_t)g * P.M + c];
-        if (!init && !last) {
-          wv[kk] = a >= NE ? V.wi[o] : gather_w(M, Win, w4[a], g, PP, p);
-          if (warm) sv[kk] = sin[o];
-        }
-        if (warm && mine) {
-          pv[kk] = V.p[o];
-          dv[kk] = V.d[o];
-        }
+  for (int k = 0; k < NP; k++) {
+    const int a = w + k * NP, g = gtab[a], t = emt[a], o = t * MX_CH + lane;
+    const bool solve = a >= NE || g < ns;
+    const bool mine = a >= NE || ((own >> a) & 1ull);
+    const float pc = PCs[t * 16 + (lane >> 1)];
+    float un = 0.0f;
+    if (init) {
+      Rs[o] = gv[k];  // zero at essential nodes
+      un = pc * gv[k];
+      if (solve && mine) gam += (double)gv[k] * (double)un;
+    } else if (solve) {
+      const float r = Rs[o];
+      const float uo = pc * r;
+      const float pp = warm ? uo + beta * Ps[o] : uo;
+      const float dd = warm ? Ds[o] + alpha * pp : alpha * pp;
+      if (last) {
+        if (mine) V.x64[(size_t)g * PP + p] += (double)dd;
+      } else {
+        const float wv = a >= NE ? B1[o] : gv[k];
+        const float s = warm ? wv + beta * Ss[o] : wv;
+        const float rn = r - alpha * s;
+        un = pc * rn;
+        Rs[o] = rn;
+        Ss[o] = s;
+        Ps[o] = pp;
+        Ds[o] = dd;
+        if (mine) gam += (double)rn * (double)un;
       }
     }
-#pragma unroll
-    for (int kk = 0; kk < KB; kk++) {
-      if (k0 + kk >= NP) continue;
-      const int a = w + (k0 + kk) * NP;
-      const int g = gtab[a];
-      const bool solve = a >= NE || g < ns;
-      const bool mine = a >= NE || ((own >> a) & 1ull);
-      const size_t o = (size_t)g * PP + p;
-      float un = 0.0f;
-      if (init) {
-        un = cv[kk] * rv[kk];
-        if (solve && mine) gam += (double)rv[kk] * (double)un;
-      } else if (solve) {
-        const float uo = cv[kk] * rv[kk];
-        const float pp = warm ? uo + beta * pv[kk] : uo;
-        const float dd = warm ? dv[kk] + alpha * pp : alpha * pp;
-        if (last) {
-          if (mine) V.x64[o] += (double)dd;
-        } else {
-          const float s = warm ? wv[kk] + beta * sv[kk] : wv[kk];
-          const float rn = rv[kk] - alpha * s;
-          un = cv[kk] * rn;
-          if (mine) {
-            sout[o] = s;
-            rout[o] = rn;
-            V.p[o] = pp;
-            V.d[o] = dd;
-            gam += (double)rn * (double)un;
-          }
-        }
-      }
-      if (!last) B0[emt[a] * MX_CH + lane] = un;
-    }
+    if (!last) B0[o] = un;
   }
-  if (last) return;  // block-uniform
+  if (last) return;  // block-uniform; nothing staged for storing
+  // the updated spans go back while the operator runs
+  fence_proxy_async_smem();
   __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_s2g(V.rE + base, Rs, SPAN);
+    if (!init) {
+      bulk_s2g(V.sE + base, Ss, SPAN);
+      bulk_s2g(V.pE + base, Ps, SPAN);
+      bulk_s2g(V.dE + base, Ds, SPAN);
+    }
+    bulk_commit();
+  }
 
   // ---- operator: out = hc Q4 u + D^T S + R D on tensor lines
   float ur[NP], R[NP], S[NP];
@@ -610,13 +660,16 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
     float b = 0.0f;
 #pragma unroll
     for (int k = 0; k < NP; k++) b += R[k] * c_Df[DO + k * NP + j];
-    const int t = w * NP + j, a = tsl[t];
+    const int t = w * NP + j;
     const float out = G[t].w * hc * ur[j] + B1[t * MX_CH + lane] + b;
-    if (a < NE)
-      Wout[((size_t)e * NE + a) * PP + p] = out;
-    else
-      V.wi[(size_t)gtab[a] * PP + p] = out;
+    B0[t * MX_CH + lane] = out;  // every warp is past its reads of u in B0
     del += (double)ur[j] * (double)out;
+  }
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_s2g(Wout + base, B0, SPAN);
+    bulk_commit();
   }
 
   // ---- gamma = (r, u), delta = (A u, u); the chunk's last block forms the
@@ -637,6 +690,7 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
     alpha_out[p] = an;
     beta_out[p] = bn;
   }
+  if (threadIdx.x == 0) bulk_wait_all();  // the stores read shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -764,8 +818,9 @@ static int set_smem_attrs() {
                                (int)(4 * NN * MX_CH * sizeof(double))));
   SX_CUDA(cudaFuncSetAttribute(k_x_op64<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)(3 * NN * MX_CH * sizeof(double))));
-  SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(2 * NN * MX_CH * sizeof(float))));
+  SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_smem(NP)));
+  // the largest carveout, so that cg_min_blocks(NP) blocks fit an SM
+  SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   return SX_OK;
 }
 
@@ -786,16 +841,16 @@ static MxScalPtrs scal_ptrs(const MixedWork &W) {
 static CgVecs cg_vecs(MixedWork &W) {
   const MxScalPtrs s = scal_ptrs(W);
   CgVecs v;
-  v.r[0] = W.r0.p;
-  v.r[1] = W.r1.p;
-  v.s[0] = W.s0.p;
-  v.s[1] = W.s1.p;
-  v.W[0] = W.W0.p;
-  v.W[1] = W.W1.p;
-  v.wi = W.wi.p;
-  v.p = W.p.p;
-  v.d = W.d.p;
+  v.rE = W.rE.p;
+  v.sE = W.sE.p;
+  v.pE = W.pE.p;
+  v.dE = W.dE.p;
+  v.WE[0] = W.WE0.p;
+  v.WE[1] = W.WE1.p;
+  v.pcE = W.pcE.p;
+  v.r0 = W.r0.p;
   v.x64 = W.x64.p;
+  v.status = W.status;
   for (int k = 0; k < 2; k++) {
     v.gam[k] = s.gam[k];
     v.alpha[k] = s.alpha[k];
@@ -828,13 +883,15 @@ static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStrea
   const MxParams P = W.prm;
   const MxScalPtrs s = scal_ptrs(W);
   const CgVecs V = cg_vecs(W);
-  const size_t smcg = 2 * NN * MX_CH * sizeof(float), sm64 = 3 * NN * MX_CH * sizeof(double);
+  const size_t sm64 = 3 * NN * MX_CH * sizeof(double);
   const dim3 eg(M.nel, nch);
   *nl = 0;
-  SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, smcg, st>>>(M, P, V, 0, CG_INIT, W.part.p, W.cnt.p)));
+  SX_NP_SWITCH_M(M.np,
+                 (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(M, P, V, 0, CG_INIT, W.part.p, W.cnt.p)));
   for (int it = 0; it < n_inner; it++) {
     const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
-    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, smcg, st>>>(M, P, V, it, mode, W.part.p, W.cnt.p)));
+    SX_NP_SWITCH_M(M.np,
+                   (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(M, P, V, it, mode, W.part.p, W.cnt.p)));
   }
   SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, 256, sm64, st>>>(M, P, W.x64.p, W.Ye64.p)));
   k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r0.p, s.r2, W.part.p, W.cnt.p);
@@ -846,12 +903,11 @@ static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStrea
 int mixed_profile_iterations(const MeshView &M, MixedWork &W, int reps, cudaStream_t st) {
   // iteration 1 reads what iteration 0 of the last round wrote
   if (W.PP == 0 || W.n_inner < 2 || reps <= 0) return SX_ERR_ARG;
-  const int nch = W.PP / MX_CH, NN = M.npnp;
+  const int nch = W.PP / MX_CH;
   const CgVecs V = cg_vecs(W);
-  const size_t smcg = 2 * NN * MX_CH * sizeof(float);
   for (int r = 0; r < reps; r++)
-    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, nch), N_ * 32, smcg, st>>>(M, W.prm, V, 1, CG_ITER, W.part.p,
-                                                                             W.cnt.p)));
+    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, nch), N_ * 32, cg_smem(N_), st>>>(M, W.prm, V, 1, CG_ITER,
+                                                                                    W.part.p, W.cnt.p)));
   SX_CUDA(cudaGetLastError());
   return SX_OK;
 }
@@ -879,6 +935,24 @@ __global__ void k_x_pc(int npts, int M, const float *const *pcs, float *out) {
   for (int m = 0; m < M; m++) out[(size_t)g * M + m] = pcs[m][g];
 }
 
+// Element-layout preconditioner pairs, pcE[((e * nch + y) * np^2 + t) * 16 +
+// q] = the inverse Jacobi diagonal of mode column 16 y + q (clamped to the
+// last mode) at the global node of (e, t); lanes 2q and 2q + 1 -- the mode's
+// two planes -- read it.
+__global__ void k_x_pce(MeshView M, int nch, int Mc, const float *__restrict__ pcf, float *pcE) {
+  const int NN = M.npnp;
+  const size_t n = (size_t)M.nel * nch * NN * 16;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i & 15);
+    const size_t r = i >> 4;
+    const int t = (int)(r % NN);
+    const size_t ey = r / NN;
+    const int y = (int)(ey % nch), e = (int)(ey / nch);
+    const int g = gidx(M, e, M.pmap[t]);
+    pcE[i] = pcf[(size_t)g * Mc + min(16 * y + q, Mc - 1)];
+  }
+}
+
 static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
                  cudaStream_t st) {
   const int npts = M.nglobal + M.nel * M.nint;
@@ -892,15 +966,15 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
     SX_TRY(need(W.b64, n));
     SX_TRY(need(W.x64, n));
     SX_TRY(need(W.Ye64, (size_t)PP * M.nel * M.npnp));
+    const size_t ne = (size_t)PP * M.nel * M.npnp;  // one E-vector
     SX_TRY(need(W.r0, n));
-    SX_TRY(need(W.r1, n));
-    SX_TRY(need(W.s0, n));
-    SX_TRY(need(W.s1, n));
-    SX_TRY(need(W.p, n));
-    SX_TRY(need(W.d, n));
-    SX_TRY(need(W.wi, n));
-    SX_TRY(need(W.W0, (size_t)PP * M.nel * M.next));
-    SX_TRY(need(W.W1, (size_t)PP * M.nel * M.next));
+    SX_TRY(need(W.rE, ne));
+    SX_TRY(need(W.sE, ne));
+    SX_TRY(need(W.pE, ne));
+    SX_TRY(need(W.dE, ne));
+    SX_TRY(need(W.WE0, ne));
+    SX_TRY(need(W.WE1, ne));
+    SX_TRY(need(W.pcE, ne / 2));
     SX_TRY(need(W.scal, (size_t)MX_NSCAL * PP));
     SX_TRY(need(W.hcon, (size_t)PP));
     SX_TRY(need(W.gess, (size_t)PP * M.nglobal));
@@ -936,6 +1010,9 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
   DBuf<const float *> dp;
   SX_TRY(dp.upload_on(pcs.data(), pcs.size(), st));
   k_x_pc<<<(npts + 255) / 256, 256, 0, st>>>(npts, Mc, dp.p, W.pcf.p);
+  const size_t npce = (size_t)M.nel * (PP / MX_CH) * M.npnp * 16;
+  k_x_pce<<<(int)std::min<size_t>((npce + 255) / 256, 8 * 148), 256, 0, st>>>(M, PP / MX_CH, Mc, W.pcf.p,
+                                                                               W.pcE.p);
   SX_CUDA(cudaGetLastError());
   SX_CUDA(cudaStreamSynchronize(st));
   return SX_OK;

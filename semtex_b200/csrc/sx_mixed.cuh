@@ -35,17 +35,23 @@ struct MxScalPtrs {
   double *r2, *b2, *gam[2], *alpha[2], *beta[2];
 };
 
-// Vectors of the FP32 inner iteration, plane-interleaved [npts][PP] unless
-// noted.  r and s alternate between two buffers by iteration parity (other
-// elements still read the old value of a shared node while its owner writes
-// the new one); p and d are read only by the node's owner and stay in place.
+// Vectors of the FP32 inner iteration in element layout ("E-vectors"): every
+// element keeps its own copy of its nodes' values, chunk-major,
+// V[((e * nch + y) * np^2 + t) * 32 + l] for element e, plane chunk y,
+// tensor node t and lane (plane) l, so one block's data is one contiguous
+// np^2 * 128-byte span that a single TMA bulk copy moves.  The copies of a
+// shared node are updated by every element that holds it, with the same
+// arithmetic on the same inputs, so they stay equal; r, s, p, d are read and
+// written only by their element's block and stay in place.  A u is gathered
+// across elements, so it alternates between two buffers by parity.
 struct CgVecs {
-  float *r[2], *s[2];
-  float *W[2];     // element boundary slots of A u, [nel][next][PP]
-  float *wi;       // A u at interior nodes, by global node
-  float *p, *d;
+  float *rE, *sE, *pE, *dE;
+  float *WE[2];       // A u at every element node (unassembled)
+  const float *pcE;   // inverse Jacobi diagonal, [e][y][t][16] by mode pair
+  const float *r0;    // residual of the last refinement step, [npts][PP]
   double *x64;
   double *gam[2], *alpha[2], *beta[2];
+  int *status;        // device status bits (1 << SX_ERR_*)
 };
 
 struct MixedWork {
@@ -53,7 +59,8 @@ struct MixedWork {
   DBuf<double> hcon, b64, x64, Ye64, scal, part, gess;
   DBuf<int> nsolve, active;
   DBuf<unsigned> cnt;
-  DBuf<float> pcf, r0, r1, s0, s1, p, d, wi, W0, W1;
+  DBuf<float> pcf, r0, rE, sE, pE, dE, WE0, WE1, pcE;
+  int *status = nullptr;  // the owner's device status word
   cudaGraphExec_t g_init = nullptr, g_round = nullptr;
   int launches_init = 0, launches_round = 0;
   std::vector<double> hscal;

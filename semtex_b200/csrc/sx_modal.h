@@ -63,7 +63,7 @@ struct sx_modal_s {
   const void *mkey[3] = {nullptr, nullptr, nullptr};
   int mnz = 0, mstride = 0;
   std::vector<int> mmodes;           // local modes the FP32 iterations solve
-  int n_inner = 12;                  // FP32 PCG iterations per refinement round
+  int n_inner = 12;                  // FP32 PCG iterations per refinement round, at least
   int mixed_route = 0;               // 0 auto, 1 FP32 CG only, 2 band solve where factored
   bool use_graphs = true;
   std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size

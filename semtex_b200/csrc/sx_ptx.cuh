@@ -66,6 +66,28 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// 1-D TMA bulk copy this CTA's shared memory -> global, in the calling
+// thread's bulk group.  dst/src 16-B aligned, bytes a multiple of 16.  The
+// shared-memory source must have been written before a
+// fence_proxy_async_smem() (and the barrier that orders the writers).
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Wait until every bulk group this thread committed has completed (global
+// writes done, shared-memory sources free).
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Make this thread's generic-proxy shared-memory writes visible to the async
+// proxy (TMA) before a bulk store reads them.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Address of the same shared variable in CTA `rank` of this cluster.
 __device__ __forceinline__ uint32_t map_rank(const void *p, uint32_t rank) {
   uint32_t r;

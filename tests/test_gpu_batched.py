@@ -140,7 +140,9 @@ def test_mixed_hybrid_route_vs_oracle(sx, torch, method):
     go to the FP64 band Cholesky, the others to the FP32 iterations, both in
     one call; every plane meets the 1e-10 bar against the oracle."""
     from semtex_b200.workloads import small_channel
-    w = small_channel(nx=10, ny=8, np_=9, nz=16, lam=1e6, seed=13)
+    # 20 x 12 elements at N = 8: modes 0-5 (lambda2 <= 5.2e3) to the band,
+    # predicted CG / band time 2.7 on mode 5; modes 6-7 to CG, ratio 0.76
+    w = small_channel(nx=20, ny=12, np_=9, nz=16, lam=1e6, seed=13)
     w.lambda2 = np.logspace(-2, 6, w.num_modes)
     mesh = sx.Mesh(w.mesh)
     S = sx.ModalMatrixSys(mesh, num_modes=w.num_modes, method=sx.DIRECT if method == "direct" else sx.AUTO,
