@@ -211,6 +211,26 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
 enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3 };
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 
+/* Autotuner (no reference counterpart): times the batched form on the
+ * caller's own data for each candidate schedule and keeps the fastest in the
+ * modal system, as sx_modal_tune would set it --
+ *   the band-sweep cluster size (CTAs sharing one system's tiles; sizes the
+ *   SM groups cannot hold are skipped), for SX_FP64 and for the modes that
+ *   SX_MIXED_FP32 routes to the band Cholesky;
+ *   the floor on FP32 iterations per refinement round, for SX_MIXED_FP32.
+ * d_f is only read (each trial solves a copy, allocated for the duration);
+ * d_u holds the last trial's solution.  Candidates whose solve does not
+ * reach tol_rel are kept only when none does. */
+typedef struct {
+  int band_cluster; /* chosen CTAs per cluster (0: the form runs no band sweeps) */
+  int inner_iters;  /* chosen floor on FP32 iterations per round (0: FP64 form) */
+  double ms;        /* one solve with the chosen schedule                     */
+  int trials;       /* schedules timed                                        */
+} sx_tune_result;
+SX_API int sx_modal_autotune(sx_modal modal, double *d_u, const double *d_f, const double *d_bc, int nz,
+                             int plane_stride, int precision, double tol_rel, int max_refine, void *stream,
+                             sx_tune_result *out);
+
 /* Profiling hook (no reference counterpart): re-launch only the banded
  * forward/backward sweeps of the last batched solve `reps` times on
  * `stream`, so the dominant kernel can be timed on its own.  The RHS

@@ -61,6 +61,14 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("band_cluster", C.c_int), ("inner_iters", C.c_int), ("ms", C.c_double),
+                ("trials", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_ulonglong), ("slots", C.c_int), ("precision", C.c_int),
                 ("tol_rel", C.c_double), ("max_refine", C.c_int), ("inner_iters", C.c_int)]
@@ -115,6 +123,7 @@ def _load():
     L.sx_profile_mixed_iterations.argtypes = [vp, ip, vp]
     L.sx_modal_status.argtypes = [vp]
     L.sx_modal_tune.argtypes = [vp, ip, ip]
+    L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
     L.sx_server_create.argtypes = [P(ServerConfig), P(vp)]
     L.sx_server_submit.argtypes = [vp, P(Request), P(C.c_ulonglong)]
     L.sx_server_wait.argtypes = [vp, C.c_ulonglong, dp, P(ip), P(dp)]
@@ -301,6 +310,14 @@ class ModalMatrixSys:
             _check(lib.sx_modal_tune(self.h, TUNE_BAND_CLUSTER, int(band_cluster)), "sx_modal_tune")
         if mixed_route is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_MIXED_ROUTE, int(mixed_route)), "sx_modal_tune")
+
+    def autotune(self, d_u, d_f, d_bc, nz, stride, precision=FP64, tol_rel=1e-12, max_refine=20, stream=0):
+        """Time the batched form's candidate schedules on this data (device
+        pointers; d_f is only read) and keep the fastest; returns the choice."""
+        r = TuneResult()
+        _check(lib.sx_modal_autotune(self.h, d_u, d_f, d_bc, nz, stride, precision, tol_rel, max_refine,
+                                     stream, C.byref(r)), "sx_modal_autotune")
+        return r.as_dict()
 
     def profile_band_sweeps(self, reps, stream=0):
         _check(lib.sx_profile_band_sweeps(self.h, reps, stream), "sx_profile_band_sweeps")

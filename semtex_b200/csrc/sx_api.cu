@@ -591,6 +591,100 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
   return rc;
 }
 
+extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, const double *d_bc, int nz,
+                                 int plane_stride, int precision, double tol_rel, int max_refine, void *stream,
+                                 sx_tune_result *out) {
+  if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+  if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+  if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
+  cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
+  std::vector<Group> groups;
+  SX_TRY(plane_groups(*s, nz, groups));
+  // does this form run band sweeps, and how many tiles do they stream?
+  bool band = precision == SX_FP64;
+  if (!band) {
+    for (auto &u : s->uniq)
+      if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, st));
+    for (auto &g : groups) band = band || route_direct(*s, *s->sys[g.mode], tol_rel, max_refine);
+  }
+  int J = 1;
+  for (auto &u : s->uniq) J = std::max(J, u->J);
+  std::vector<int> clusters, inners;
+  if (band)
+    for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
+      if (C <= J && band_active_clusters(C, 2, J + 2) > 0) clusters.push_back(C);
+  if (clusters.empty()) clusters.push_back(0);
+  if (precision == SX_MIXED_FP32)
+    inners = {8, 12, 16, 24};
+  else
+    inners = {0};
+  const size_t n = (size_t)nz * plane_stride;
+  DBuf<double> fw;  // the trials' forcing: a solve overwrites its forcing
+  SX_TRY(fw.alloc(n));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SX_CUDA(cudaEventCreate(&e0));
+  SX_CUDA(cudaEventCreate(&e1));
+  const int saved_cluster = s->forced_cluster, saved_inner = s->n_inner;
+  double best = INFINITY;
+  bool best_ok = false;
+  int bc = saved_cluster, bi = saved_inner, trials = 0, rc = SX_OK;
+  for (int C : clusters)
+    for (int I : inners) {
+      s->forced_cluster = C;
+      if (I > 0) s->n_inner = I;
+      s->fp64.reset();  // the captured graphs bake in the cluster size
+      s->hyb.reset();
+      double t_min = INFINITY;
+      int r = SX_OK;
+      for (int rep = 0; rep < 3 && (r == SX_OK || r == SX_WARN_STEP_LIMIT); rep++) {
+        if ((rc = (cudaMemcpyAsync(fw.p, d_f, n * 8, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? SX_OK
+                                                                                                   : SX_ERR_CUDA)))
+          break;
+        cudaEventRecord(e0, st);
+        r = solve_batched_on(s, d_u, fw.p, d_bc, nz, plane_stride, precision, tol_rel, max_refine, st, nullptr);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = SX_ERR_CUDA;
+          break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) t_min = std::min(t_min, (double)ms);  // rep 0 captures the graphs
+      }
+      if (rc != SX_OK) break;
+      if (r != SX_OK && r != SX_WARN_STEP_LIMIT) continue;
+      trials++;
+      const bool ok = r == SX_OK;
+      if ((ok && !best_ok) || (ok == best_ok && t_min < best)) {
+        best = t_min;
+        best_ok = ok;
+        bc = C;
+        bi = I > 0 ? I : saved_inner;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the graphs captured on the trial forcing must not outlive it
+  s->fp64.reset();
+  s->hyb.reset();
+  s->mkey[0] = s->mkey[1] = s->mkey[2] = nullptr;
+  s->forced_cluster = trials ? bc : saved_cluster;
+  s->n_inner = trials ? bi : saved_inner;
+  SX_CUDA(cudaStreamSynchronize(st));
+  if (rc != SX_OK) return rc;
+  if (!trials) {
+    set_error("autotune: no candidate schedule solved");
+    return SX_ERR_UNSUPPORTED;
+  }
+  if (out) {
+    out->band_cluster = band ? s->forced_cluster : 0;
+    out->inner_iters = precision == SX_MIXED_FP32 ? s->n_inner : 0;
+    out->ms = best;
+    out->trials = trials;
+  }
+  return SX_OK;
+}
+
 extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *f, const double *bc,
                                            int nz, int plane_stride, int precision, double tol_rel,
                                            int max_refine, sx_solve_stats *stats) {

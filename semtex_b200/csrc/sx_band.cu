@@ -329,6 +329,31 @@ int prepare_band_kernels() {
 
 // Largest cluster size (<= cmax) for which `nj` clusters can be resident at
 // once; at least 1.
+int band_active_clusters(int C, int pmax, int Wmax) {
+  int S = 4;
+  while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
+  if (sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = sweep_smem(pmax, C, S, Wmax);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  const cudaError_t e = pmax == 2 ? cudaOccupancyMaxActiveClusters(&n, k_band_sweep<2>, &cfg)
+                                  : cudaOccupancyMaxActiveClusters(&n, k_band_sweep<8>, &cfg);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 int pick_cluster(int nj, int cmax, int pmax, int Wmax) {
   int best = 1;
   for (int C = 1; C <= cmax; C++) {

@@ -680,12 +680,19 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
     if (init) {
       bn = 0.0;
       an = dn > 0.0 ? gn / dn : 0.0;
+      V.gam0[p] = gn;
     } else {
       const double go = gam_in[p], ao = alpha_in[p];
       bn = go > 0.0 ? gn / go : 0.0;
       const double den = ao > 0.0 ? dn - bn * gn / ao : dn;
       an = (gn > 0.0 && den > 0.0) ? gn / den : 0.0;
+      // a plane whose round has cut (r, PC r) by 1e13 -- about as far as
+      // FP32 vectors go -- stops here: alpha = beta = 0 leaves r, d and
+      // gamma unchanged, so it stays stopped for the rest of the round
+      // (iterating on in FP32 only feeds rounding noise into alpha)
+      if (gn <= 1e-13 * V.gam0[p]) an = bn = 0.0;
     }
+    if (!isfinite(an) || !isfinite(bn)) an = bn = 0.0;
     gam_out[p] = gn;
     alpha_out[p] = an;
     beta_out[p] = bn;
@@ -835,6 +842,7 @@ static MxScalPtrs scal_ptrs(const MixedWork &W) {
     r.alpha[k] = s + (4 + k) * PP;
     r.beta[k] = s + (6 + k) * PP;
   }
+  r.gam0 = s + 8 * PP;
   return r;
 }
 
@@ -856,6 +864,7 @@ static CgVecs cg_vecs(MixedWork &W) {
     v.alpha[k] = s.alpha[k];
     v.beta[k] = s.beta[k];
   }
+  v.gam0 = s.gam0;
   return v;
 }
 

@@ -29,10 +29,11 @@ struct MxParams {
 
 // Per-plane scalars, each an array of PP doubles: residual and RHS norms
 // (read by the host between rounds), then the inner iteration's gamma,
-// alpha, beta in two slots (iteration parity).
-constexpr int MX_NSCAL = 8;
+// alpha, beta in two slots (iteration parity), and gamma at the start of the
+// round.
+constexpr int MX_NSCAL = 9;
 struct MxScalPtrs {
-  double *r2, *b2, *gam[2], *alpha[2], *beta[2];
+  double *r2, *b2, *gam[2], *alpha[2], *beta[2], *gam0;
 };
 
 // Vectors of the FP32 inner iteration in element layout ("E-vectors"): every
@@ -51,6 +52,7 @@ struct CgVecs {
   const float *r0;    // residual of the last refinement step, [npts][PP]
   double *x64;
   double *gam[2], *alpha[2], *beta[2];
+  double *gam0;       // gamma at the start of the round
   int *status;        // device status bits (1 << SX_ERR_*)
 };
 

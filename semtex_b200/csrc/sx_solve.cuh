@@ -75,6 +75,9 @@ int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job
 int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st);
 int prepare_band_kernels();
 int pick_cluster(int nj, int cmax, int pmax, int Wmax);
+// Clusters of C band-sweep CTAs that can be resident at once (0: C does not
+// fit an SM group, so a launch with it would fail).
+int band_active_clusters(int C, int pmax, int Wmax);
 size_t sweep_smem(int pmax, int C, int S, int Wmax);
 // Set kernel attributes (max dynamic smem) ahead of any stream capture.
 int prepare_direct_kernels(const MeshView &M);

@@ -157,6 +157,30 @@ def test_mixed_hybrid_route_vs_oracle(sx, torch, method):
         assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (p, l2, mx, st)
 
 
+def test_autotune_keeps_results(sx, torch):
+    """The autotuner picks a schedule among the candidates, leaves the
+    forcing untouched, and the batched forms give the same answers after it:
+    bit for bit for FP64 (the cluster size does not change the arithmetic),
+    within the mixed form's bar for the mixed form."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=8, ny=8, np_=9, nz=12, lam=1e6, seed=11)
+    _, S = _setup(sx, w)
+    ub, _ = _run_device(torch, S, w, batched=True)
+    f = torch.tensor(w.forcing, device="cuda")
+    u = torch.zeros_like(f)
+    r64 = S.autotune(u.data_ptr(), f.data_ptr(), 0, w.nz, w.mesh.nplane, sx.FP64)
+    assert r64["trials"] >= 1 and r64["band_cluster"] >= 1 and r64["ms"] > 0.0
+    assert np.array_equal(f.cpu().numpy(), w.forcing)
+    ub2, _ = _run_device(torch, S, w, batched=True)
+    sp = solved_planes(w.nz)
+    assert np.array_equal(ub2[sp], ub[sp])
+    rm = S.autotune(u.data_ptr(), f.data_ptr(), 0, w.nz, w.mesh.nplane, sx.MIXED_FP32)
+    assert rm["inner_iters"] in (8, 12, 16, 24)
+    um, st = _run_device(torch, S, w, batched=True, precision=sx.MIXED_FP32)
+    l2, mx = rel_errs(um[sp], ub[sp])
+    assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (l2, mx, st, rm)
+
+
 def test_batched_host_entry(sx, torch):
     from semtex_b200.workloads import small_channel
     w = small_channel(nx=5, ny=4, np_=6, nz=6, lam=10.0, seed=3)
