@@ -75,79 +75,31 @@ __device__ __forceinline__ size_t ye_index(const MeshView &M, int e, int a, int 
                     : ((size_t)M.nel * M.next + (size_t)e * M.nint + (a - M.next)) * PP;
 }
 
-// Per-plane sums over the 8 rows of the block, then over the blocks of the
-// chunk (last block, index order).
-__device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, unsigned *cnt, int G, double *outA,
-                                              double *outB) {
-  __shared__ double sa[MX_ROWS][MX_CH], sb[MX_ROWS][MX_CH];
-  __shared__ int last;
-  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane;
-  sa[row][lane] = a;
-  sb[row][lane] = b;
-  __syncthreads();
-  // partials laid out [block][plane][2] so the final pass reads them
-  // coalesced across the lanes (planes)
-  const int PPc = gridDim.y * MX_CH;
-  if (row == 0) {
-    double ta = 0.0, tb = 0.0;
-    for (int r = 0; r < MX_ROWS; r++) {
-      ta += sa[r][lane];
-      tb += sb[r][lane];
-    }
-    double2 *pp = reinterpret_cast<double2 *>(part) + (size_t)blockIdx.x * PPc + p;
-    *pp = make_double2(ta, tb);
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&cnt[blockIdx.y], 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  double ta = 0.0, tb = 0.0;
-  const double2 *pp = reinterpret_cast<const double2 *>(part) + p;
-  int bx = row;
-#pragma unroll 1
-  for (; bx + 3 * MX_ROWS < G; bx += 4 * MX_ROWS) {
-    const double2 v0 = __ldcg(&pp[(size_t)bx * PPc]);
-    const double2 v1 = __ldcg(&pp[(size_t)(bx + MX_ROWS) * PPc]);
-    const double2 v2 = __ldcg(&pp[(size_t)(bx + 2 * MX_ROWS) * PPc]);
-    const double2 v3 = __ldcg(&pp[(size_t)(bx + 3 * MX_ROWS) * PPc]);
-    ta += v0.x; tb += v0.y;
-    ta += v1.x; tb += v1.y;
-    ta += v2.x; tb += v2.y;
-    ta += v3.x; tb += v3.y;
-  }
-  for (; bx < G; bx += MX_ROWS) {
-    const double2 v = __ldcg(&pp[(size_t)bx * PPc]);
-    ta += v.x;
-    tb += v.y;
-  }
-  sa[row][lane] = ta;
-  sb[row][lane] = tb;
-  __syncthreads();
-  if (row == 0) {
-    double fa = 0.0, fb = 0.0;
-    for (int r = 0; r < MX_ROWS; r++) {
-      fa += sa[r][lane];
-      fb += sb[r][lane];
-    }
-    if (outA) outA[p] = fa;
-    if (outB) outB[p] = fb;
-  }
-  if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
-}
+// Per-plane sums of (a, b) over the whole grid, deterministic and without
+// floating-point atomics, as a two-level tree so that no block sums more
+// than a few dozen partials at the end of a launch.  Every block writes its
+// total (over its ROWS warps) to part[block]; the last block of each group
+// of RED_GROUP blocks (an integer counter per chunk and group) sums the
+// group's partials in block order into part[G + group]; the last group to
+// finish sums the group totals in group order.  Returns true in warp 0 of
+// that last block, with the chunk's totals in fa, fb.  part holds
+// (G + ceil(G / RED_GROUP)) * PP double2; cnt holds nch * (1 + ceil(G /
+// RED_GROUP)) counters, zero on entry and left zero.
+constexpr int RED_GROUP = 32;
+inline int red_groups(int G) { return (G + RED_GROUP - 1) / RED_GROUP; }
 
-// chunk_reduce2 for a block of ROWS warps that leaves the per-plane totals
-// to the caller: returns true in warp 0 of the chunk's last block, with the
-// sums of a and b over the chunk's blocks in fa, fb.
 template <int ROWS>
 __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsigned *cnt, int G, double &fa,
                                           double &fb) {
   __shared__ double sa[ROWS][MX_CH], sb[ROWS][MX_CH];
   __shared__ int last;
-  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PPc = gridDim.y * MX_CH;
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31, y = blockIdx.y;
+  const int p = y * MX_CH + lane, PPc = gridDim.y * MX_CH;
+  const int ngrp = (G + RED_GROUP - 1) / RED_GROUP, grp = blockIdx.x / RED_GROUP;
+  const int g0 = grp * RED_GROUP, gn = min(RED_GROUP, G - g0);
+  double2 *P1 = reinterpret_cast<double2 *>(part), *P2 = P1 + (size_t)G * PPc;
+  unsigned *cg = cnt + gridDim.y + (size_t)y * ngrp;
+  // ---- the block's total
   sa[row][lane] = a;
   sb[row][lane] = b;
   __syncthreads();
@@ -157,37 +109,50 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
       ta += sa[r][lane];
       tb += sb[r][lane];
     }
-    reinterpret_cast<double2 *>(part)[(size_t)blockIdx.x * PPc + p] = make_double2(ta, tb);
+    P1[(size_t)blockIdx.x * PPc + p] = make_double2(ta, tb);
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&cnt[blockIdx.y], 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) last = (atomicAdd(&cg[grp], 1u) == (unsigned)gn - 1u);
   __syncthreads();
   if (!last) return false;
+  // ---- the group's total, over its blocks in order
   __threadfence();
   double ta = 0.0, tb = 0.0;
-  const double2 *pp = reinterpret_cast<const double2 *>(part) + p;
-  int bx = row;
-#pragma unroll 1
-  for (; bx + 3 * ROWS < G; bx += 4 * ROWS) {
-    const double2 v0 = __ldcg(&pp[(size_t)bx * PPc]);
-    const double2 v1 = __ldcg(&pp[(size_t)(bx + ROWS) * PPc]);
-    const double2 v2 = __ldcg(&pp[(size_t)(bx + 2 * ROWS) * PPc]);
-    const double2 v3 = __ldcg(&pp[(size_t)(bx + 3 * ROWS) * PPc]);
-    ta += v0.x; tb += v0.y;
-    ta += v1.x; tb += v1.y;
-    ta += v2.x; tb += v2.y;
-    ta += v3.x; tb += v3.y;
-  }
-  for (; bx < G; bx += ROWS) {
-    const double2 v = __ldcg(&pp[(size_t)bx * PPc]);
+  for (int k = row; k < gn; k += ROWS) {
+    const double2 v = __ldcg(&P1[(size_t)(g0 + k) * PPc + p]);
     ta += v.x;
     tb += v.y;
   }
   sa[row][lane] = ta;
   sb[row][lane] = tb;
   __syncthreads();
-  if (threadIdx.x == 0) cnt[blockIdx.y] = 0;
+  if (row == 0) {
+    ta = tb = 0.0;
+    for (int r = 0; r < ROWS; r++) {
+      ta += sa[r][lane];
+      tb += sb[r][lane];
+    }
+    P2[(size_t)grp * PPc + p] = make_double2(ta, tb);
+  }
+  if (threadIdx.x == 0) cg[grp] = 0;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&cnt[y], 1u) == (unsigned)ngrp - 1u);
+  __syncthreads();
+  if (!last) return false;
+  // ---- the chunk's total, over the groups in order
+  __threadfence();
+  ta = tb = 0.0;
+  for (int k = row; k < ngrp; k += ROWS) {
+    const double2 v = __ldcg(&P2[(size_t)k * PPc + p]);
+    ta += v.x;
+    tb += v.y;
+  }
+  sa[row][lane] = ta;
+  sb[row][lane] = tb;
+  __syncthreads();
+  if (threadIdx.x == 0) cnt[y] = 0;
   if (row != 0) return false;
   fa = fb = 0.0;
   for (int r = 0; r < ROWS; r++) {
@@ -195,6 +160,17 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
     fb += sb[r][lane];
   }
   return true;
+}
+
+// chunk_sum for the 8-warp node kernels, storing the totals.
+__device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, unsigned *cnt, int G, double *outA,
+                                              double *outB) {
+  double fa, fb;
+  if (chunk_sum<MX_ROWS>(a, b, part, cnt, G, fa, fb)) {
+    const int p = blockIdx.y * MX_CH + (threadIdx.x & 31);
+    if (outA) outA[p] = fa;
+    if (outB) outB[p] = fb;
+  }
 }
 
 // GLL derivative matrices for np = 3..12, FP32 and FP64, in constant memory:
@@ -990,9 +966,12 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
     SX_TRY(need(W.nsolve, (size_t)PP));
     SX_TRY(need(W.active, (size_t)PP));
     SX_TRY(need(W.pcf, (size_t)npts * Mc));
-    SX_TRY(need(W.part, (size_t)PP * std::max(W.G, M.nel) * 2));
-    if (W.cnt.n < (size_t)(PP / MX_CH)) {
-      SX_TRY(W.cnt.alloc(PP / MX_CH));
+    // reduction tree: block and group partials, chunk and group counters
+    const int gmax = std::max(W.G, M.nel);
+    SX_TRY(need(W.part, (size_t)PP * (gmax + red_groups(gmax)) * 2));
+    const size_t ncnt = (size_t)(PP / MX_CH) * (1 + red_groups(gmax));
+    if (W.cnt.n < ncnt) {
+      SX_TRY(W.cnt.alloc(ncnt));
       SX_TRY(W.cnt.zero(st));
     }
     W.hscal.assign((size_t)2 * PP, 0.0);

@@ -126,6 +126,41 @@ def config3(nx=64, ny=64, np_=11, nz=128, seed=3):
                     seed=seed, info={"jitter": 0.20})
 
 
+def config5(nx=128, ny=64, np_=11, nz=256, seed=5, nu=5e-4, dt=5e-4):
+    """The elliptic phase of one DNS timestep on a jittered periodic channel
+    (+-15 %, [0,2pi] x [0,1]): three viscous Helmholtz solves (velocity,
+    Dirichlet walls) with lambda2 = 1/(nu dt), betak2 = k^2, and the pressure
+    Poisson solve (natural walls) with lambda2 = 0, betak2 = k^2, whose k = 0
+    mode is singular and pinned like the reference's.  Forcing: seeded random
+    smooth velocity-like fields with spectral energy ~ k^-5/3 up to k = 32 (the
+    viscous forcing -u/(nu dt), the pressure forcing of the same law scaled by
+    1/dt).  Returns [u, v, w, p] workloads; u, v, w share one mesh."""
+    mv = _jittered_channel(nx, ny, np_, 0.15, seed)
+    mp = rect_mesh(nx, ny, np_, 0.0, 2 * np.pi, 0.0, 1.0, jitter=0.15, seed=seed, periodic_x=True,
+                   bc={"bottom": "N", "top": "N"})
+    rng = np.random.default_rng(seed)
+    nm = max(nz // 2, 1)
+    k = np.arange(nm, dtype=np.float64)
+    amp = np.where(k < 32, np.maximum(k, 1.0) ** (-5.0 / 6.0), 0.0)  # energy ~ k^-5/3
+
+    def field(m):
+        f = np.zeros((nz, m.nplane))
+        for plane in range(nz):
+            if plane == 1 and nz > 1:
+                continue
+            f[plane] = scatter_global(m, rng.standard_normal(m.n_unique) * amp[plane >> 1])
+        return f
+
+    out = []
+    for name in ("u", "v", "w"):
+        lam = np.full(nm, 1.0 / (nu * dt))
+        out.append(Workload(f"cfg5_{name}_{nx}x{ny}_N{np_ - 1}_nz{nz}", mv, nz, 1.0, lam, k ** 2,
+                            -field(mv) / (nu * dt), seed=seed, info={"solve": "viscous"}))
+    out.append(Workload(f"cfg5_p_{nx}x{ny}_N{np_ - 1}_nz{nz}", mp, nz, 1.0, np.zeros(nm), k ** 2,
+                        field(mp) / dt, seed=seed, info={"solve": "pressure"}))
+    return out
+
+
 @dataclass
 class ServeRequest:
     t_arrival: float             # seconds after the first arrival
