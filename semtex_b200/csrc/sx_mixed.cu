@@ -11,23 +11,23 @@
 //            r  = b - A x        (FP64 operator, FP64 residual)
 //   until  ||r|| <= tol ||b|| for every plane
 //
-// Layout: vectors are plane-interleaved, V[g * PP + p] (node g, plane p),
-// so a gather or scatter through btog moves 32 consecutive planes of one
-// node in one coalesced access, and index, geometry and operator tables are
-// loaded once for all planes.  Thread mapping everywhere: lane = plane
-// within a chunk of 32 (blockIdx.y = chunk), warp = node row.
+// Layout: the FP64 vectors (b, x, the residual) are plane-interleaved,
+// V[g * PP + p] (node g, plane p), so a gather or scatter through btog moves
+// 32 consecutive planes of one node in one coalesced access; the FP32 CG
+// vectors are element vectors (sx_mixed.cuh: CgVecs).  Thread mapping
+// everywhere: lane = plane within a chunk of 32 (blockIdx.y = chunk); the
+// element kernels give each of their np warps one tensor row and one
+// tensor column, the node kernels one node row per warp.
 //
 // One inner iteration is one kernel, k_cg: the Chronopoulos-Gear form of
 // PCG (one global reduction per iteration), element by element --
-//   gather w = A u of the previous launch (direct-stiffness sum of the
-//   element boundary slots, in element order), the vector updates at the
-//   element's nodes (every element computes its shared nodes, the owner
-//   writes them), u = PC r, the element operator A_e u_e, and the two dots
-//   (r, u) and (A u, u) = sum_e u_e . A_e u_e.
-// Reductions are two-level and deterministic: per-block partials per plane,
-// the last block of a chunk sums them in index order and computes the next
-// iteration's scalars.  Each refinement round is one captured CUDA graph;
-// the host reads the residual norms between rounds.
+//   gather w = A u of the previous launch (direct-stiffness sum over the
+//   node's holders, in element order), the updates of the element's copies
+//   of s, r, p, d, u = PC r, the element operator A_e u_e, and the two dots
+//   (r, u) (each node once, by its owner) and (A u, u) = sum_e u_e . A_e u_e.
+// Reductions are deterministic trees over the blocks (chunk_sum); the last
+// block forms the next iteration's scalars.  Each refinement round is one
+// captured CUDA graph; the host reads the residual norms between rounds.
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -64,8 +64,6 @@ __device__ __forceinline__ T dss_gather(const MeshView &M, const T *__restrict__
   const T v3 = q.w >= 0 ? Y[(size_t)q.w * PP + p] : T(0);
   return ((v0 + v1) + v2) + v3;
 }
-
-__device__ __forceinline__ int pc_col(const MxParams &P, int p) { return min(p >> 1, P.M - 1); }
 
 // FP64 element results: boundary slots as an element-local buffer
 // [nel][next][PP] (gathered through btog's CSR), then interior nodes in
@@ -188,17 +186,6 @@ template <>
 struct DOff<3> {
   static constexpr int v = 0;
 };
-template <typename T>
-__device__ __forceinline__ T cD(int i);
-template <>
-__device__ __forceinline__ float cD<float>(int i) {
-  return c_Df[i];
-}
-template <>
-__device__ __forceinline__ double cD<double>(int i) {
-  return c_Dd[i];
-}
-
 static int ensure_constD() {
   static std::mutex mu;
   static std::vector<char> done(256, 0);
@@ -224,47 +211,6 @@ static int ensure_constD() {
   return SX_OK;
 }
 
-// Sum-factorised element operator on plane-interleaved smem arrays
-// U, R, S [NN][32]: out(idx) for the calling lane (Element::HelmholtzOp +
-// HelmholtzKern, src/element.cpp:1564-1650).
-template <int NP, typename T>
-__device__ __forceinline__ void op_stage1(const T *, const T *Q1, const T *Q2, const T *Q3, bool q3, const T *U,
-                                          T *R, T *S) {
-  constexpr int NN = NP * NP, DO = DOff<NP>::v;
-  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int idx = row; idx < NN; idx += MX_ROWS) {
-    const int i = idx / NP, j = idx - i * NP;
-    T r = 0, s = 0;
-#pragma unroll
-    for (int k = 0; k < NP; k++) {
-      r += U[(i * NP + k) * MX_CH + lane] * cD<T>(DO + j * NP + k);
-      s += cD<T>(DO + i * NP + k) * U[(k * NP + j) * MX_CH + lane];
-    }
-    if (q3) {
-      R[idx * MX_CH + lane] = Q1[idx] * r + Q3[idx] * s;
-      S[idx * MX_CH + lane] = Q2[idx] * s + Q3[idx] * r;
-    } else {
-      R[idx * MX_CH + lane] = Q1[idx] * r;
-      S[idx * MX_CH + lane] = Q2[idx] * s;
-    }
-  }
-}
-
-template <int NP, typename T>
-__device__ __forceinline__ T op_stage2(const T *, const T *Q4, T hcon, const T *U, const T *R, const T *S, int idx) {
-  constexpr int DO = DOff<NP>::v;
-  const int lane = threadIdx.x & 31;
-  const int i = idx / NP, j = idx - i * NP;
-  T t = Q4[idx] * U[idx * MX_CH + lane] * hcon;
-  T a = 0, b = 0;
-#pragma unroll
-  for (int k = 0; k < NP; k++) {
-    a += cD<T>(DO + k * NP + i) * S[(k * NP + j) * MX_CH + lane];
-    b += R[(i * NP + k) * MX_CH + lane] * cD<T>(DO + k * NP + j);
-  }
-  return t + a + b;
-}
-
 // ---------------------------------------------------------------------------
 // RHS (FP64)
 // ---------------------------------------------------------------------------
@@ -288,49 +234,130 @@ __global__ void k_x_ess(MeshView M, MxParams P) {
   }
 }
 
-// Ye[(e*NN + a)*PP + p] = -(M f + H g) at edge-map slot a (Field::constrain).
+// (A_e u)(w, j), j = 0..NP-1, in FP64 for the calling warp's tensor row w
+// and lane's plane, on tensor lines as in k_cg: warp w holds row w (the
+// x-derivative terms) and column w (the y-derivative terms) in registers,
+// the derivative matrix from constant memory with compile-time subscripts.
+// u in B0 ([NN][32], tensor order; overwritten on curved elements), B1 an
+// exchange buffer; entered with B0 filled and the block synchronised, left
+// with both buffers still being read (synchronise before reusing them).
 template <int NP>
-__global__ void __launch_bounds__(256) k_x_constrain(MeshView M, MxParams P, double *__restrict__ Ye) {
-  constexpr int NN = NP * NP, NE = 4 * (NP - 1);
+__device__ __forceinline__ void line_apply64(const MeshView &M, int e, double hc, double *B0, double *B1,
+                                             double out[NP]) {
+  constexpr int NN = NP * NP, DO = DOff<NP>::v;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t eo = (size_t)e * NN;
+  double ur[NP], R[NP], S[NP];
+  {
+    double uc[NP];
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      ur[j] = B0[(w * NP + j) * MX_CH + lane];
+      uc[j] = B0[(j * NP + w) * MX_CH + lane];
+    }
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      double r = 0.0, s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NP; k++) {
+        r += ur[k] * c_Dd[DO + j * NP + k];
+        s += c_Dd[DO + j * NP + k] * uc[k];
+      }
+      R[j] = r;
+      S[j] = s;
+    }
+  }
+  if (M.hasQ3[e]) {
+    __syncthreads();  // every warp has its u lines: B0 is free
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      B1[(w * NP + j) * MX_CH + lane] = R[j];
+      B0[(j * NP + w) * MX_CH + lane] = S[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      const double s_wj = B0[(w * NP + j) * MX_CH + lane], r_jw = B1[(j * NP + w) * MX_CH + lane];
+      R[j] = M.Q1[eo + w * NP + j] * R[j] + M.Q3[eo + w * NP + j] * s_wj;
+      S[j] = M.Q2[eo + j * NP + w] * S[j] + M.Q3[eo + j * NP + w] * r_jw;
+    }
+    __syncthreads();  // B1 is free for the column results
+  } else {
+#pragma unroll
+    for (int j = 0; j < NP; j++) {
+      R[j] *= M.Q1[eo + w * NP + j];
+      S[j] *= M.Q2[eo + j * NP + w];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    double a = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) a += c_Dd[DO + k * NP + i] * S[k];
+    B1[(i * NP + w) * MX_CH + lane] = a;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NP; j++) {
+    double b = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) b += R[k] * c_Dd[DO + k * NP + j];
+    const int t = w * NP + j;
+    out[j] = M.Q4[eo + t] * ur[j] * hc + B1[t * MX_CH + lane] + b;
+  }
+}
+
+// Dynamic shared memory of the FP64 element kernels: two [NN][32] buffers
+// and the [32][NN | 1] forcing stage.
+constexpr size_t x64_smem(int np) {
+  return (2 * (size_t)np * np * MX_CH + (size_t)MX_CH * ((np * np) | 1)) * sizeof(double);
+}
+
+// Ye at edge-map slot a = -(M f + H g) (Field::constrain), NP warps per
+// (element, 32 planes).  The forcing of the 32 planes is staged plane by
+// plane with coalesced loads into [32][NN | 1] (an odd row stride keeps the
+// lanes' column reads on distinct bank pairs), then read by lane.
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, 2) k_x_constrain(MeshView M, MxParams P, double *__restrict__ Ye) {
+  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, TS = NN | 1;
   extern __shared__ __align__(16) double smx[];
-  double *F = smx, *U = F + NN * MX_CH, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
-  __shared__ double D[NN], Q[5][NN];
-  __shared__ int emap[NN];
-  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  double *B0 = smx, *B1 = B0 + NN * MX_CH, *T = B1 + NN * MX_CH;
+  __shared__ int gtab[NN], emt[NN], tsl[NN];
+  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p0 = blockIdx.y * MX_CH, p = p0 + lane;
   const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 256) {
-    D[i] = M.D[i];
-    Q[0][i] = M.Q1[eo + i];
-    Q[1][i] = M.Q2[eo + i];
-    Q[2][i] = M.Q3[eo + i];
-    Q[3][i] = M.Q4[eo + i];
-    Q[4][i] = M.Q8[eo + i];
-    emap[i] = M.emap[i];
+  for (int a = threadIdx.x; a < NN; a += NP * 32) {
+    gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
+    emt[a] = M.emap[a];
+    tsl[a] = M.pmap[a];
+  }
+  for (int i = threadIdx.x; i < MX_CH * NN; i += NP * 32) {
+    const int q = i / NN, k = i - q * NN, pl = p0 + q;
+    T[q * TS + k] = real_plane(P, pl) ? P.f[(size_t)pl * P.stride + eo + k] : 0.0;
   }
   __syncthreads();
-  // transpose the forcing in: plane by plane, contiguous element values
-  for (int q = 0; q < MX_CH; q++) {
-    const int pl = p0 + q;
-    const bool rp = real_plane(P, pl);
-    for (int k = tid; k < NN; k += 256)
-      F[k * MX_CH + q] = rp ? Q[4][k] * P.f[(size_t)pl * P.stride + eo + k] : 0.0;
-  }
-  __syncthreads();
-  if (M.emask[e]) {
+  double F[NP];
+#pragma unroll
+  for (int j = 0; j < NP; j++) F[j] = M.Q8[eo + w * NP + j] * T[lane * TS + w * NP + j];
+  if (M.emask[e]) {  // block-uniform: H g, g the essential values
     const double *g = P.gess + (size_t)p * M.nglobal;
     const bool rp = real_plane(P, p);
-    for (int a = row; a < NN; a += MX_ROWS)
-      U[emap[a] * MX_CH + lane] = (rp && a < NE) ? g[M.btog[(size_t)e * NE + a]] : 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      const int a = w + k * NP;
+      B0[emt[a] * MX_CH + lane] = (rp && a < NE) ? g[gtab[a]] : 0.0;
+    }
     __syncthreads();
-    op_stage1<NP, double>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
-    __syncthreads();
-    const double hc = P.hcon[p];
-    for (int idx = row; idx < NN; idx += MX_ROWS)
-      F[idx * MX_CH + lane] += op_stage2<NP, double>(D, Q[3], hc, U, R, S, idx);
-    __syncthreads();
+    double hg[NP];
+    line_apply64<NP>(M, e, P.hcon[p], B0, B1, hg);
+#pragma unroll
+    for (int j = 0; j < NP; j++) F[j] += hg[j];
   }
-  for (int a = row; a < NN; a += MX_ROWS) Ye[ye_index(M, e, a, P.PP) + p] = -F[emap[a] * MX_CH + lane];
+#pragma unroll
+  for (int j = 0; j < NP; j++) {
+    const int t = w * NP + j;
+    Ye[ye_index(M, e, tsl[t], P.PP) + p] = -F[j];
+  }
 }
 
 // b = DSS(Ye) + <h,w>, essential tail zero; x = 0, r = b (FP32); per-plane
@@ -680,33 +707,34 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
 // FP64 residual
 // ---------------------------------------------------------------------------
 
+// Ye = A_e x at the element's slots (FP64), NP warps per (element, 32
+// planes): x gathered through btog in slot order, the operator on tensor
+// lines (line_apply64).
 template <int NP>
-__global__ void __launch_bounds__(256) k_x_op64(MeshView M, MxParams P, const double *__restrict__ x64,
-                                                double *__restrict__ Ye) {
-  constexpr int NN = NP * NP;
+__global__ void __launch_bounds__(NP * 32, 2) k_x_op64(MeshView M, MxParams P, const double *__restrict__ x64,
+                                                    double *__restrict__ Ye) {
+  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
   extern __shared__ __align__(16) double smx[];
-  double *U = smx, *R = U + NN * MX_CH, *S = R + NN * MX_CH;
-  __shared__ double D[NN], Q[4][NN];
-  __shared__ int emap[NN];
-  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  double *B0 = smx, *B1 = B0 + NN * MX_CH;
+  __shared__ int gtab[NN], emt[NN], tsl[NN];
+  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
-  const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 256) {
-    D[i] = M.D[i];
-    Q[0][i] = M.Q1[eo + i];
-    Q[1][i] = M.Q2[eo + i];
-    Q[2][i] = M.Q3[eo + i];
-    Q[3][i] = M.Q4[eo + i];
-    emap[i] = M.emap[i];
+  for (int a = threadIdx.x; a < NN; a += NP * 32) {
+    gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
+    emt[a] = M.emap[a];
+    tsl[a] = M.pmap[a];
   }
   __syncthreads();
-  for (int a = row; a < NN; a += MX_ROWS) U[emap[a] * MX_CH + lane] = x64[(size_t)gidx(M, e, a) * PP + p];
+  double xv[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) xv[k] = x64[(size_t)gtab[w + k * NP] * PP + p];
+#pragma unroll
+  for (int k = 0; k < NP; k++) B0[emt[w + k * NP] * MX_CH + lane] = xv[k];
   __syncthreads();
-  op_stage1<NP, double>(D, Q[0], Q[1], Q[2], M.hasQ3[e] != 0, U, R, S);
-  __syncthreads();
-  const double hc = P.hcon[p];
-  for (int a = row; a < NN; a += MX_ROWS)
-    Ye[ye_index(M, e, a, PP) + p] = op_stage2<NP, double>(D, Q[3], hc, U, R, S, emap[a]);
+  double out[NP];
+  line_apply64<NP>(M, e, P.hcon[p], B0, B1, out);
+#pragma unroll
+  for (int j = 0; j < NP; j++) Ye[ye_index(M, e, tsl[w * NP + j], PP) + p] = out[j];
 }
 
 // r = b - A x (FP64), essential tail zero; the next round's inner solve
@@ -796,11 +824,9 @@ static int grid_nodes(int npts) {
 
 template <int NP>
 static int set_smem_attrs() {
-  constexpr int NN = NP * NP;
   SX_CUDA(cudaFuncSetAttribute(k_x_constrain<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(4 * NN * MX_CH * sizeof(double))));
-  SX_CUDA(cudaFuncSetAttribute(k_x_op64<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(3 * NN * MX_CH * sizeof(double))));
+                               (int)x64_smem(NP)));
+  SX_CUDA(cudaFuncSetAttribute(k_x_op64<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x64_smem(NP)));
   SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_smem(NP)));
   // the largest carveout, so that cg_min_blocks(NP) blocks fit an SM
   SX_CUDA(cudaFuncSetAttribute(k_cg<NP>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -845,7 +871,7 @@ static CgVecs cg_vecs(MixedWork &W) {
 }
 
 static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream_t st, int *nl) {
-  const int nch = W.PP / MX_CH, NN = M.npnp;
+  const int nch = W.PP / MX_CH;
   const MxParams P = W.prm;
   const MxScalPtrs s = scal_ptrs(W);
   *nl = 0;
@@ -853,8 +879,8 @@ static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream
     k_x_ess<<<W.PP, 32, 0, st>>>(M, P);
     (*nl)++;
   }
-  const size_t sm64x4 = 4 * NN * MX_CH * sizeof(double);
-  SX_NP_SWITCH_M(M.np, (k_x_constrain<N_><<<dim3(M.nel, nch), 256, sm64x4, st>>>(M, P, W.Ye64.p)));
+  SX_NP_SWITCH_M(M.np,
+                 (k_x_constrain<N_><<<dim3(M.nel, nch), N_ * 32, x64_smem(N_), st>>>(M, P, W.Ye64.p)));
   k_x_rhs<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.x64.p, W.r0.p, s.b2, W.part.p, W.cnt.p);
   *nl += 2;
   SX_CUDA(cudaGetLastError());
@@ -864,11 +890,10 @@ static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream
 // One refinement round: the inner solve from r (r0 buffer, d = 0), x += d,
 // then the FP64 residual into r0 for the next round.
 static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStream_t st, int *nl) {
-  const int nch = W.PP / MX_CH, NN = M.npnp;
+  const int nch = W.PP / MX_CH;
   const MxParams P = W.prm;
   const MxScalPtrs s = scal_ptrs(W);
   const CgVecs V = cg_vecs(W);
-  const size_t sm64 = 3 * NN * MX_CH * sizeof(double);
   const dim3 eg(M.nel, nch);
   *nl = 0;
   SX_NP_SWITCH_M(M.np,
@@ -878,7 +903,7 @@ static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStrea
     SX_NP_SWITCH_M(M.np,
                    (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(M, P, V, it, mode, W.part.p, W.cnt.p)));
   }
-  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, 256, sm64, st>>>(M, P, W.x64.p, W.Ye64.p)));
+  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, N_ * 32, x64_smem(N_), st>>>(M, P, W.x64.p, W.Ye64.p)));
   k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r0.p, s.r2, W.part.p, W.cnt.p);
   *nl = n_inner + 3;
   SX_CUDA(cudaGetLastError());
