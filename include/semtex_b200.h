@@ -242,6 +242,28 @@ SX_API int sx_profile_band_sweeps(sx_modal modal, int reps, void *stream);
  * the next solve starts afresh. */
 SX_API int sx_profile_mixed_iterations(sx_modal modal, int reps, void *stream);
 
+/* ---- multi-mesh batch (no reference counterpart) --------------------------
+ * Solves the planes of several modal systems -- different meshes, element
+ * counts, orders and mode sets -- together, on device buffers.  Each is the
+ * batched form of that system (same answer as sx_field_solve_batched within
+ * the stated tolerance), but the kernels cover all of them at once:
+ *   SX_MIXED_FP32  one launch per kernel and element order covers the tiles
+ *                  of every member of that order (the orders run side by
+ *                  side); refinement rounds continue until every plane of
+ *                  every member meets tol_rel;
+ *   SX_FP64 (and the modes SX_MIXED_FP32 routes to the band Cholesky)
+ *                  one band-sweep launch covers every member's systems.
+ * The launch sequence is captured as CUDA graphs and replayed while the set
+ * of members and their buffers stay the same.  A modal system may appear
+ * once per call.  stats, when non-null, has `count` entries.  The batch
+ * object holds the tables and graphs; it does not own the modal systems. */
+typedef struct sx_batch_s *sx_batch;
+SX_API int sx_batch_create(sx_batch *out);
+SX_API int sx_batch_solve(sx_batch batch, int count, const sx_modal *modals, double *const *d_u,
+                          double *const *d_f, const double *const *d_bc, const int *nz, const int *plane_stride,
+                          int precision, double tol_rel, int max_refine, void *stream, sx_solve_stats *stats);
+SX_API int sx_batch_destroy(sx_batch batch);
+
 /* ---- serving loop (no reference counterpart) -----------------------------
  * A request loop for Helmholtz solves of different meshes, orders and mode
  * counts.  Requests are admitted in arrival order as device slots and memory

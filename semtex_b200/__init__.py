@@ -124,6 +124,10 @@ def _load():
     L.sx_modal_status.argtypes = [vp]
     L.sx_modal_tune.argtypes = [vp, ip, ip]
     L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
+    L.sx_batch_create.argtypes = [P(vp)]
+    L.sx_batch_destroy.argtypes = [vp]
+    L.sx_batch_solve.argtypes = [vp, ip, P(vp), P(vp), P(vp), P(vp), P(ip), P(ip), ip, dp, ip, vp,
+                                 P(SolveStats)]
     L.sx_server_create.argtypes = [P(ServerConfig), P(vp)]
     L.sx_server_submit.argtypes = [vp, P(Request), P(C.c_ulonglong)]
     L.sx_server_wait.argtypes = [vp, C.c_ulonglong, dp, P(ip), P(dp)]
@@ -331,6 +335,43 @@ class ModalMatrixSys:
     def close(self):
         if getattr(self, "h", None) and lib is not None:
             lib.sx_modal_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Multi-mesh batch (sx_batch_solve): the planes of several modal systems
+    -- different meshes, element counts, orders and mode sets -- solved
+    together, each kernel launched once per element order over all members.
+    Holds the tables and captured graphs between calls."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(lib.sx_batch_create(C.byref(h)), "sx_batch_create")
+        self.h = h
+
+    def solve(self, members, precision=MIXED_FP32, tol_rel=1e-12, max_refine=20, stream=0):
+        """members: sequence of (modal, d_u, d_f, d_bc, nz, stride) with device
+        pointers as ints (d_bc may be None).  Returns one stats dict per member."""
+        n = len(members)
+        mods = (C.c_void_p * n)(*[m[0].h for m in members])
+        du = (C.c_void_p * n)(*[m[1] for m in members])
+        df = (C.c_void_p * n)(*[m[2] for m in members])
+        bcs = [m[3] for m in members]
+        dbc = (C.c_void_p * n)(*[b if b else None for b in bcs]) if any(bcs) else None
+        nzs = (C.c_int * n)(*[m[4] for m in members])
+        strides = (C.c_int * n)(*[m[5] for m in members])
+        st = (SolveStats * n)()
+        rc = lib.sx_batch_solve(self.h, n, mods, du, df, dbc, nzs, strides, precision, tol_rel, max_refine,
+                                stream, st)
+        _check(rc, "sx_batch_solve", allow=(OK, WARN_STEP_LIMIT))
+        return [s.as_dict() for s in st]
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.sx_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

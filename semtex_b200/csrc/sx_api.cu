@@ -731,3 +731,266 @@ extern "C" int sx_profile_mixed_iterations(sx_modal s, int reps, void *stream) {
   if (!s) return SX_ERR_ARG;
   return mixed_profile_iterations(s->mesh->view(), s->mixed, reps, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// multi-mesh batch
+// ---------------------------------------------------------------------------
+
+sx_batch_s::~sx_batch_s() {
+  if (dexec) cudaGraphExecDestroy(dexec);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
+  if (aux) cudaStreamDestroy(aux);
+  if (own) cudaStreamDestroy(own);
+}
+
+extern "C" int sx_batch_create(sx_batch *out) {
+  if (!out) return SX_ERR_ARG;
+  *out = new sx_batch_s();
+  return SX_OK;
+}
+
+extern "C" int sx_batch_destroy(sx_batch b) {
+  delete b;
+  return SX_OK;
+}
+
+namespace {
+
+// One member's share of a batch solve.
+struct Part {
+  sx_modal s = nullptr;
+  std::vector<Group> gd;       // plane groups for the band Cholesky
+  std::vector<MxGroup> mg;     // plane groups for the FP32 iterations
+  std::vector<int> jmodes;     // local modes of mg
+  double *u = nullptr, *f = nullptr;
+  const double *bc = nullptr;
+  int nz = 0, stride = 0;
+};
+
+void key_ptr(std::vector<long long> &k, const void *p) { k.push_back((long long)(intptr_t)p); }
+
+}  // namespace
+
+// The band Cholesky part of a batch: per member its RHS kernels, then one
+// band-sweep launch over every member's jobs, then per member the interior
+// back-substitution; captured once per member set and buffers.
+static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaStream_t st) {
+  std::vector<long long> key;
+  for (Part &q : parts) {
+    if (q.gd.empty()) continue;
+    int planes = 0;
+    for (auto &g : q.gd) planes += g.P;
+    SX_TRY(reserve_ws(*q.s, planes));
+    key_ptr(key, q.s);
+    key_ptr(key, q.u);
+    key_ptr(key, q.f);
+    key_ptr(key, q.bc);
+    key_ptr(key, q.s->rhs.p);
+    key_ptr(key, q.s->Fb.p);
+    key_ptr(key, q.s->gess.p);
+    key.push_back(q.nz);
+    key.push_back(q.stride);
+    key.push_back(q.s->forced_cluster);
+    for (auto &g : q.gd) key.push_back(g.mode);
+    key.push_back(-1);
+  }
+  if (key.empty()) return SX_OK;
+  if (b->dexec && graphs && key == b->dkey) {
+    SX_CUDA(cudaGraphLaunch(b->dexec, st));
+    return SX_OK;
+  }
+  if (b->dexec) cudaGraphExecDestroy(b->dexec);
+  b->dexec = nullptr;
+  b->dkey.clear();
+  std::vector<Job> jobs;
+  std::vector<size_t> j0;
+  int maxJ = 1, maxP = 1, forced = 0;
+  for (Part &q : parts) {
+    j0.push_back(jobs.size());
+    if (q.gd.empty()) continue;
+    const long long bcstride = (long long)std::max(q.s->mesh->nbound, 1) * q.s->mesh->np;
+    int slot = 0;
+    for (auto &g : q.gd) {
+      jobs.push_back(make_job(*q.s, g, slot, q.u, q.f, q.bc, q.stride, bcstride));
+      maxJ = std::max(maxJ, jobs.back().J);
+      maxP = std::max(maxP, g.P);
+      slot += g.P;
+    }
+    forced = std::max(forced, q.s->forced_cluster);
+    SX_TRY(prepare_direct_kernels(q.s->mesh->view()));
+  }
+  j0.push_back(jobs.size());
+  if (b->djobs.n < jobs.size()) SX_TRY(b->djobs.alloc(jobs.size()));
+  SX_CUDA(cudaMemcpyAsync(b->djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
+  SX_CUDA(cudaStreamSynchronize(st));
+  b->jobs = jobs;
+  b->C = forced > 0 ? forced
+                    : pick_cluster((int)jobs.size(), std::min(16, std::max(1, maxJ)), maxP <= 2 ? 2 : 8, maxJ + 2);
+  auto body = [&]() -> int {
+    int nl = 0;
+    for (size_t i = 0; i < parts.size(); i++) {
+      if (parts[i].gd.empty()) continue;
+      const std::vector<Job> slice(jobs.begin() + j0[i], jobs.begin() + j0[i + 1]);
+      SX_TRY(direct_rhs_jobs(parts[i].s->mesh->view(), b->djobs.p + j0[i], slice, st, &nl));
+    }
+    SX_TRY(band_sweep_jobs(b->djobs.p, jobs, b->C, st));
+    nl++;
+    for (size_t i = 0; i < parts.size(); i++) {
+      if (parts[i].gd.empty()) continue;
+      SX_TRY(direct_backsub_jobs(parts[i].s->mesh->view(), b->djobs.p + j0[i], (int)(j0[i + 1] - j0[i]), st,
+                                 &nl));
+    }
+    b->dlaunches = nl;
+    return SX_OK;
+  };
+  if (!graphs) return body();
+  cudaGraph_t g = nullptr;
+  SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  const cudaError_t ce = cudaStreamEndCapture(st, &g);
+  if (rc != SX_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  SX_CUDA(ce);
+  const cudaError_t ie = cudaGraphInstantiate(&b->dexec, g, 0);
+  cudaGraphDestroy(g);
+  SX_CUDA(ie);
+  b->dkey = key;
+  SX_CUDA(cudaGraphLaunch(b->dexec, st));
+  return SX_OK;
+}
+
+extern "C" int sx_batch_solve(sx_batch b, int count, const sx_modal *modals, double *const *d_u,
+                              double *const *d_f, const double *const *d_bc, const int *nz, const int *plane_stride,
+                              int precision, double tol_rel, int max_refine, void *stream, sx_solve_stats *stats) {
+  if (!b || count <= 0 || !modals || !d_u || !d_f || !nz || !plane_stride) return SX_ERR_ARG;
+  if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+  std::vector<Part> parts(count);
+  for (int i = 0; i < count; i++) {
+    sx_modal s = modals[i];
+    if (!s || !d_u[i] || !d_f[i] || plane_stride[i] < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+    for (int j = 0; j < i; j++)
+      if (modals[j] == s) {
+        set_error("sx_batch_solve: modal system %d appears twice (members %d and %d)", i, j, i);
+        return SX_ERR_ARG;
+      }
+    Part &q = parts[i];
+    q.s = s;
+    q.u = d_u[i];
+    q.f = d_f[i];
+    q.bc = d_bc ? d_bc[i] : nullptr;
+    q.nz = nz[i];
+    q.stride = plane_stride[i];
+  }
+  if (!b->own) SX_CUDA(cudaStreamCreateWithFlags(&b->own, cudaStreamDefault));
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->own;
+  // plane groups and their routes
+  bool any_direct = false, any_mixed = false;
+  for (Part &q : parts) {
+    std::vector<Group> groups;
+    SX_TRY(plane_groups(*q.s, q.nz, groups));
+    if (!q.s->dstatus.p) {
+      SX_TRY(q.s->dstatus.alloc(1));
+      SX_TRY(q.s->dstatus.zero(st));
+    }
+    if (precision == SX_FP64) {
+      for (auto &g : groups)
+        if (q.s->sys[g.mode]->method != SX_DIRECT) {
+          set_error("the batched band solve needs DIRECT systems (local mode %d is not)", g.mode);
+          return SX_ERR_UNSUPPORTED;
+        }
+      q.gd = groups;
+    } else {
+      for (auto &u : q.s->uniq)
+        if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, st));
+      for (auto &g : groups) {
+        const System *S = q.s->sys[g.mode].get();
+        if (route_direct(*q.s, *S, tol_rel, max_refine)) {
+          q.gd.push_back(g);
+        } else {
+          q.mg.push_back({g.mode, g.plane0, g.P, S});
+          q.jmodes.push_back(g.mode);
+        }
+      }
+    }
+    any_direct |= !q.gd.empty();
+    any_mixed |= !q.mg.empty();
+  }
+  const bool graphs = true;
+  cudaStream_t sd = st;  // stream of the band part
+  if (any_direct && any_mixed) {
+    if (!b->aux) SX_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+    if (!b->ev_fork) SX_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    if (!b->ev_join) SX_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    SX_CUDA(cudaEventRecord(b->ev_fork, st));
+    SX_CUDA(cudaStreamWaitEvent(b->aux, b->ev_fork, 0));
+    sd = b->aux;
+  }
+  if (any_direct) SX_TRY(batch_direct(b, parts, graphs, sd));
+  if (any_direct && any_mixed) SX_CUDA(cudaEventRecord(b->ev_join, b->aux));
+  int rc = SX_OK;
+  std::vector<MxItem> items;
+  std::vector<int> item_of(count, -1);
+  if (any_mixed) {
+    std::vector<long long> key;
+    int n_inner = 1;
+    for (int i = 0; i < count; i++) {
+      Part &q = parts[i];
+      if (q.mg.empty()) continue;
+      n_inner = std::max(n_inner, std::max(q.s->n_inner, 1));
+      for (const MxGroup &g : q.mg)
+        n_inner = std::max(n_inner, std::min(CG_ROUND_CAP, cg_round_iters(q.s->mesh->kratio,
+                                                                           g.sys->lambda2 + g.sys->betak2)));
+      q.s->mixed.status = q.s->dstatus.p;
+      MxItem it;
+      it.M = q.s->mesh->view();
+      it.W = &q.s->mixed;
+      it.groups = q.mg;
+      it.nz = q.nz;
+      it.num_modes = q.s->num_modes;
+      it.u = q.u;
+      it.f = q.f;
+      it.bc = q.bc;
+      it.stride = q.stride;
+      item_of[i] = (int)items.size();
+      items.push_back(it);
+      key_ptr(key, q.s);
+      key_ptr(key, q.u);
+      key_ptr(key, q.f);
+      key_ptr(key, q.bc);
+      key_ptr(key, q.s->dstatus.p);
+      key.push_back(q.nz);
+      key.push_back(q.stride);
+      for (int m : q.jmodes) key.push_back(m);
+      key.push_back(-1);
+    }
+    key.push_back(n_inner);
+    const bool rebuild = key != b->mkey;
+    rc = mixed_solve_multi(items, b->mixed, rebuild, tol_rel, max_refine, n_inner, graphs, st);
+    if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT)
+      b->mkey = key;
+    else
+      b->mkey.clear();
+  }
+  if (any_direct && any_mixed) SX_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
+  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+  if (stats) {
+    for (int i = 0; i < count; i++) {
+      sx_solve_stats &S = stats[i];
+      if (item_of[i] >= 0)
+        S = items[item_of[i]].stats;
+      else
+        std::memset(&S, 0, sizeof(S));
+      int dplanes = 0;
+      for (auto &g : parts[i].gd) dplanes += g.P;
+      S.planes_solved += dplanes;
+      S.planes_direct = dplanes;
+      if (dplanes) S.kernel_launches += b->dlaunches;
+    }
+  }
+  if (!stream)
+    for (Part &q : parts) SX_TRY(take_status(q.s, true, st, false));
+  return rc;
+}

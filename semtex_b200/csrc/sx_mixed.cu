@@ -28,6 +28,7 @@
 // Reductions are deterministic trees over the blocks (chunk_sum); the last
 // block forms the next iteration's scalars.  Each refinement round is one
 // captured CUDA graph; the host reads the residual norms between rounds.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -87,16 +88,16 @@ constexpr int RED_GROUP = 32;
 inline int red_groups(int G) { return (G + RED_GROUP - 1) / RED_GROUP; }
 
 template <int ROWS>
-__device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsigned *cnt, int G, double &fa,
-                                          double &fb) {
+__device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsigned *cnt, int blk, int G, int y,
+                                          int nch, double &fa, double &fb) {
   __shared__ double sa[ROWS][MX_CH], sb[ROWS][MX_CH];
   __shared__ int last;
-  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31, y = blockIdx.y;
-  const int p = y * MX_CH + lane, PPc = gridDim.y * MX_CH;
-  const int ngrp = (G + RED_GROUP - 1) / RED_GROUP, grp = blockIdx.x / RED_GROUP;
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = y * MX_CH + lane, PPc = nch * MX_CH;
+  const int ngrp = (G + RED_GROUP - 1) / RED_GROUP, grp = blk / RED_GROUP;
   const int g0 = grp * RED_GROUP, gn = min(RED_GROUP, G - g0);
   double2 *P1 = reinterpret_cast<double2 *>(part), *P2 = P1 + (size_t)G * PPc;
-  unsigned *cg = cnt + gridDim.y + (size_t)y * ngrp;
+  unsigned *cg = cnt + nch + (size_t)y * ngrp;
   // ---- the block's total
   sa[row][lane] = a;
   sb[row][lane] = b;
@@ -107,7 +108,7 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
       ta += sa[r][lane];
       tb += sb[r][lane];
     }
-    P1[(size_t)blockIdx.x * PPc + p] = make_double2(ta, tb);
+    P1[(size_t)blk * PPc + p] = make_double2(ta, tb);
   }
   __threadfence();
   __syncthreads();
@@ -161,14 +162,54 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
 }
 
 // chunk_sum for the 8-warp node kernels, storing the totals.
-__device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, unsigned *cnt, int G, double *outA,
-                                              double *outB) {
+__device__ __forceinline__ void chunk_reduce2(double a, double b, double *part, unsigned *cnt, int blk, int G,
+                                              int y, int nch, double *outA, double *outB) {
   double fa, fb;
-  if (chunk_sum<MX_ROWS>(a, b, part, cnt, G, fa, fb)) {
-    const int p = blockIdx.y * MX_CH + (threadIdx.x & 31);
+  if (chunk_sum<MX_ROWS>(a, b, part, cnt, blk, G, y, nch, fa, fb)) {
+    const int p = y * MX_CH + (threadIdx.x & 31);
     if (outA) outA[p] = fa;
     if (outB) outB[p] = fb;
   }
+}
+
+// ---------------------------------------------------------------------------
+// tiles of a multi-mesh batch
+// ---------------------------------------------------------------------------
+//
+// A multi-mesh batch launches every kernel once over the tiles of all its
+// members of one element order: member m owns tiles [t0[m], t0[m + 1]) of
+// the one-dimensional grid (t0[0] = 0, t0[count] = the grid).  A block finds
+// its member by counting the prefixes at or below its tile (one ballot per
+// 32 members), copies the member's descriptor into shared memory and runs
+// the same body as the single-mesh kernel.
+struct MxTable {
+  const MxMember *mem;
+  const int *t0;  // count + 1 tile prefixes
+  int count;
+};
+
+static_assert(sizeof(MxMember) % 8 == 0, "the descriptor is copied in 8-byte words");
+
+__device__ __forceinline__ bool tile_member(const MxTable &T, MxMember &sB, int &local) {
+  __shared__ int sm;
+  const int t = blockIdx.x;
+  if (threadIdx.x < 32) {
+    int c = 0;
+    for (int k0 = 1; k0 <= T.count; k0 += 32) {
+      const int k = k0 + (int)threadIdx.x;
+      c += __popc(__ballot_sync(0xffffffffu, k <= T.count && T.t0[k] <= t));
+    }
+    if (threadIdx.x == 0) sm = c < T.count ? c : -1;
+  }
+  __syncthreads();
+  const int m = sm;
+  if (m < 0) return false;  // block-uniform: past the last tile
+  local = t - T.t0[m];
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(T.mem + m);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sB);
+  for (int i = threadIdx.x; i < (int)(sizeof(MxMember) / 8); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  return true;
 }
 
 // GLL derivative matrices for np = 3..12, FP32 and FP64, in constant memory:
@@ -215,8 +256,11 @@ static int ensure_constD() {
 // RHS (FP64)
 // ---------------------------------------------------------------------------
 
-__global__ void k_x_ess(MeshView M, MxParams P) {
-  const int p = blockIdx.x;
+// Essential values of plane p into gess (Boundary::set through btog,
+// src/boundary.cpp:50-64); one thread per plane.
+__device__ __forceinline__ void ess_body(const MxMember &B, int p) {
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
   if (threadIdx.x || !P.bc || !real_plane(P, p)) return;
   const int np = M.np, nm = np - 1;
   double *g = P.gess + (size_t)p * M.nglobal;
@@ -232,6 +276,14 @@ __global__ void k_x_ess(MeshView M, MxParams P) {
     else
       g[bmap[side * nm + nm]] = src[nm];
   }
+}
+
+__global__ void k_x_ess(const __grid_constant__ MxMember B) { ess_body(B, blockIdx.x); }
+
+__global__ void k_x_ess_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) ess_body(sB, t);
 }
 
 // (A_e u)(w, j), j = 0..NP-1, in FP64 for the calling warp's tensor row w
@@ -318,13 +370,16 @@ constexpr size_t x64_smem(int np) {
 // plane with coalesced loads into [32][NN | 1] (an odd row stride keeps the
 // lanes' column reads on distinct bank pairs), then read by lane.
 template <int NP>
-__global__ void __launch_bounds__(NP * 32, 2) k_x_constrain(MeshView M, MxParams P, double *__restrict__ Ye) {
+__device__ __forceinline__ void constrain_body(const MxMember &B, int e, int y) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, TS = NN | 1;
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  double *__restrict__ Ye = B.Ye;
   extern __shared__ __align__(16) double smx[];
   double *B0 = smx, *B1 = B0 + NN * MX_CH, *T = B1 + NN * MX_CH;
   __shared__ int gtab[NN], emt[NN], tsl[NN];
-  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p0 = blockIdx.y * MX_CH, p = p0 + lane;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p0 = y * MX_CH, p = p0 + lane;
   const size_t eo = (size_t)e * NN;
   for (int a = threadIdx.x; a < NN; a += NP * 32) {
     gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
@@ -360,17 +415,33 @@ __global__ void __launch_bounds__(NP * 32, 2) k_x_constrain(MeshView M, MxParams
   }
 }
 
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, 2) k_x_constrain(const __grid_constant__ MxMember B) {
+  constrain_body<NP>(B, blockIdx.x, blockIdx.y);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, 2) k_x_constrain_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) constrain_body<NP>(sB, t % sB.M.nel, t / sB.M.nel);
+}
+
 // b = DSS(Ye) + <h,w>, essential tail zero; x = 0, r = b (FP32); per-plane
 // ||b||^2.
-__global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const double *__restrict__ Ye, double *b64,
-                                               double *x64, float *r32, double *b2, double *part, unsigned *cnt) {
+__device__ __forceinline__ void rhs_body(const MxMember &B, int blk, int y) {
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  const double *__restrict__ Ye = B.Ye;
+  double *b64 = B.b64, *x64 = B.V.x64;
+  float *r32 = B.V.r0;
   const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
+  const int p = y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
   const int ns = P.nsolve[p];
   const bool rp = real_plane(P, p);
   double bb = 0.0;
-  for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
+  for (int g = blk * MX_ROWS + row; g < npts; g += B.G * MX_ROWS) {
     double s = 0.0;
     if (g < M.nglobal) {
       if (g < ns) {
@@ -393,7 +464,17 @@ __global__ void __launch_bounds__(256) k_x_rhs(MeshView M, MxParams P, const dou
     r32[o] = (float)s;
     bb += s * s;
   }
-  chunk_reduce2(bb, 0.0, part, cnt, gridDim.x, b2, nullptr);
+  chunk_reduce2(bb, 0.0, B.part, B.cnt, blk, B.G, y, B.nch, B.b2, nullptr);
+}
+
+__global__ void __launch_bounds__(256) k_x_rhs(const __grid_constant__ MxMember B) {
+  rhs_body(B, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(256) k_x_rhs_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) rhs_body(sB, t % sB.G, t / sB.G);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,9 +549,11 @@ constexpr long long CG_WAIT_LIMIT = 2000000000LL;  // clock cycles: about a seco
 constexpr size_t cg_smem(int np) { return (size_t)np * np * (6 * MX_CH + 16) * sizeof(float); }
 
 template <int NP>
-__global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
-    k_cg(MeshView M, MxParams P, CgVecs V, int it, int mode, double *part, unsigned *cnt) {
+__device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it, int mode) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, DO = DOff<NP>::v;
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  const CgVecs &V = B.V;
   constexpr uint32_t SPAN = NN * MX_CH * sizeof(float), PSPAN = NN * 16 * sizeof(float);
   // shared spans, NN * 32 floats each: r, s, p, d (updated in place); B1 =
   // the element's own A u, then the column results (and r on curved
@@ -483,7 +566,7 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
   __shared__ int4 w4[NE];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int staged;
-  const int e = blockIdx.x, y = blockIdx.y, nch = gridDim.y, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nch = B.nch, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = y * MX_CH + lane, PP = P.PP;
   const bool init = mode == CG_INIT, last = mode == CG_LAST;
   const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
@@ -678,7 +761,7 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
   // ---- gamma = (r, u), delta = (A u, u); the chunk's last block forms the
   // next iteration's scalars
   double gn, dn;
-  if (chunk_sum<NP>(gam, del, part, cnt, gridDim.x, gn, dn)) {
+  if (chunk_sum<NP>(gam, del, B.part, B.cnt, e, M.nel, y, nch, gn, dn)) {
     double an, bn;
     if (init) {
       bn = 0.0;
@@ -703,6 +786,19 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
   if (threadIdx.x == 0) bulk_wait_all();  // the stores read shared memory
 }
 
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
+    k_cg(const __grid_constant__ MxMember B, int it, int mode) {
+  cg_body<NP>(B, blockIdx.x, blockIdx.y, it, mode);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP)) k_cg_multi(MxTable T, int it, int mode) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) cg_body<NP>(sB, t % sB.M.nel, t / sB.M.nel, it, mode);
+}
+
 // ---------------------------------------------------------------------------
 // FP64 residual
 // ---------------------------------------------------------------------------
@@ -711,14 +807,17 @@ __global__ void __launch_bounds__(NP * 32, cg_min_blocks(NP))
 // planes): x gathered through btog in slot order, the operator on tensor
 // lines (line_apply64).
 template <int NP>
-__global__ void __launch_bounds__(NP * 32, 2) k_x_op64(MeshView M, MxParams P, const double *__restrict__ x64,
-                                                    double *__restrict__ Ye) {
+__device__ __forceinline__ void op64_body(const MxMember &B, int e, int y) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  const double *__restrict__ x64 = B.V.x64;
+  double *__restrict__ Ye = B.Ye;
   extern __shared__ __align__(16) double smx[];
   double *B0 = smx, *B1 = B0 + NN * MX_CH;
   __shared__ int gtab[NN], emt[NN], tsl[NN];
-  const int e = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = y * MX_CH + lane, PP = P.PP;
   for (int a = threadIdx.x; a < NN; a += NP * 32) {
     gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
     emt[a] = M.emap[a];
@@ -737,18 +836,33 @@ __global__ void __launch_bounds__(NP * 32, 2) k_x_op64(MeshView M, MxParams P, c
   for (int j = 0; j < NP; j++) Ye[ye_index(M, e, tsl[w * NP + j], PP) + p] = out[j];
 }
 
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, 2) k_x_op64(const __grid_constant__ MxMember B) {
+  op64_body<NP>(B, blockIdx.x, blockIdx.y);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(NP * 32, 2) k_x_op64_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) op64_body<NP>(sB, t % sB.M.nel, t / sB.M.nel);
+}
+
 // r = b - A x (FP64), essential tail zero; the next round's inner solve
 // starts from r32 = r (and d = 0, which its first iteration assumes);
 // per-plane ||r||^2.
-__global__ void __launch_bounds__(256) k_x_res(MeshView M, MxParams P, const double *__restrict__ Ye,
-                                               const double *__restrict__ b64, float *r32, double *r2, double *part,
-                                               unsigned *cnt) {
+__device__ __forceinline__ void res_body(const MxMember &B, int blk, int y) {
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  const double *__restrict__ Ye = B.Ye;
+  const double *__restrict__ b64 = B.b64;
+  float *r32 = B.V.r0;
   const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int p = blockIdx.y * MX_CH + lane, PP = P.PP;
+  const int p = y * MX_CH + lane, PP = P.PP;
   const int npts = M.nglobal + M.nel * M.nint;
   const int ns = P.nsolve[p];
   double rr = 0.0;
-  for (int g = blockIdx.x * MX_ROWS + row; g < npts; g += gridDim.x * MX_ROWS) {
+  for (int g = blk * MX_ROWS + row; g < npts; g += B.G * MX_ROWS) {
     double ax = 0.0;
     bool solve = true;
     if (g < M.nglobal) {
@@ -762,19 +876,32 @@ __global__ void __launch_bounds__(256) k_x_res(MeshView M, MxParams P, const dou
     r32[o] = (float)r;
     rr += r * r;
   }
-  chunk_reduce2(rr, 0.0, part, cnt, gridDim.x, r2, nullptr);
+  chunk_reduce2(rr, 0.0, B.part, B.cnt, blk, B.G, y, B.nch, B.r2, nullptr);
+}
+
+__global__ void __launch_bounds__(256) k_x_res(const __grid_constant__ MxMember B) {
+  res_body(B, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(256) k_x_res_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) res_body(sB, t % sB.G, t / sB.G);
 }
 
 // u = x at element nodes, essential values from gess (global2local +
 // setEssential, src/field.cpp:710-713, 1022-1040); transposed back to the
 // caller's plane-major layout through shared memory.
 template <int NP>
-__global__ void __launch_bounds__(256) k_x_unpack(MeshView M, MxParams P, const double *__restrict__ x64) {
+__device__ __forceinline__ void unpack_body(const MxMember &B, int e, int y) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1);
+  const MeshView &M = B.M;
+  const MxParams &P = B.P;
+  const double *__restrict__ x64 = B.V.x64;
   __shared__ double V[NN * MX_CH];
   __shared__ int emap[NN];
-  const int e = blockIdx.x, tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
-  const int p0 = blockIdx.y * MX_CH, p = p0 + lane, PP = P.PP;
+  const int tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
+  const int p0 = y * MX_CH, p = p0 + lane, PP = P.PP;
   for (int i = tid; i < NN; i += 256) emap[i] = M.emap[i];
   __syncthreads();
   const bool masked = M.emask[e] != 0;
@@ -795,6 +922,18 @@ __global__ void __launch_bounds__(256) k_x_unpack(MeshView M, MxParams P, const 
     double *u = P.u + (size_t)pl * P.stride + (size_t)e * NN;
     for (int k = tid; k < NN; k += 256) u[k] = V[k * MX_CH + q];
   }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256) k_x_unpack(const __grid_constant__ MxMember B) {
+  unpack_body<NP>(B, blockIdx.x, blockIdx.y);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256) k_x_unpack_multi(MxTable T) {
+  __shared__ MxMember sB;
+  int t;
+  if (tile_member(T, sB, t)) unpack_body<NP>(sB, t % sB.M.nel, t / sB.M.nel);
 }
 
 // ---------------------------------------------------------------------------
@@ -870,18 +1009,34 @@ static CgVecs cg_vecs(MixedWork &W) {
   return v;
 }
 
-static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream_t st, int *nl) {
-  const int nch = W.PP / MX_CH;
-  const MxParams P = W.prm;
+// The kernels' descriptor of a solve on mesh M with workspace W (W.prm set).
+static MxMember member_of(const MeshView &M, MixedWork &W) {
   const MxScalPtrs s = scal_ptrs(W);
+  MxMember B;
+  std::memset(&B, 0, sizeof(B));
+  B.M = M;
+  B.P = W.prm;
+  B.V = cg_vecs(W);
+  B.Ye = W.Ye64.p;
+  B.b64 = W.b64.p;
+  B.r2 = s.r2;
+  B.b2 = s.b2;
+  B.part = W.part.p;
+  B.cnt = W.cnt.p;
+  B.nch = W.PP / MX_CH;
+  B.G = W.G;
+  return B;
+}
+
+static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream_t st, int *nl) {
+  const MxMember B = member_of(M, W);
   *nl = 0;
   if (any_bc) {
-    k_x_ess<<<W.PP, 32, 0, st>>>(M, P);
+    k_x_ess<<<W.PP, 32, 0, st>>>(B);
     (*nl)++;
   }
-  SX_NP_SWITCH_M(M.np,
-                 (k_x_constrain<N_><<<dim3(M.nel, nch), N_ * 32, x64_smem(N_), st>>>(M, P, W.Ye64.p)));
-  k_x_rhs<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.x64.p, W.r0.p, s.b2, W.part.p, W.cnt.p);
+  SX_NP_SWITCH_M(M.np, (k_x_constrain<N_><<<dim3(M.nel, B.nch), N_ * 32, x64_smem(N_), st>>>(B)));
+  k_x_rhs<<<dim3(W.G, B.nch), 256, 0, st>>>(B);
   *nl += 2;
   SX_CUDA(cudaGetLastError());
   return SX_OK;
@@ -890,21 +1045,16 @@ static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream
 // One refinement round: the inner solve from r (r0 buffer, d = 0), x += d,
 // then the FP64 residual into r0 for the next round.
 static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStream_t st, int *nl) {
-  const int nch = W.PP / MX_CH;
-  const MxParams P = W.prm;
-  const MxScalPtrs s = scal_ptrs(W);
-  const CgVecs V = cg_vecs(W);
-  const dim3 eg(M.nel, nch);
+  const MxMember B = member_of(M, W);
+  const dim3 eg(M.nel, B.nch);
   *nl = 0;
-  SX_NP_SWITCH_M(M.np,
-                 (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(M, P, V, 0, CG_INIT, W.part.p, W.cnt.p)));
+  SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(B, 0, CG_INIT)));
   for (int it = 0; it < n_inner; it++) {
     const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
-    SX_NP_SWITCH_M(M.np,
-                   (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(M, P, V, it, mode, W.part.p, W.cnt.p)));
+    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(B, it, mode)));
   }
-  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, N_ * 32, x64_smem(N_), st>>>(M, P, W.x64.p, W.Ye64.p)));
-  k_x_res<<<dim3(W.G, nch), 256, 0, st>>>(M, P, W.Ye64.p, W.b64.p, W.r0.p, s.r2, W.part.p, W.cnt.p);
+  SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, N_ * 32, x64_smem(N_), st>>>(B)));
+  k_x_res<<<dim3(W.G, B.nch), 256, 0, st>>>(B);
   *nl = n_inner + 3;
   SX_CUDA(cudaGetLastError());
   return SX_OK;
@@ -913,11 +1063,9 @@ static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStrea
 int mixed_profile_iterations(const MeshView &M, MixedWork &W, int reps, cudaStream_t st) {
   // iteration 1 reads what iteration 0 of the last round wrote
   if (W.PP == 0 || W.n_inner < 2 || reps <= 0) return SX_ERR_ARG;
-  const int nch = W.PP / MX_CH;
-  const CgVecs V = cg_vecs(W);
+  const MxMember B = member_of(M, W);
   for (int r = 0; r < reps; r++)
-    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, nch), N_ * 32, cg_smem(N_), st>>>(M, W.prm, V, 1, CG_ITER,
-                                                                                    W.part.p, W.cnt.p)));
+    SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, B.nch), N_ * 32, cg_smem(N_), st>>>(B, 1, CG_ITER)));
   SX_CUDA(cudaGetLastError());
   return SX_OK;
 }
@@ -1028,7 +1176,38 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
                                                                                W.pcE.p);
   SX_CUDA(cudaGetLastError());
   SX_CUDA(cudaStreamSynchronize(st));
+  W.epoch++;
   return SX_OK;
+}
+
+static void bind_params(const MeshView &M, MixedWork &W, int nz, double *d_u, double *d_f, const double *d_bc,
+                        long long stride) {
+  MxParams &P = W.prm;
+  P.PP = W.PP;
+  P.nz = nz;
+  P.active = W.active.p;
+  P.M = W.M;
+  P.hcon = W.hcon.p;
+  P.nsolve = W.nsolve.p;
+  P.pcf = W.pcf.p;
+  P.f = d_f;
+  P.u = d_u;
+  P.stride = stride;
+  P.bc = d_bc;
+  P.bcstride = (long long)std::max(M.nbound, 1) * M.np;
+  P.gess = W.gess.p;
+}
+
+// Largest relative residual over the planes of one member from its norms
+// (r2[0..PP), b2[0..PP)); infinity for a NaN.
+static double worst_rel(const double *r2, const double *b2, int PP) {
+  double worst = 0.0;
+  for (int p = 0; p < PP; p++) {
+    const double rel = b2[p] > 0.0 ? std::sqrt(std::max(r2[p], 0.0) / b2[p]) : 0.0;
+    if (!(rel == rel)) return INFINITY;
+    worst = std::max(worst, rel);
+  }
+  return worst;
 }
 
 int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
@@ -1040,7 +1219,7 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     return SX_ERR_UNSUPPORTED;
   }
   SX_TRY(ensure_constD());
-  if (rebuild || !graphs || !W.g_init || W.n_inner != n_inner) {
+  if (rebuild || !graphs || !W.g_init || W.n_inner != n_inner || W.graph_epoch != W.epoch) {
     if (W.g_init) cudaGraphExecDestroy(W.g_init);
     if (W.g_round) cudaGraphExecDestroy(W.g_round);
     W.g_init = W.g_round = nullptr;
@@ -1048,26 +1227,14 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     int attr_rc = SX_OK;
     SX_NP_SWITCH_M(M.np, (attr_rc = set_smem_attrs<N_>()));
     SX_TRY(attr_rc);
-    MxParams &P = W.prm;
-    P.PP = W.PP;
-    P.nz = nz;
-    P.active = W.active.p;
-    P.M = W.M;
-    P.hcon = W.hcon.p;
-    P.nsolve = W.nsolve.p;
-    P.pcf = W.pcf.p;
-    P.f = d_f;
-    P.u = d_u;
-    P.stride = stride;
-    P.bc = d_bc;
-    P.bcstride = (long long)std::max(M.nbound, 1) * M.np;
-    P.gess = W.gess.p;
+    bind_params(M, W, nz, d_u, d_f, d_bc, stride);
     if (graphs) {
       const bool any_bc = d_bc != nullptr;
       SX_TRY(capture(st, &W.g_init, [&]() { return enqueue_init(M, W, any_bc, st, &W.launches_init); }));
       SX_TRY(capture(st, &W.g_round, [&]() { return enqueue_round(M, W, n_inner, st, &W.launches_round); }));
     }
     W.n_inner = n_inner;
+    W.graph_epoch = W.epoch;
   }
   // essential values: zeroed here, set from the BC lines inside g_init
   SX_CUDA(cudaMemsetAsync(W.gess.p, 0, sizeof(double) * (size_t)W.PP * M.nglobal, st));
@@ -1087,17 +1254,11 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     // r2 and b2 lead the scalar block
     SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(double) * 2 * PP, cudaMemcpyDeviceToHost, st));
     SX_CUDA(cudaStreamSynchronize(st));
-    worst = 0.0;
-    for (int p = 0; p < PP; p++) {
-      const double r2 = W.hscal[p], b2 = W.hscal[PP + p];
-      const double rel = b2 > 0.0 ? std::sqrt(std::max(r2, 0.0) / b2) : 0.0;
-      if (!(rel == rel)) worst = INFINITY;  // NaN
-      worst = std::max(worst, rel);
-    }
+    worst = worst_rel(W.hscal.data(), W.hscal.data() + PP, PP);
     if (worst <= tol_rel) break;
   }
   if (rounds > max_refine) rounds = max_refine;
-  SX_NP_SWITCH_M(M.np, (k_x_unpack<N_><<<dim3(M.nel, PP / MX_CH), 256, 0, st>>>(M, W.prm, W.x64.p)));
+  SX_NP_SWITCH_M(M.np, (k_x_unpack<N_><<<dim3(M.nel, PP / MX_CH), 256, 0, st>>>(member_of(M, W))));
   SX_CUDA(cudaGetLastError());
   int solved = 0;
   for (const MxGroup &g : groups) solved += g.P;
@@ -1111,6 +1272,241 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     stats->kernel_launches = launches;
   }
   return worst <= tol_rel ? SX_OK : SX_WARN_STEP_LIMIT;
+}
+
+// ---------------------------------------------------------------------------
+// multi-mesh batch
+// ---------------------------------------------------------------------------
+
+void MxBatch::reset() {
+  if (g_init) cudaGraphExecDestroy(g_init);
+  if (g_round) cudaGraphExecDestroy(g_round);
+  g_init = g_round = nullptr;
+  cls.clear();
+  order.clear();
+  noff.clear();
+  epochs.clear();
+}
+
+MxBatch::~MxBatch() {
+  reset();
+  for (cudaEvent_t e : events) cudaEventDestroy(e);
+  for (cudaStream_t s : streams) cudaStreamDestroy(s);
+}
+
+// The three tile tables of class c: element, node and plane tiles.
+static MxTable class_table(const MxBatch &B, const MxBatch::Class &c, int kind) {
+  MxTable T;
+  T.mem = B.mem.p + c.m0;
+  T.t0 = B.tiles.p + c.t0 + (size_t)kind * (c.count + 1);
+  T.count = c.count;
+  return T;
+}
+
+// Runs body(c, stream) for every class, each on its own stream, forked from
+// and joined back into st (inside a capture this makes parallel branches).
+// The class streams and events, created before any capture.
+static int ensure_streams(MxBatch &B) {
+  const int nc = (int)B.cls.size();
+  if (nc < 2) return SX_OK;
+  while ((int)B.streams.size() < nc) {
+    cudaStream_t s = nullptr;
+    SX_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    B.streams.push_back(s);
+  }
+  while ((int)B.events.size() < nc + 1) {
+    cudaEvent_t e = nullptr;
+    SX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    B.events.push_back(e);
+  }
+  return SX_OK;
+}
+
+static int per_class(MxBatch &B, cudaStream_t st,
+                     const std::function<int(const MxBatch::Class &, cudaStream_t)> &body) {
+  const int nc = (int)B.cls.size();
+  if (nc == 1) return body(B.cls[0], st);
+  SX_TRY(ensure_streams(B));
+  SX_CUDA(cudaEventRecord(B.events[0], st));
+  int rc = SX_OK;
+  for (int c = 0; c < nc; c++) {
+    SX_CUDA(cudaStreamWaitEvent(B.streams[c], B.events[0], 0));
+    if (rc == SX_OK) rc = body(B.cls[c], B.streams[c]);
+    SX_CUDA(cudaEventRecord(B.events[c + 1], B.streams[c]));
+  }
+  for (int c = 0; c < nc; c++) SX_CUDA(cudaStreamWaitEvent(st, B.events[c + 1], 0));
+  return rc;
+}
+
+static int enqueue_init_multi(MxBatch &B, bool any_bc, cudaStream_t st, int *nl) {
+  *nl = 0;
+  for (auto &c : B.cls) *nl += any_bc ? 3 : 2;
+  return per_class(B, st, [&](const MxBatch::Class &c, cudaStream_t s) {
+    if (any_bc) k_x_ess_multi<<<c.tp, 32, 0, s>>>(class_table(B, c, 2));
+    SX_NP_SWITCH_M(c.np, (k_x_constrain_multi<N_><<<c.te, N_ * 32, x64_smem(N_), s>>>(class_table(B, c, 0))));
+    k_x_rhs_multi<<<c.tn, 256, 0, s>>>(class_table(B, c, 1));
+    SX_CUDA(cudaGetLastError());
+    return SX_OK;
+  });
+}
+
+static int enqueue_round_multi(MxBatch &B, int n_inner, cudaStream_t st, int *nl) {
+  *nl = (int)B.cls.size() * (n_inner + 3);
+  return per_class(B, st, [&](const MxBatch::Class &c, cudaStream_t s) {
+    const MxTable Te = class_table(B, c, 0), Tn = class_table(B, c, 1);
+    SX_NP_SWITCH_M(c.np, (k_cg_multi<N_><<<c.te, N_ * 32, cg_smem(N_), s>>>(Te, 0, CG_INIT)));
+    for (int it = 0; it < n_inner; it++) {
+      const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
+      SX_NP_SWITCH_M(c.np, (k_cg_multi<N_><<<c.te, N_ * 32, cg_smem(N_), s>>>(Te, it, mode)));
+    }
+    SX_NP_SWITCH_M(c.np, (k_x_op64_multi<N_><<<c.te, N_ * 32, x64_smem(N_), s>>>(Te)));
+    k_x_res_multi<<<c.tn, 256, 0, s>>>(Tn);
+    SX_CUDA(cudaGetLastError());
+    return SX_OK;
+  });
+}
+
+template <int NP>
+static int set_smem_attrs_multi() {
+  SX_CUDA(cudaFuncSetAttribute(k_x_constrain_multi<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)x64_smem(NP)));
+  SX_CUDA(cudaFuncSetAttribute(k_x_op64_multi<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)x64_smem(NP)));
+  SX_CUDA(cudaFuncSetAttribute(k_cg_multi<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_smem(NP)));
+  SX_CUDA(cudaFuncSetAttribute(k_cg_multi<NP>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  return SX_OK;
+}
+
+int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, double tol_rel, int max_refine,
+                      int n_inner, bool graphs, cudaStream_t st) {
+  const int n = (int)items.size();
+  if (n == 0) return SX_OK;
+  for (const MxItem &it : items) {
+    if (it.M.mixed) {
+      set_error("mixed-precision form does not take Robin (mixed) boundary conditions");
+      return SX_ERR_UNSUPPORTED;
+    }
+    if (it.groups.empty() || !it.W) return SX_ERR_ARG;
+  }
+  SX_TRY(ensure_constD());
+  bool any_bc = false;
+  for (const MxItem &it : items) any_bc |= it.bc != nullptr;
+  bool stale = (int)B.order.size() != n || B.epochs.size() != B.order.size();
+  for (int m = 0; !stale && m < n; m++) stale = items[B.order[m]].W->epoch != B.epochs[m];
+  if (rebuild || stale || !graphs || !B.g_init || B.n_inner != n_inner) {
+    B.reset();
+    // members by element order, then item order
+    B.order.resize(n);
+    for (int i = 0; i < n; i++) B.order[i] = i;
+    std::stable_sort(B.order.begin(), B.order.end(),
+                     [&](int a, int b) { return items[a].M.np < items[b].M.np; });
+    std::vector<MxMember> mem(n);
+    size_t ntot = 0;
+    for (int m = 0; m < n; m++) {
+      MxItem &it = items[B.order[m]];
+      SX_TRY(setup(it.M, *it.W, it.groups, it.nz, it.num_modes, st));
+      int attr_rc = SX_OK;
+      SX_NP_SWITCH_M(it.M.np, (attr_rc = set_smem_attrs_multi<N_>()));
+      SX_TRY(attr_rc);
+      bind_params(it.M, *it.W, it.nz, it.u, it.f, it.bc, it.stride);
+      B.noff.push_back(ntot);
+      ntot += 2 * (size_t)it.W->PP;
+    }
+    SX_TRY(B.norms.n < ntot ? B.norms.alloc(ntot) : SX_OK);
+    B.hnorms.assign(ntot, 0.0);
+    std::vector<int> tiles;
+    for (int m = 0; m < n; m++) {
+      MxItem &it = items[B.order[m]];
+      mem[m] = member_of(it.M, *it.W);
+      mem[m].r2 = B.norms.p + B.noff[m];
+      mem[m].b2 = mem[m].r2 + it.W->PP;
+      if (B.cls.empty() || B.cls.back().np != it.M.np) {
+        MxBatch::Class c;
+        c.np = it.M.np;
+        c.m0 = m;
+        B.cls.push_back(c);
+      }
+      B.cls.back().count++;
+    }
+    for (auto &c : B.cls) {
+      c.t0 = tiles.size();
+      std::vector<int> te(1, 0), tn(1, 0), tp(1, 0);
+      for (int m = c.m0; m < c.m0 + c.count; m++) {
+        const MxMember &b = mem[m];
+        te.push_back(te.back() + b.M.nel * b.nch);
+        tn.push_back(tn.back() + b.G * b.nch);
+        tp.push_back(tp.back() + b.P.PP);
+      }
+      c.te = te.back();
+      c.tn = tn.back();
+      c.tp = tp.back();
+      tiles.insert(tiles.end(), te.begin(), te.end());
+      tiles.insert(tiles.end(), tn.begin(), tn.end());
+      tiles.insert(tiles.end(), tp.begin(), tp.end());
+    }
+    B.epochs.clear();
+    for (int m = 0; m < n; m++) B.epochs.push_back(items[B.order[m]].W->epoch);
+    SX_TRY(B.mem.n < (size_t)n ? B.mem.alloc(n) : SX_OK);
+    SX_TRY(B.tiles.n < tiles.size() ? B.tiles.alloc(tiles.size()) : SX_OK);
+    SX_CUDA(cudaMemcpyAsync(B.mem.p, mem.data(), sizeof(MxMember) * n, cudaMemcpyHostToDevice, st));
+    SX_CUDA(cudaMemcpyAsync(B.tiles.p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, st));
+    SX_CUDA(cudaStreamSynchronize(st));
+    SX_TRY(ensure_streams(B));
+    if (graphs) {
+      SX_TRY(capture(st, &B.g_init, [&]() { return enqueue_init_multi(B, any_bc, st, &B.launches_init); }));
+      SX_TRY(capture(st, &B.g_round, [&]() { return enqueue_round_multi(B, n_inner, st, &B.launches_round); }));
+    }
+    B.n_inner = n_inner;
+  }
+  // essential values: zeroed here, set from the BC lines inside the init
+  for (const MxItem &it : items)
+    SX_CUDA(cudaMemsetAsync(it.W->gess.p, 0, sizeof(double) * (size_t)it.W->PP * it.M.nglobal, st));
+  if (graphs)
+    SX_CUDA(cudaGraphLaunch(B.g_init, st));
+  else
+    SX_TRY(enqueue_init_multi(B, any_bc, st, &B.launches_init));
+  int rounds = 0, launches = B.launches_init + (int)B.cls.size();
+  std::vector<double> worst(n, 0.0);
+  for (rounds = 1; rounds <= max_refine; rounds++) {
+    if (graphs)
+      SX_CUDA(cudaGraphLaunch(B.g_round, st));
+    else
+      SX_TRY(enqueue_round_multi(B, n_inner, st, &B.launches_round));
+    launches += B.launches_round;
+    SX_CUDA(cudaMemcpyAsync(B.hnorms.data(), B.norms.p, sizeof(double) * B.hnorms.size(), cudaMemcpyDeviceToHost,
+                            st));
+    SX_CUDA(cudaStreamSynchronize(st));
+    bool all = true;
+    for (int m = 0; m < n; m++) {
+      const int PP = items[B.order[m]].W->PP;
+      const double *r2 = B.hnorms.data() + B.noff[m];
+      worst[m] = worst_rel(r2, r2 + PP, PP);
+      all &= worst[m] <= tol_rel;
+    }
+    if (all) break;
+  }
+  if (rounds > max_refine) rounds = max_refine;
+  SX_TRY(per_class(B, st, [&](const MxBatch::Class &c, cudaStream_t s) {
+    SX_NP_SWITCH_M(c.np, (k_x_unpack_multi<N_><<<c.te, 256, 0, s>>>(class_table(B, c, 0))));
+    SX_CUDA(cudaGetLastError());
+    return SX_OK;
+  }));
+  int rc = SX_OK;
+  for (int m = 0; m < n; m++) {
+    MxItem &it = items[B.order[m]];
+    int solved = 0;
+    for (const MxGroup &g : it.groups) solved += g.P;
+    sx_solve_stats &S = it.stats;
+    std::memset(&S, 0, sizeof(S));
+    S.planes_solved = solved;
+    S.refinements = rounds;
+    S.iterations_max = rounds * n_inner;
+    S.iterations_total = rounds * n_inner * solved;
+    S.final_rel_residual = worst[m];
+    S.kernel_launches = launches;
+    if (!(worst[m] <= tol_rel)) rc = SX_WARN_STEP_LIMIT;
+  }
+  return rc;
 }
 
 }  // namespace sx

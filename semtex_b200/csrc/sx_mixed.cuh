@@ -3,6 +3,8 @@
 // plane-interleaved vectors.
 #pragma once
 
+#include <vector>
+
 #include "sx_internal.h"
 
 namespace sx {
@@ -49,11 +51,27 @@ struct CgVecs {
   float *rE, *sE, *pE, *dE;
   float *WE[2];       // A u at every element node (unassembled)
   const float *pcE;   // inverse Jacobi diagonal, [e][y][t][16] by mode pair
-  const float *r0;    // residual of the last refinement step, [npts][PP]
+  float *r0;          // residual of the last refinement step, [npts][PP]
   double *x64;
   double *gam[2], *alpha[2], *beta[2];
   double *gam0;       // gamma at the start of the round
   int *status;        // device status bits (1 << SX_ERR_*)
+};
+
+// Everything the kernels of one solve read and write: the mesh, the
+// per-plane constants, the CG vectors and scalars, and the reduction
+// scratch.  A single-mesh solve passes it as a kernel parameter; a
+// multi-mesh batch keeps one per member in device memory.
+struct MxMember {
+  MeshView M;
+  MxParams P;
+  CgVecs V;
+  double *Ye, *b64;  // FP64 element results, FP64 RHS [npts][PP]
+  double *r2, *b2;   // per-plane ||r||^2 and ||b||^2, read by the host
+  double *part;      // reduction partials
+  unsigned *cnt;     // reduction counters
+  int nch;           // plane chunks of 32 (P.PP / 32)
+  int G;             // blocks per chunk of the node kernels
 };
 
 struct MixedWork {
@@ -65,6 +83,9 @@ struct MixedWork {
   int *status = nullptr;  // the owner's device status word
   cudaGraphExec_t g_init = nullptr, g_round = nullptr;
   int launches_init = 0, launches_round = 0;
+  // setup() counts its runs here; a captured graph (this workspace's own,
+  // or a batch's) is valid while the count it was captured at still holds
+  unsigned epoch = 0, graph_epoch = 0;
   std::vector<double> hscal;
   MxParams prm{};
   ~MixedWork() {
@@ -88,6 +109,54 @@ struct MxGroup {
 int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
                 double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild, double tol_rel,
                 int max_refine, int n_inner, bool graphs, cudaStream_t st, sx_solve_stats *stats);
+
+// One member of a multi-mesh mixed-precision solve: a mesh, its workspace
+// and plane groups, and the caller's arrays.  `stats` is filled on return.
+struct MxItem {
+  MeshView M;
+  MixedWork *W = nullptr;
+  std::vector<MxGroup> groups;
+  int nz = 0, num_modes = 0;
+  double *u = nullptr, *f = nullptr;
+  const double *bc = nullptr;
+  long long stride = 0;
+  sx_solve_stats stats{};
+};
+
+// Device tables, streams and graphs of a multi-mesh mixed-precision solve.
+// Members are ordered by element order; the members of one order form a
+// class, and every kernel runs once per class over all its members' tiles
+// (element tiles: nel * nch per member; node tiles: G * nch; plane tiles:
+// PP), the classes on their own streams side by side.
+struct MxBatch {
+  struct Class {
+    int np = 0, m0 = 0, count = 0;  // order, first member, members
+    int te = 0, tn = 0, tp = 0;     // element, node and plane tiles
+    size_t t0 = 0;                  // offset of the 3 (count + 1) tile prefixes
+  };
+  DBuf<MxMember> mem;
+  DBuf<int> tiles;
+  DBuf<double> norms;             // r2 then b2 of each member, PP each
+  std::vector<Class> cls;
+  std::vector<int> order;         // item index of each member
+  std::vector<size_t> noff;       // each member's offset in norms
+  std::vector<unsigned> epochs;   // each member workspace's epoch after setup
+  std::vector<double> hnorms;
+  std::vector<cudaStream_t> streams;  // one per class
+  std::vector<cudaEvent_t> events;    // fork + one join per class
+  cudaGraphExec_t g_init = nullptr, g_round = nullptr;
+  int launches_init = 0, launches_round = 0, n_inner = 0;
+  void reset();
+  ~MxBatch();
+};
+
+// Solve every item's plane groups in one batch: each refinement round is
+// one graph whose kernels cover the tiles of all members (one launch per
+// kernel and element order).  Rounds continue until every plane of every
+// member meets tol_rel, or max_refine.  Returns SX_WARN_STEP_LIMIT when a
+// member did not converge.
+int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, double tol_rel, int max_refine,
+                      int n_inner, bool graphs, cudaStream_t st);
 
 // Enqueue `reps` inner-iteration launches (k_cg, iteration 1) on the
 // workspace of the last mixed solve, for timing the kernel on its own.  The

@@ -75,6 +75,21 @@ struct sx_modal_s {
   ~sx_modal_s();
 };
 
+// A multi-mesh batch (sx_batch_solve): the mixed-precision tables and
+// graphs, and the direct solve whose band sweeps cover every member.
+struct sx_batch_s {
+  sx::MxBatch mixed;
+  std::vector<long long> mkey;  // members and buffers the mixed tables were built for
+  sx::DBuf<sx::Job> djobs;      // every member's direct jobs, member by member
+  std::vector<sx::Job> jobs;
+  std::vector<long long> dkey;  // members and buffers the direct graph was captured for
+  cudaGraphExec_t dexec = nullptr;
+  int dlaunches = 0, C = 1;
+  cudaStream_t own = nullptr, aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  ~sx_batch_s();
+};
+
 namespace sx {
 
 // Supplies the system for (lambda2, betak2, kind) of a mode: builds it, or

@@ -230,8 +230,8 @@ int prepare_direct_kernels(const MeshView &M) {
   return prepare_band_kernels();
 }
 
-int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st, int C, int *launches) {
+int direct_rhs_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs, cudaStream_t st,
+                    int *launches) {
   const int nj = (int)hjobs.size();
   int maxpad = 0;
   bool any_bc = false;
@@ -243,10 +243,25 @@ int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job
   if (any_bc) k_essential<<<dim3(1, nj), 32, 0, st>>>(M, djobs);
   dispatch_elem(M, djobs, nj, true, st);
   k_rhs_dss<<<dim3((maxpad + 255) / 256, nj), 256, 0, st>>>(M, djobs);
-  SX_TRY(band_sweep_jobs(djobs, hjobs, C, st));
+  SX_CUDA(cudaGetLastError());
+  if (launches) *launches += (any_bc ? 1 : 0) + 2;
+  return SX_OK;
+}
+
+int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_t st, int *launches) {
   dispatch_elem(M, djobs, nj, false, st);
   SX_CUDA(cudaGetLastError());
-  if (launches) *launches = (any_bc ? 1 : 0) + 4;
+  if (launches) *launches += 1;
+  return SX_OK;
+}
+
+int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
+                      cudaStream_t st, int C, int *launches) {
+  int nl = 0;
+  SX_TRY(direct_rhs_jobs(M, djobs, hjobs, st, &nl));
+  SX_TRY(band_sweep_jobs(djobs, hjobs, C, st));
+  SX_TRY(direct_backsub_jobs(M, djobs, (int)hjobs.size(), st, &nl));
+  if (launches) *launches = nl + 1;
   return SX_OK;
 }
 

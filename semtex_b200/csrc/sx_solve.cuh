@@ -72,6 +72,13 @@ __device__ __forceinline__ void helm_op(const T *D, const T *Q1, const T *Q2, co
 // Returns the number of kernels launched through *launches when non-null.
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
                       cudaStream_t st, int C, int *launches = nullptr);
+// The phases of direct_solve_jobs, for batches whose band sweeps run in one
+// launch across meshes: essential values, condensed RHS (element kernels
+// and direct-stiffness sum); then, after the sweeps, the interior
+// back-substitution.  Each adds its launches to *launches when non-null.
+int direct_rhs_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs, cudaStream_t st,
+                    int *launches);
+int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_t st, int *launches);
 int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st);
 int prepare_band_kernels();
 int pick_cluster(int nj, int cmax, int pmax, int Wmax);
