@@ -267,12 +267,15 @@ SX_API int sx_batch_destroy(sx_batch batch);
 /* ---- serving loop (no reference counterpart) -----------------------------
  * A request loop for Helmholtz solves of different meshes, orders and mode
  * counts.  Requests are admitted in arrival order as device slots and memory
- * free up (bounded by hbm_budget); admitted requests run concurrently, each
- * on its own stream.  Element geometry and per-mode systems (Jacobi
- * diagonals, or factored condensed matrices for SX_FP64) stay resident
- * across requests, keyed by (mesh, lambda2, betak2), with least-recently-
- * used eviction.  A request's result does not depend on what else is in
- * flight. */
+ * free up (bounded by hbm_budget).  Each slot takes every admissible pending
+ * request (up to max_batch) and solves them together as one multi-mesh
+ * batch (sx_batch_solve) on its own stream; the slots' batches run
+ * concurrently, and requests that arrive meanwhile join the next batch.
+ * Element geometry and per-mode systems (Jacobi diagonals, or factored
+ * condensed matrices) stay resident across requests, keyed by (mesh,
+ * lambda2, betak2, kind), with least-recently-used eviction.  A request's
+ * result is the same alone or in a mix within the solve tolerance (the
+ * FP64 form: to rounding). */
 typedef struct sx_server_s *sx_server;
 
 typedef struct {
@@ -282,6 +285,7 @@ typedef struct {
   double tol_rel;                /* mixed: FP64 relative residual target; 0 = 1e-12            */
   int max_refine;                /* mixed: refinement rounds cap; 0 = 30                        */
   int inner_iters;               /* mixed: FP32 PCG iterations per round; 0 = 12                */
+  int max_batch;                 /* requests solved together by one slot; 0 = 8                 */
 } sx_server_config;
 
 typedef struct {
@@ -300,6 +304,10 @@ typedef struct {
   unsigned long long mesh_hits, mesh_misses, system_hits, system_misses, evictions;
   unsigned long long bytes_cached, bytes_budget;
   double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency of completed requests     */
+  unsigned long long batches;     /* batches served                                          */
+  double queue_ms, build_ms, solve_ms; /* summed over requests: waiting for admission; geometry,
+                                          system builds and factorisation; the batch solve with
+                                          its host <-> device copies                            */
 } sx_server_stats;
 
 SX_API int sx_server_create(const sx_server_config *cfg, sx_server *out);

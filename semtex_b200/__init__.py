@@ -71,7 +71,8 @@ class TuneResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_ulonglong), ("slots", C.c_int), ("precision", C.c_int),
-                ("tol_rel", C.c_double), ("max_refine", C.c_int), ("inner_iters", C.c_int)]
+                ("tol_rel", C.c_double), ("max_refine", C.c_int), ("inner_iters", C.c_int),
+                ("max_batch", C.c_int)]
 
 
 class Request(C.Structure):
@@ -86,7 +87,9 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("submitted", "completed", "failed", "rejected", "mesh_hits", "mesh_misses",
                  "system_hits", "system_misses", "evictions", "bytes_cached", "bytes_budget")] + \
-               [("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double)]
+               [("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("batches", C.c_ulonglong), ("queue_ms", C.c_double), ("build_ms", C.c_double),
+                ("solve_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -380,13 +383,14 @@ class Batch:
 
 class Server:
     """Continuous-batching request loop (sx_server_*): requests of any mesh,
-    order and mode count are admitted as device slots and memory free up,
-    run concurrently, and keep geometry and systems resident across requests.
+    order and mode count are admitted as device slots and memory free up;
+    each slot solves up to max_batch of them together as one multi-mesh
+    batch; geometry and systems stay resident across requests.
     """
 
     def __init__(self, slots=4, precision=MIXED_FP32, hbm_budget=0, tol_rel=1e-12,
-                 max_refine=30, inner_iters=12):
-        cfg = ServerConfig(int(hbm_budget), slots, precision, tol_rel, max_refine, inner_iters)
+                 max_refine=30, inner_iters=12, max_batch=8):
+        cfg = ServerConfig(int(hbm_budget), slots, precision, tol_rel, max_refine, inner_iters, max_batch)
         h = C.c_void_p()
         _check(lib.sx_server_create(C.byref(cfg), C.byref(h)), "sx_server_create")
         self.h = h

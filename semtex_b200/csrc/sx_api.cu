@@ -918,7 +918,7 @@ extern "C" int sx_batch_solve(sx_batch b, int count, const sx_modal *modals, dou
     any_direct |= !q.gd.empty();
     any_mixed |= !q.mg.empty();
   }
-  const bool graphs = true;
+  const bool graphs = b->use_graphs;
   cudaStream_t sd = st;  // stream of the band part
   if (any_direct && any_mixed) {
     if (!b->aux) SX_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));

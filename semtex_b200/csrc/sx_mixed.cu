@@ -569,6 +569,11 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   const int nch = B.nch, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = y * MX_CH + lane, PP = P.PP;
   const bool init = mode == CG_INIT, last = mode == CG_LAST;
+  // a chunk whose planes have all stopped leaves r, d (and so x) as they
+  // are: its blocks skip the iteration (block-uniform, before any barrier);
+  // the last one still folds d into x, with alpha = beta = 0
+  const bool stopped = !init && V.skip[y] != 0;
+  if (stopped && !last) return;
   const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
   const bool warm = !init && it > 0;  // s, p, d hold previous iterates
   const size_t base = eidx<NN>(e, nch, y, 0, 0), pbase = ((size_t)e * nch + y) * NN * 16;
@@ -602,7 +607,7 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   double *beta_out = nxt ? V.beta[1] : V.beta[0];
   const int ns = P.nsolve[p];
   float alpha = 0.0f, beta = 0.0f;
-  if (!init) {
+  if (!init && !stopped) {
     alpha = (float)alpha_in[p];
     beta = (float)beta_in[p];
   }
@@ -782,6 +787,8 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
     gam_out[p] = gn;
     alpha_out[p] = an;
     beta_out[p] = bn;
+    const unsigned live = __ballot_sync(0xffffffffu, real_plane(P, p) && (an != 0.0 || bn != 0.0));
+    if (lane == 0) V.skip[y] = live == 0u;
   }
   if (threadIdx.x == 0) bulk_wait_all();  // the stores read shared memory
 }
@@ -1000,6 +1007,7 @@ static CgVecs cg_vecs(MixedWork &W) {
   v.r0 = W.r0.p;
   v.x64 = W.x64.p;
   v.status = W.status;
+  v.skip = W.skip.p;
   for (int k = 0; k < 2; k++) {
     v.gam[k] = s.gam[k];
     v.alpha[k] = s.alpha[k];
@@ -1064,6 +1072,8 @@ int mixed_profile_iterations(const MeshView &M, MixedWork &W, int reps, cudaStre
   // iteration 1 reads what iteration 0 of the last round wrote
   if (W.PP == 0 || W.n_inner < 2 || reps <= 0) return SX_ERR_ARG;
   const MxMember B = member_of(M, W);
+  // every chunk works in the timed launches
+  SX_CUDA(cudaMemsetAsync(W.skip.p, 0, sizeof(int) * B.nch, st));
   for (int r = 0; r < reps; r++)
     SX_NP_SWITCH_M(M.np, (k_cg<N_><<<dim3(M.nel, B.nch), N_ * 32, cg_smem(N_), st>>>(B, 1, CG_ITER)));
   SX_CUDA(cudaGetLastError());
@@ -1138,6 +1148,7 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
     SX_TRY(need(W.gess, (size_t)PP * M.nglobal));
     SX_TRY(need(W.nsolve, (size_t)PP));
     SX_TRY(need(W.active, (size_t)PP));
+    SX_TRY(need(W.skip, (size_t)PP / MX_CH));
     SX_TRY(need(W.pcf, (size_t)npts * Mc));
     // reduction tree: block and group partials, chunk and group counters
     const int gmax = std::max(W.G, M.nel);
@@ -1168,6 +1179,7 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
   SX_CUDA(cudaMemcpyAsync(W.hcon.p, hc.data(), sizeof(double) * PP, cudaMemcpyHostToDevice, st));
   SX_CUDA(cudaMemcpyAsync(W.nsolve.p, ns.data(), sizeof(int) * PP, cudaMemcpyHostToDevice, st));
   SX_CUDA(cudaMemcpyAsync(W.active.p, act.data(), sizeof(int) * PP, cudaMemcpyHostToDevice, st));
+  SX_CUDA(cudaMemsetAsync(W.skip.p, 0, sizeof(int) * (PP / MX_CH), st));
   DBuf<const float *> dp;
   SX_TRY(dp.upload_on(pcs.data(), pcs.size(), st));
   k_x_pc<<<(npts + 255) / 256, 256, 0, st>>>(npts, Mc, dp.p, W.pcf.p);

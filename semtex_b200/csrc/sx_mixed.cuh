@@ -56,6 +56,10 @@ struct CgVecs {
   double *gam[2], *alpha[2], *beta[2];
   double *gam0;       // gamma at the start of the round
   int *status;        // device status bits (1 << SX_ERR_*)
+  // per plane chunk: 1 when every plane of the chunk has stopped for the
+  // rest of the round (alpha = beta = 0), so the chunk's blocks skip the
+  // following iterations; written by each launch's reduction for the next
+  int *skip;
 };
 
 // Everything the kernels of one solve read and write: the mesh, the
@@ -77,7 +81,7 @@ struct MxMember {
 struct MixedWork {
   int PP = 0, npts = 0, n_inner = 0, M = 0, G = 0;
   DBuf<double> hcon, b64, x64, Ye64, scal, part, gess;
-  DBuf<int> nsolve, active;
+  DBuf<int> nsolve, active, skip;
   DBuf<unsigned> cnt;
   DBuf<float> pcf, r0, rE, sE, pE, dE, WE0, WE1, pcE;
   int *status = nullptr;  // the owner's device status word

@@ -85,6 +85,8 @@ struct sx_batch_s {
   std::vector<long long> dkey;  // members and buffers the direct graph was captured for
   cudaGraphExec_t dexec = nullptr;
   int dlaunches = 0, C = 1;
+  bool use_graphs = true;       // capture and replay (the serving loop, whose member set
+                                // changes from batch to batch, enqueues directly)
   cudaStream_t own = nullptr, aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~sx_batch_s();

@@ -2,17 +2,23 @@
 //
 // Requests (a mesh, per-mode Helmholtz constants, forcing planes) are queued
 // by sx_server_submit and served by `slots` worker threads, each owning a
-// non-blocking CUDA stream and a reusable solve workspace, so admitted
-// requests run concurrently on the device.  Admission is first come, first
-// served and bounded by a device-memory budget: a request is admitted when
-// the cached objects plus the reservations of the requests in flight plus its
-// own estimate fit; least-recently-used cache entries no request is using are
-// evicted to make room.  Element geometry (per mesh) and per-mode systems
-// (Jacobi diagonals, or factored condensed matrices for SX_FP64) stay
-// resident across requests, keyed by (mesh contents, lambda2, betak2, kind),
-// as the reference's MatrixSys cache keys them (src/matrix.cpp:85-102,
-// 326-347).  Each request's solve uses only its own workspace and stream, so
-// its result is the same alone or in a mix.
+// non-blocking CUDA stream, a multi-mesh batch object and a pool of
+// per-request workspaces.  A free worker takes every admissible pending
+// request, in arrival order and up to max_batch, builds what the cache does
+// not hold (element geometry, per-mode systems, one batched factorisation
+// for the batch's new band factors) and solves the requests together with
+// sx_batch_solve: one launch per kernel and element order covers all of
+// them.  Requests that arrive while batches are on the device join the next
+// one.  Admission is bounded by a device-memory budget: a request is
+// admitted when the cached objects plus the reservations of the requests in
+// flight plus its own estimate fit; least-recently-used cache entries no
+// request is using are evicted to make room.  Element geometry (per mesh)
+// and per-mode systems (Jacobi diagonals, or factored condensed matrices)
+// stay resident across requests, keyed by (mesh contents, lambda2, betak2,
+// kind), as the reference's MatrixSys cache keys them (src/matrix.cpp:85-102,
+// 326-347).  A request's result is the same alone or in a batch within the
+// solve tolerance: the batch shares the iteration count per refinement round
+// and the number of rounds, each plane's arithmetic is its own.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -156,7 +162,24 @@ struct sx_server_s {
   bool admissible(Req *r, size_t &need);
   void evict_for(size_t need, uint64_t keep_mesh);
   void worker(int slot);
-  int serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &df, DBuf<double> &dbc, cudaStream_t stream);
+  // One request's mesh and systems, looked up or built (caller holds
+  // build_mu); new band factors are appended to to_factor.
+  struct Prep {
+    sx_mesh_s *mesh = nullptr;
+    std::vector<std::shared_ptr<System>> sys;
+    std::vector<std::tuple<uint64_t, uint64_t, uint64_t, int>> keys;
+    bool mesh_ref = false;
+  };
+  int prepare(Req *r, Prep &p, std::vector<System *> &to_factor, cudaStream_t stream);
+  void release(const Req *r, const Prep &p);
+  // A worker's workspace for one batch member.
+  struct Member {
+    std::unique_ptr<sx_modal_s> ws;
+    DBuf<double> du, df, dbc;
+    size_t bytes = 0;  // estimate of what the last request left allocated
+  };
+  void serve_batch(std::vector<Req *> &batch, std::vector<std::unique_ptr<Member>> &pool, sx_batch b,
+                   cudaStream_t stream);
 };
 
 // Memory this request still needs beyond what is cached (caller holds mu).
@@ -203,114 +226,201 @@ void sx_server_s::evict_for(size_t need, uint64_t keep_mesh) {
   }
 }
 
-int sx_server_s::serve(Req *r, sx_modal_s &ws, DBuf<double> &du, DBuf<double> &df, DBuf<double> &dbc,
-                       cudaStream_t stream) {
-  sx_mesh_s *mesh = nullptr;
-  std::vector<std::shared_ptr<System>> sys(r->num_modes);
-  std::vector<std::tuple<uint64_t, uint64_t, uint64_t, int>> keys(r->num_modes);
-  {
-    // look up or build the mesh and the systems (one builder at a time)
-    std::lock_guard<std::mutex> bl(build_mu);
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      auto it = meshes.find(r->mesh.key);
-      if (it != meshes.end()) {
-        mesh = it->second.mesh.get();
-        it->second.refs++;
-        it->second.last_use = ++tick;
-        st.mesh_hits++;
-      }
-    }
-    if (!mesh) {
-      const sx_mesh_desc d = r->mesh.desc();
-      sx_mesh m = nullptr;
-      SX_TRY(sx_mesh_create(&d, &m));
-      std::lock_guard<std::mutex> lk(mu);
-      MeshEntry &e = meshes[r->mesh.key];
-      e.mesh.reset(m);
-      e.bytes = mesh_estimate(r->mesh);
-      e.refs = 1;
-      e.last_use = ++tick;
-      bytes_cached += e.bytes;
-      mesh = m;
-      st.mesh_misses++;
-    }
-    std::vector<System *> to_factor;
-    for (int l = 0; l < r->num_modes; l++) {
-      const int kind = r->kinds[l];
-      uint64_t a, b;
-      std::memcpy(&a, &r->lam[l], 8);
-      std::memcpy(&b, &r->bk2[l], 8);
-      keys[l] = std::make_tuple(r->mesh.key, a, b, kind);
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        auto it = systems.find(keys[l]);
-        if (it != systems.end()) {
-          sys[l] = it->second.sys;
-          it->second.refs++;
-          it->second.last_use = ++tick;
-          st.system_hits++;
-          continue;
-        }
-      }
-      auto S = std::make_shared<System>();
-      S->mesh = mesh;
-      S->lambda2 = r->lam[l];
-      S->betak2 = r->bk2[l];
-      S->method = kind;
-      if (kind == SX_DIRECT) {
-        SX_TRY(system_build_direct(*S, stream));
-        if (S->nsolve > 0) to_factor.push_back(S.get());
-        SX_TRY(system_build_jacobi_diag(*S, stream));
-      } else {
-        SX_TRY(system_build_jacobi(*S, stream));
-      }
-      sys[l] = S;
-      std::lock_guard<std::mutex> lk(mu);
-      SysEntry &e = systems[keys[l]];
-      e.sys = S;
-      e.mesh_key = r->mesh.key;
-      e.bytes = system_estimate(r->mesh, kind);
-      e.refs = 1;
-      e.last_use = ++tick;
-      bytes_cached += e.bytes;
-      st.system_misses++;
-    }
-    SX_TRY(factor_batch(to_factor, stream));
-  }
-  ws.rebind(mesh, r->base_mode, r->num_modes, cfg.precision == SX_FP64 ? SX_DIRECT : SX_MIXED, sys);
-  ws.n_inner = cfg.inner_iters;
-  const size_t n = (size_t)r->nz * r->stride;
-  if (du.n < n) SX_TRY(du.alloc(n));
-  if (df.n < n) SX_TRY(df.alloc(n));
-  if (!r->bc.empty() && dbc.n < r->bc.size()) SX_TRY(dbc.alloc(r->bc.size()));
-  SX_CUDA(cudaMemcpyAsync(df.p, r->f.data(), n * 8, cudaMemcpyHostToDevice, stream));
-  if (!r->bc.empty()) SX_CUDA(cudaMemcpyAsync(dbc.p, r->bc.data(), r->bc.size() * 8, cudaMemcpyHostToDevice, stream));
-  if (!ws.dstatus.p) {
-    SX_TRY(ws.dstatus.alloc(1));
-    SX_TRY(ws.dstatus.zero(stream));
-  }
-  sx_solve_stats sst{};
-  int rc = solve_batched_on(&ws, du.p, df.p, r->bc.empty() ? nullptr : dbc.p, r->nz, r->stride,
-                            cfg.precision, cfg.tol_rel, cfg.max_refine, stream, &sst);
-  if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
-    int c = copy_solved_planes(r->u, du.p, r->nz, r->stride, r->base_mode, stream);
-    if (c == SX_OK && cudaStreamSynchronize(stream) != cudaSuccess) {
-      set_error("serving: device -> host copy of a result failed");
-      c = SX_ERR_CUDA;
-    }
-    if (c != SX_OK) rc = c;
-  }
+int sx_server_s::prepare(Req *r, Prep &pp, std::vector<System *> &to_factor, cudaStream_t stream) {
   {
     std::lock_guard<std::mutex> lk(mu);
-    auto mi = meshes.find(r->mesh.key);
-    if (mi != meshes.end()) mi->second.refs--;
-    for (auto &k : keys) {
-      auto si = systems.find(k);
-      if (si != systems.end()) si->second.refs--;
+    auto it = meshes.find(r->mesh.key);
+    if (it != meshes.end()) {
+      pp.mesh = it->second.mesh.get();
+      it->second.refs++;
+      it->second.last_use = ++tick;
+      pp.mesh_ref = true;
+      st.mesh_hits++;
     }
   }
-  return rc;
+  if (!pp.mesh) {
+    const sx_mesh_desc d = r->mesh.desc();
+    sx_mesh m = nullptr;
+    SX_TRY(sx_mesh_create(&d, &m));
+    std::lock_guard<std::mutex> lk(mu);
+    MeshEntry &e = meshes[r->mesh.key];
+    e.mesh.reset(m);
+    e.bytes = mesh_estimate(r->mesh);
+    e.refs = 1;
+    e.last_use = ++tick;
+    bytes_cached += e.bytes;
+    pp.mesh = m;
+    pp.mesh_ref = true;
+    st.mesh_misses++;
+  }
+  pp.sys.resize(r->num_modes);
+  for (int l = 0; l < r->num_modes; l++) {
+    const int kind = r->kinds[l];
+    uint64_t a, b;
+    std::memcpy(&a, &r->lam[l], 8);
+    std::memcpy(&b, &r->bk2[l], 8);
+    const auto key = std::make_tuple(r->mesh.key, a, b, kind);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = systems.find(key);
+      if (it != systems.end()) {
+        pp.sys[l] = it->second.sys;
+        it->second.refs++;
+        it->second.last_use = ++tick;
+        pp.keys.push_back(key);
+        st.system_hits++;
+        continue;
+      }
+    }
+    auto S = std::make_shared<System>();
+    S->mesh = pp.mesh;
+    S->lambda2 = r->lam[l];
+    S->betak2 = r->bk2[l];
+    S->method = kind;
+    if (kind == SX_DIRECT) {
+      SX_TRY(system_build_direct(*S, stream));
+      if (S->nsolve > 0) to_factor.push_back(S.get());
+      SX_TRY(system_build_jacobi_diag(*S, stream));
+    } else {
+      SX_TRY(system_build_jacobi(*S, stream));
+    }
+    pp.sys[l] = S;
+    std::lock_guard<std::mutex> lk(mu);
+    SysEntry &e = systems[key];
+    e.sys = S;
+    e.mesh_key = r->mesh.key;
+    e.bytes = system_estimate(r->mesh, kind);
+    e.refs = 1;
+    e.last_use = ++tick;
+    bytes_cached += e.bytes;
+    pp.keys.push_back(key);
+    st.system_misses++;
+  }
+  return SX_OK;
+}
+
+void sx_server_s::release(const Req *r, const Prep &pp) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (pp.mesh_ref) {
+    auto mi = meshes.find(r->mesh.key);
+    if (mi != meshes.end()) mi->second.refs--;
+  }
+  for (auto &k : pp.keys) {
+    auto si = systems.find(k);
+    if (si != systems.end()) si->second.refs--;
+  }
+}
+
+// Workspaces above this size are freed after their batch instead of kept
+// for the next one (a pool slot otherwise holds the largest request it saw).
+constexpr size_t KEEP_WS_BYTES = size_t(256) << 20;
+
+void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique_ptr<Member>> &pool, sx_batch b,
+                              cudaStream_t stream) {
+  const int n = (int)batch.size();
+  const auto t0 = Clock::now();
+  std::vector<Prep> prep(n);
+  std::vector<int> rc(n, SX_OK);
+  {
+    // look up or build the meshes and systems (one builder at a time), then
+    // factor the batch's new band systems together
+    std::lock_guard<std::mutex> bl(build_mu);
+    std::vector<System *> to_factor;
+    for (int i = 0; i < n; i++) rc[i] = prepare(batch[i], prep[i], to_factor, stream);
+    const int fr = factor_batch(to_factor, stream);
+    if (fr != SX_OK)
+      for (int i = 0; i < n; i++) rc[i] = rc[i] == SX_OK ? fr : rc[i];
+  }
+  const auto t1 = Clock::now();
+  while ((int)pool.size() < n) pool.emplace_back(new Member());
+  std::vector<sx_modal> mods;
+  std::vector<double *> du, df;
+  std::vector<const double *> dbc;
+  std::vector<int> nz, stride, idx;
+  bool any_bc = false;
+  for (int i = 0; i < n; i++) {
+    if (rc[i] != SX_OK) continue;
+    Req *r = batch[i];
+    Member &m = *pool[i];
+    if (!m.ws) {
+      m.ws.reset(new sx_modal_s());
+      m.ws->own = stream;
+      m.ws->own_stream_external = true;
+      m.ws->use_graphs = false;
+    }
+    sx_modal_s &ws = *m.ws;
+    ws.rebind(prep[i].mesh, r->base_mode, r->num_modes, cfg.precision == SX_FP64 ? SX_DIRECT : SX_MIXED,
+              prep[i].sys);
+    ws.n_inner = cfg.inner_iters;
+    const size_t len = (size_t)r->nz * r->stride;
+    int e = SX_OK;
+    if (m.du.n < len) e = m.du.alloc(len);
+    if (e == SX_OK && m.df.n < len) e = m.df.alloc(len);
+    if (e == SX_OK && !r->bc.empty() && m.dbc.n < r->bc.size()) e = m.dbc.alloc(r->bc.size());
+    if (e == SX_OK && cudaMemcpyAsync(m.df.p, r->f.data(), len * 8, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      e = SX_ERR_CUDA;
+    if (e == SX_OK && !r->bc.empty() &&
+        cudaMemcpyAsync(m.dbc.p, r->bc.data(), r->bc.size() * 8, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      e = SX_ERR_CUDA;
+    if (e != SX_OK) {
+      rc[i] = e;
+      continue;
+    }
+    m.bytes = work_estimate(r->mesh, r->nz, cfg.precision);
+    mods.push_back(&ws);
+    du.push_back(m.du.p);
+    df.push_back(m.df.p);
+    dbc.push_back(r->bc.empty() ? nullptr : m.dbc.p);
+    any_bc |= !r->bc.empty();
+    nz.push_back(r->nz);
+    stride.push_back(r->stride);
+    idx.push_back(i);
+  }
+  if (!mods.empty()) {
+    std::vector<sx_solve_stats> sst(mods.size());
+    int br = sx_batch_solve(b, (int)mods.size(), mods.data(), du.data(), df.data(), any_bc ? dbc.data() : nullptr,
+                            nz.data(), stride.data(), cfg.precision, cfg.tol_rel, cfg.max_refine, stream,
+                            sst.data());
+    for (size_t k = 0; k < idx.size(); k++) {
+      const int i = idx[k];
+      Req *r = batch[i];
+      int c = br;
+      if (br == SX_OK || br == SX_WARN_STEP_LIMIT) {
+        c = copy_solved_planes(r->u, du[k], r->nz, r->stride, r->base_mode, stream);
+        if (c == SX_OK)
+          c = (cfg.precision == SX_MIXED_FP32 && !(sst[k].final_rel_residual <= cfg.tol_rel)) ? SX_WARN_STEP_LIMIT
+                                                                                             : SX_OK;
+      }
+      rc[i] = c;
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+      set_error("serving: batch solve or device -> host copy failed");
+      for (int i : idx) rc[i] = SX_ERR_CUDA;
+    }
+    // the batch's device-side status words (bounded waits that ran out)
+    for (size_t k = 0; k < idx.size(); k++) {
+      int h = 0;
+      sx_modal_s &ws = *pool[idx[k]]->ws;
+      if (ws.dstatus.p && cudaMemcpy(&h, ws.dstatus.p, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && h) {
+        cudaMemset(ws.dstatus.p, 0, sizeof(int));
+        rc[idx[k]] = SX_ERR_TIMEOUT;
+      }
+    }
+  }
+  const auto t2 = Clock::now();
+  for (int i = 0; i < n; i++) {
+    release(batch[i], prep[i]);
+    batch[i]->status = rc[i];
+  }
+  // keep small workspaces for the next batch, free the large ones
+  for (int i = 0; i < n; i++)
+    if (pool[i]->bytes > KEEP_WS_BYTES) pool[i].reset(new Member());
+  std::lock_guard<std::mutex> lk(mu);
+  st.batches++;
+  const double bms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  const double sms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  st.build_ms += bms * n;
+  st.solve_ms += sms * n;
 }
 
 void sx_server_s::worker(int slot) {
@@ -318,56 +428,59 @@ void sx_server_s::worker(int slot) {
   cudaSetDevice(device);
   cudaStream_t stream = nullptr;
   cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-  sx_modal_s ws;
-  ws.own = stream;
-  ws.own_stream_external = true;
-  ws.use_graphs = false;
-  DBuf<double> du, df, dbc;
+  sx_batch b = nullptr;
+  sx_batch_create(&b);
+  b->use_graphs = false;
+  std::vector<std::unique_ptr<Member>> pool;
   for (;;) {
-    Req *r = nullptr;
+    std::vector<Req *> batch;
     {
       std::unique_lock<std::mutex> lk(mu);
       for (;;) {
         if (stopping && pending.empty()) break;
-        if (!pending.empty()) {
+        // every admissible pending request, in arrival order, up to max_batch
+        while (!pending.empty() && (int)batch.size() < cfg.max_batch) {
           Req *h = pending.front();
           size_t need = 0;
           if (!admissible(h, need)) evict_for(need, h->mesh.key);
-          if (admissible(h, need) || inflight == 0) {
-            pending.pop_front();
-            h->reserve = work_estimate(h->mesh, h->nz, cfg.precision);
-            bytes_reserved += h->reserve;
-            inflight++;
-            r = h;
-            break;
-          }
+          if (!(admissible(h, need) || (inflight == 0 && batch.empty()))) break;
+          pending.pop_front();
+          h->reserve = work_estimate(h->mesh, h->nz, cfg.precision);
+          bytes_reserved += h->reserve;
+          inflight++;
+          st.queue_ms += std::chrono::duration<double, std::milli>(Clock::now() - h->t_submit).count();
+          batch.push_back(h);
         }
+        if (!batch.empty()) break;
         cv_work.wait(lk);
       }
     }
-    if (!r) break;
-    const int rc = serve(r, ws, du, df, dbc, stream);
+    if (batch.empty()) break;
+    serve_batch(batch, pool, b, stream);
     {
       std::lock_guard<std::mutex> lk(mu);
-      r->status = rc;
-      r->latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - r->t_submit).count();
-      r->done = true;
-      bytes_reserved -= r->reserve;
-      inflight--;
-      if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
-        st.completed++;
-        latencies.push_back(r->latency_ms);
-      } else {
-        st.failed++;
+      for (Req *r : batch) {
+        r->latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - r->t_submit).count();
+        r->done = true;
+        bytes_reserved -= r->reserve;
+        inflight--;
+        if (r->status == SX_OK || r->status == SX_WARN_STEP_LIMIT) {
+          st.completed++;
+          latencies.push_back(r->latency_ms);
+        } else {
+          st.failed++;
+        }
+        // drop the big copies now; the record stays for sx_server_wait
+        r->f.clear();
+        r->f.shrink_to_fit();
+        r->bc.clear();
       }
-      // drop the big copies now; the record stays for sx_server_wait
-      r->f.clear();
-      r->f.shrink_to_fit();
-      r->bc.clear();
     }
     cv_done.notify_all();
     cv_work.notify_all();
   }
+  pool.clear();
+  sx_batch_destroy(b);
   cudaStreamDestroy(stream);
 }
 
@@ -383,6 +496,8 @@ extern "C" int sx_server_create(const sx_server_config *cfg, sx_server *out) {
   if (c.tol_rel <= 0.0) c.tol_rel = 1e-12;
   if (c.max_refine <= 0) c.max_refine = 30;
   if (c.inner_iters <= 0) c.inner_iters = 12;
+  if (c.max_batch <= 0) c.max_batch = 8;
+  if (c.max_batch > 256) return SX_ERR_ARG;
   SX_CUDA(cudaGetDevice(&S->device));
   if (c.hbm_budget == 0) {
     size_t fr = 0, tot = 0;

@@ -1,8 +1,10 @@
 """GPU tests of the serving loop (sx_server_*).
 
 * Requests of different meshes, orders and mode counts, submitted together
-  and run concurrently, give bitwise the same results as each solved alone
-  through ModalMatrixSys.solve_batched_host (same kernels, same schedule).
+  and solved in multi-mesh batches, give the same results as each served
+  alone (a one-slot server, batch of one) within the 1e-10 bar: a batch
+  shares the FP32 iteration count per round and the number of refinement
+  rounds, each plane's arithmetic is its own.
 * Results match the oracle's FP64 direct solve within 1e-10.
 * Geometry and systems are reused across requests (cache hits).
 * A request larger than the memory budget is refused with SX_ERR_CAPACITY.
@@ -55,22 +57,44 @@ def _alone(sx, m, lam, bk2, f):
     return u
 
 
-def test_mix_equals_alone_and_oracle(sx):
+def _solved(nz):
+    return [0] + list(range(2, nz)) if nz > 1 else [0]
+
+
+def _blocker():
+    """A larger request that keeps a one-slot server busy while the test's
+    requests queue behind it (so that they are served as one batch)."""
+    from semtex_b200.mesh import rect_mesh
+    from semtex_b200.workloads import fourier_forcing
+    m = rect_mesh(24, 24, 9, 0.0, 1.0, 0.0, 1.0)
+    nm = 16
+    return (m, np.full(nm, 3e3), np.arange(nm, dtype=np.float64) ** 2,
+            fourier_forcing(m, 2 * nm, np.random.default_rng(3)))
+
+
+@pytest.mark.parametrize("slots", [1, 3])
+def test_mix_equals_alone_and_oracle(sx, slots):
     reqs = _requests()
     alone = [_alone(sx, *r) for r in reqs]
-    srv = sx.Server(slots=3, **_cfg(sx))
+    srv = sx.Server(slots=slots, **_cfg(sx))
     try:
+        first = srv.submit(*_blocker())
         ids = [srv.submit(*r) for r in reqs]
         res = [srv.wait(i, timeout_s=120.0) for i in ids]
+        srv.wait(first, timeout_s=120.0)
         stats = srv.stats()
     finally:
         srv.close()
-    for (status, lat, u), a in zip(res, alone):
+    for (status, lat, u), a, r in zip(res, alone, reqs):
         assert status in (sx.OK, sx.WARN_STEP_LIMIT)
         assert lat > 0.0
-        bad = [p for p in range(u.shape[0]) if not np.array_equal(u[p], a[p])]
-        assert not bad, f"planes {bad} differ (max {np.max(np.abs(u - a)):.3e})"
-    assert stats["completed"] == len(reqs)
+        sp = _solved(u.shape[0])
+        err = np.linalg.norm(u[sp] - a[sp]) / np.linalg.norm(a[sp])
+        assert err <= TOL, err
+    assert stats["completed"] == len(reqs) + 1
+    if slots == 1:
+        # the six queued behind the blocker are served together
+        assert stats["batches"] <= 3, stats
     assert stats["mesh_hits"] >= 1          # requests 0 and 4 share a mesh
     assert stats["system_hits"] >= 2        # ... and both of their systems
     assert stats["p99_ms"] >= stats["p50_ms"] > 0.0
