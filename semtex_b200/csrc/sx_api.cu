@@ -282,9 +282,11 @@ static int reserve_ws(sx_modal_s &M, int planes) {
   size_t npad = 1;
   for (auto &s : M.uniq) npad = std::max(npad, (size_t)std::max(s->nblk, 1) * NB);
   M.npad_max = npad;
-  if (M.rhs.n < (size_t)planes * npad) SX_TRY(M.rhs.alloc((size_t)planes * npad));
-  if (M.Fb.n < (size_t)planes * Mh.nel * Mh.next) SX_TRY(M.Fb.alloc((size_t)planes * Mh.nel * Mh.next));
-  if (M.gess.n < (size_t)planes * Mh.nglobal) SX_TRY(M.gess.alloc((size_t)planes * Mh.nglobal));
+  cudaStream_t st = M.own;
+  if (M.rhs.n < (size_t)planes * npad) SX_TRY(M.rhs.alloc_in((size_t)planes * npad, M.pool, st));
+  if (M.Fb.n < (size_t)planes * Mh.nel * Mh.next)
+    SX_TRY(M.Fb.alloc_in((size_t)planes * Mh.nel * Mh.next, M.pool, st));
+  if (M.gess.n < (size_t)planes * Mh.nglobal) SX_TRY(M.gess.alloc_in((size_t)planes * Mh.nglobal, M.pool, st));
   return SX_OK;
 }
 
@@ -524,17 +526,21 @@ static int mixed_solve_batched(sx_modal s, double *d_u, double *d_f, const doubl
     // iterations per round: the knob, raised to what the worst-conditioned
     // mode needs for a 1e-6 cut per round (a restarted CG round that stops
     // short stalls the refinement)
-    int n_inner = std::max(s->n_inner, 1);
-    for (const MxGroup &g : mg)
-      n_inner = std::max(n_inner, std::min(CG_ROUND_CAP, cg_round_iters(s->mesh->kratio,
-                                                                         g.sys->lambda2 + g.sys->betak2)));
+    int n_inner = std::max(s->n_inner, 1), easiest = CG_ROUND_CAP;
+    for (const MxGroup &g : mg) {
+      const int need = std::min(CG_ROUND_CAP, cg_round_iters(s->mesh->kratio, g.sys->lambda2 + g.sys->betak2));
+      n_inner = std::max(n_inner, need);
+      easiest = std::min(easiest, need);
+    }
+    // stop flags pay when the easiest mode needs at most half the round
+    const bool check_stop = 2 * easiest <= n_inner;
     const bool rebuild = !(s->mkey[0] == d_u && s->mkey[1] == d_f && s->mkey[2] == d_bc && s->mnz == nz &&
                            s->mstride == plane_stride && s->mixed.n_inner == n_inner && s->mmodes == jmodes &&
                            s->mixed.status == s->dstatus.p);
     s->mixed.status = s->dstatus.p;
     const MeshView M = s->mesh->view();
     rc = mixed_solve(M, s->mixed, mg, nz, s->num_modes, d_u, d_f, d_bc, plane_stride, rebuild, tol_rel,
-                     max_refine, n_inner, s->use_graphs, st, &loc);
+                     max_refine, n_inner, check_stop, s->use_graphs, st, &loc);
     if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT) {
       s->mkey[0] = d_u;
       s->mkey[1] = d_f;
@@ -935,14 +941,17 @@ extern "C" int sx_batch_solve(sx_batch b, int count, const sx_modal *modals, dou
   std::vector<int> item_of(count, -1);
   if (any_mixed) {
     std::vector<long long> key;
-    int n_inner = 1;
+    int n_inner = 1, easiest = CG_ROUND_CAP;
     for (int i = 0; i < count; i++) {
       Part &q = parts[i];
       if (q.mg.empty()) continue;
       n_inner = std::max(n_inner, std::max(q.s->n_inner, 1));
-      for (const MxGroup &g : q.mg)
-        n_inner = std::max(n_inner, std::min(CG_ROUND_CAP, cg_round_iters(q.s->mesh->kratio,
-                                                                           g.sys->lambda2 + g.sys->betak2)));
+      for (const MxGroup &g : q.mg) {
+        const int need =
+            std::min(CG_ROUND_CAP, cg_round_iters(q.s->mesh->kratio, g.sys->lambda2 + g.sys->betak2));
+        n_inner = std::max(n_inner, need);
+        easiest = std::min(easiest, need);
+      }
       q.s->mixed.status = q.s->dstatus.p;
       MxItem it;
       it.M = q.s->mesh->view();
@@ -968,7 +977,8 @@ extern "C" int sx_batch_solve(sx_batch b, int count, const sx_modal *modals, dou
     }
     key.push_back(n_inner);
     const bool rebuild = key != b->mkey;
-    rc = mixed_solve_multi(items, b->mixed, rebuild, tol_rel, max_refine, n_inner, graphs, st);
+    const bool check_stop = 2 * easiest <= n_inner;
+    rc = mixed_solve_multi(items, b->mixed, rebuild, tol_rel, max_refine, n_inner, check_stop, graphs, st);
     if (rc == SX_OK || rc == SX_WARN_STEP_LIMIT)
       b->mkey = key;
     else

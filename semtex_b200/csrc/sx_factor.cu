@@ -19,6 +19,7 @@
 // JACPCG (src/matrix.cpp:276-317): k_elem_diag + k_diag_dss.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "sx_internal.h"
 #include "sx_kernels.cuh"
@@ -31,10 +32,11 @@ namespace sx {
 
 // smem (doubles): D nn | Q1..Q4 4nn | hbb next^2 | hbi next*nint | hii nint^2 |
 // t next*nint | colk nint ; ints: emap nn
-static size_t condense_smem(const MeshView &M) {
-  const size_t nn = M.npnp, ne = M.next, ni = M.nint;
+static size_t condense_smem_np(int np) {
+  const size_t nn = (size_t)np * np, ne = 4 * (size_t)(np - 1), ni = nn - ne;
   return sizeof(double) * (5 * nn + ne * ne + 2 * ne * ni + ni * ni + ni) + sizeof(int) * nn + 16;
 }
+static size_t condense_smem(const MeshView &M) { return condense_smem_np(M.np); }
 
 __global__ void k_elem_condense(MeshView M, double hCon, double *__restrict__ hbi_out,
                                 double *__restrict__ hii_out, double *__restrict__ hbb_out,
@@ -391,7 +393,9 @@ size_t System::bytes() const {
   return (tiles.n + dinv.n + hbi.n + hii.n + pc.n) * 8 + (hbif.n + hiif.n + pcf.n) * 4;
 }
 
-int factor_batch(std::vector<System *> &systems, cudaStream_t st) {
+int system_check_status(System &S) { return S.status.p ? check_status(S.status) : SX_OK; }
+
+int factor_batch(std::vector<System *> &systems, cudaStream_t st, bool sync) {
   if (systems.empty()) return SX_OK;
   std::vector<SysDesc> hd(systems.size());
   int maxblk = 0, maxJ = 0;
@@ -421,11 +425,11 @@ int factor_batch(std::vector<System *> &systems, cudaStream_t st) {
     }
   }
   SX_CUDA(cudaGetLastError());
-  SX_CUDA(cudaStreamSynchronize(st));
+  if (sync) SX_CUDA(cudaStreamSynchronize(st));
   return SX_OK;
 }
 
-int system_build_direct(System &S, cudaStream_t st) {
+int system_build_direct(System &S, cudaStream_t st, bool sync) {
   sx_mesh_s &Mh = *S.mesh;
   const MeshView M = Mh.view();
   const double hCon = S.betak2 + S.lambda2;
@@ -434,20 +438,29 @@ int system_build_direct(System &S, cudaStream_t st) {
   const int kd = Mh.nband - 1;
   S.nblk = (S.nsolve + NB - 1) / NB;
   S.J = (kd + NB - 1) / NB;
-  if (S.status.p == nullptr) SX_TRY(S.status.alloc(1));
+  if (S.status.p == nullptr) SX_TRY(S.status.alloc_in(1, S.pool, st));
   SX_TRY(S.status.zero(st));
-  SX_TRY(S.hbi.alloc((size_t)Mh.nel * Mh.next * Mh.nint));
-  SX_TRY(S.hii.alloc((size_t)Mh.nel * Mh.nint * Mh.nint));
+  SX_TRY(S.hbi.alloc_in((size_t)Mh.nel * Mh.next * Mh.nint, S.pool, st));
+  SX_TRY(S.hii.alloc_in((size_t)Mh.nel * Mh.nint * Mh.nint, S.pool, st));
   DBuf<double> hbb;
-  SX_TRY(hbb.alloc_on((size_t)Mh.nel * Mh.next * Mh.next, st));
+  SX_TRY(hbb.alloc_in((size_t)Mh.nel * Mh.next * Mh.next, S.pool, st, true));
   const size_t smem = condense_smem(M);
-  SX_CUDA(cudaFuncSetAttribute(k_elem_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the kernel's shared-memory limit is a per-function setting: set it once,
+  // for the largest order, so that builds of different orders on other host
+  // threads never lower it under this launch
+  static std::once_flag attr_once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr_once, []() {
+    attr_err = cudaFuncSetAttribute(k_elem_condense, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)condense_smem_np(NP_MAX));
+  });
+  SX_CUDA(attr_err);
   k_elem_condense<<<Mh.nel, 256, smem, st>>>(M, hCon, S.hbi.p, S.hii.p, hbb.p, S.status.p);
   SX_CUDA(cudaGetLastError());
   const size_t ntiles = (size_t)std::max(S.nblk, 1) * (S.J + 1);
-  SX_TRY(S.tiles.alloc(ntiles * TSZ));
+  SX_TRY(S.tiles.alloc_in(ntiles * TSZ, S.pool, st));
   SX_TRY(S.tiles.zero(st));
-  SX_TRY(S.dinv.alloc((size_t)std::max(S.nblk, 1) * TSZ));
+  SX_TRY(S.dinv.alloc_in((size_t)std::max(S.nblk, 1) * TSZ, S.pool, st));
   SX_TRY(S.dinv.zero(st));
   if (S.nsolve > 0) {
     const int npad = S.nblk * NB - S.nsolve;
@@ -461,33 +474,34 @@ int system_build_direct(System &S, cudaStream_t st) {
     if (Mh.mixed) k_band_mixed<<<1, 1, 0, st>>>(M, S.tiles.p, S.J, S.nsolve);
     SX_CUDA(cudaGetLastError());
   }
+  if (!sync) return SX_OK;
   SX_CUDA(cudaStreamSynchronize(st));
   SX_TRY(check_status(S.status));
   return SX_OK;
 }
 
-int system_build_jacobi(System &S, cudaStream_t st) {
+int system_build_jacobi(System &S, cudaStream_t st, bool sync) {
   sx_mesh_s &Mh = *S.mesh;
   S.singular = (S.lambda2 + S.betak2) < EPSSP && (Mh.nglobal - Mh.nsolve) == 0 && !Mh.mixed;
   S.nsolve = S.singular ? Mh.nsolve - 1 : Mh.nsolve;
-  return system_build_jacobi_diag(S, st);
+  return system_build_jacobi_diag(S, st, sync);
 }
 
 // Inverse Jacobi diagonal only (also used by DIRECT systems for the
 // mixed-precision form).
-int system_build_jacobi_diag(System &S, cudaStream_t st) {
+int system_build_jacobi_diag(System &S, cudaStream_t st, bool sync) {
   sx_mesh_s &Mh = *S.mesh;
   const MeshView M = Mh.view();
   const double hCon = S.betak2 + S.lambda2;
   const int npts = Mh.nglobal + Mh.nel * Mh.nint;
   DBuf<double> ediag;
-  SX_TRY(ediag.alloc_on((size_t)Mh.nel * Mh.npnp, st));
-  SX_TRY(S.pc.alloc(npts));
-  SX_TRY(S.pcf.alloc(npts));
+  SX_TRY(ediag.alloc_in((size_t)Mh.nel * Mh.npnp, S.pool, st, true));
+  SX_TRY(S.pc.alloc_in(npts, S.pool, st));
+  SX_TRY(S.pcf.alloc_in(npts, S.pool, st));
   k_elem_diag<<<Mh.nel, 128, 0, st>>>(M, hCon, ediag.p);
   k_diag_dss<<<(npts + 255) / 256, 256, 0, st>>>(M, ediag.p, S.pc.p, S.pcf.p);
   SX_CUDA(cudaGetLastError());
-  SX_CUDA(cudaStreamSynchronize(st));
+  if (sync) SX_CUDA(cudaStreamSynchronize(st));
   return SX_OK;
 }
 

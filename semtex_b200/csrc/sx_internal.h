@@ -112,6 +112,25 @@ struct DBuf {
     n = count;
     return SX_OK;
   }
+  // From `pool` on stream s (stream-ordered, no device-wide synchronisation);
+  // plain alloc when pool is null.  Freed on s when free_on_s (a temporary
+  // whose last use is on s), else on the legacy stream (valid after s is
+  // gone: the owner frees it only when no enqueued work uses it).
+  int alloc_in(size_t count, cudaMemPool_t pool, cudaStream_t s, bool free_on_s = false) {
+    if (!pool) return free_on_s ? alloc_on(count, s) : alloc(count);
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), count * sizeof(T), pool, s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_error("cudaMallocFromPoolAsync(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+      return SX_ERR_NOMEM;
+    }
+    n = count;
+    ordered = true;
+    os = free_on_s ? s : nullptr;
+    return SX_OK;
+  }
   int upload(const T *h, size_t count) {
     SX_TRY(alloc(count));
     SX_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
@@ -187,6 +206,18 @@ struct sx_mesh_s {
 
 namespace sx {
 
+// A CUDA event shared by the systems one build enqueued: recorded after
+// their last kernel, waited on by streams that use them.
+struct ReadyEvent {
+  cudaEvent_t ev = nullptr;
+  ReadyEvent() = default;
+  ReadyEvent(const ReadyEvent &) = delete;
+  ReadyEvent &operator=(const ReadyEvent &) = delete;
+  ~ReadyEvent() {
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+
 // One MatrixSys: a (lambda2, betak2, method) system on a mesh.
 struct System {
   sx_mesh_s *mesh = nullptr;
@@ -203,12 +234,20 @@ struct System {
   DBuf<double> pc;         // npts: inverse Jacobi diagonal (JACPCG)
   DBuf<float> pcf;         // FP32 copy
   DBuf<int> status;        // device status bits (1 << SX_ERR_*)
+  // set when the build was enqueued without waiting for it: streams other
+  // than the builder's wait on it before using the system
+  std::shared_ptr<ReadyEvent> ready;
+  cudaMemPool_t pool = nullptr;  // when set, the builders allocate from it
   size_t bytes() const;
 };
 
-int system_build_direct(System &S, cudaStream_t st);
-int system_build_jacobi(System &S, cudaStream_t st);
-int system_build_jacobi_diag(System &S, cudaStream_t st);
+// Builders.  sync = false enqueues on st and returns without waiting: the
+// caller synchronises st (or records an event) and then calls
+// system_check_status.
+int system_build_direct(System &S, cudaStream_t st, bool sync = true);
+int system_build_jacobi(System &S, cudaStream_t st, bool sync = true);
+int system_build_jacobi_diag(System &S, cudaStream_t st, bool sync = true);
+int system_check_status(System &S);
 int system_band_export(const System &S, double *ab);  // LAPACK band, host
 
 // sx_mesh_s::kratio of a mesh description, from host geometry alone.

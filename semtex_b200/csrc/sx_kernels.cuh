@@ -31,6 +31,8 @@ __device__ __forceinline__ float warp_sumf(float v) {
   return v;
 }
 
-int factor_batch(std::vector<System *> &systems, cudaStream_t st);
+// Factor the systems' bands, all systems in each launch; sync = false
+// returns without waiting (statuses to be checked after st completes).
+int factor_batch(std::vector<System *> &systems, cudaStream_t st, bool sync = true);
 
 }  // namespace sx

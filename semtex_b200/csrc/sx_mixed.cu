@@ -492,7 +492,10 @@ __global__ void __launch_bounds__(256) k_x_rhs_multi(MxTable T) {
 // In exact arithmetic these are the iterates of the Jacobi-PCG loop of
 // src/field.cpp:672-704.
 
-enum { CG_INIT = 0, CG_ITER = 1, CG_LAST = 2 };
+enum { CG_INIT = 0, CG_ITER = 1, CG_LAST = 2, CG_MODE = 3 };
+// mode flag: read the chunk's stop flag (set when a plane is expected to stop
+// well before the round ends; otherwise the read is only latency)
+constexpr int CG_CHECK_STOP = 4;
 
 // Element-layout address of (element e, plane chunk y, tensor node t, lane l).
 template <int NN>
@@ -568,11 +571,13 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   __shared__ int staged;
   const int nch = B.nch, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = y * MX_CH + lane, PP = P.PP;
+  const bool check = (mode & CG_CHECK_STOP) != 0;
+  mode &= CG_MODE;
   const bool init = mode == CG_INIT, last = mode == CG_LAST;
   // a chunk whose planes have all stopped leaves r, d (and so x) as they
   // are: its blocks skip the iteration (block-uniform, before any barrier);
   // the last one still folds d into x, with alpha = beta = 0
-  const bool stopped = !init && V.skip[y] != 0;
+  const bool stopped = check && !init && V.skip[y] != 0;
   if (stopped && !last) return;
   const int cur = init ? 0 : (it & 1), nxt = init ? 0 : (cur ^ 1);
   const bool warm = !init && it > 0;  // s, p, d hold previous iterates
@@ -1052,13 +1057,14 @@ static int enqueue_init(const MeshView &M, MixedWork &W, bool any_bc, cudaStream
 
 // One refinement round: the inner solve from r (r0 buffer, d = 0), x += d,
 // then the FP64 residual into r0 for the next round.
-static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, cudaStream_t st, int *nl) {
+static int enqueue_round(const MeshView &M, MixedWork &W, int n_inner, bool check_stop, cudaStream_t st,
+                         int *nl) {
   const MxMember B = member_of(M, W);
   const dim3 eg(M.nel, B.nch);
   *nl = 0;
   SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(B, 0, CG_INIT)));
   for (int it = 0; it < n_inner; it++) {
-    const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
+    const int mode = (it == n_inner - 1 ? CG_LAST : CG_ITER) | (check_stop ? CG_CHECK_STOP : 0);
     SX_NP_SWITCH_M(M.np, (k_cg<N_><<<eg, N_ * 32, cg_smem(N_), st>>>(B, it, mode)));
   }
   SX_NP_SWITCH_M(M.np, (k_x_op64<N_><<<eg, N_ * 32, x64_smem(N_), st>>>(B)));
@@ -1128,7 +1134,7 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
   const int Mc = std::max(1, num_modes);
   {
     // grow-only: a workspace is reused across solves of different sizes
-    auto need = [](auto &b, size_t n) { return b.n < n ? b.alloc(n) : SX_OK; };
+    auto need = [&](auto &b, size_t n) { return b.n < n ? b.alloc_in(n, W.pool, st) : SX_OK; };
     const size_t n = (size_t)PP * npts;
     W.G = grid_nodes(npts);
     SX_TRY(need(W.b64, n));
@@ -1155,7 +1161,7 @@ static int setup(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gr
     SX_TRY(need(W.part, (size_t)PP * (gmax + red_groups(gmax)) * 2));
     const size_t ncnt = (size_t)(PP / MX_CH) * (1 + red_groups(gmax));
     if (W.cnt.n < ncnt) {
-      SX_TRY(W.cnt.alloc(ncnt));
+      SX_TRY(W.cnt.alloc_in(ncnt, W.pool, st));
       SX_TRY(W.cnt.zero(st));
     }
     W.hscal.assign((size_t)2 * PP, 0.0);
@@ -1224,14 +1230,16 @@ static double worst_rel(const double *r2, const double *b2, int PP) {
 
 int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
                 double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild, double tol_rel,
-                int max_refine, int n_inner, bool graphs, cudaStream_t st, sx_solve_stats *stats) {
+                int max_refine, int n_inner, bool check_stop, bool graphs, cudaStream_t st,
+                sx_solve_stats *stats) {
   if (groups.empty()) return SX_OK;
   if (M.mixed) {
     set_error("mixed-precision form does not take Robin (mixed) boundary conditions");
     return SX_ERR_UNSUPPORTED;
   }
   SX_TRY(ensure_constD());
-  if (rebuild || !graphs || !W.g_init || W.n_inner != n_inner || W.graph_epoch != W.epoch) {
+  if (rebuild || !graphs || !W.g_init || W.n_inner != n_inner || W.graph_epoch != W.epoch ||
+      W.check_stop != check_stop) {
     if (W.g_init) cudaGraphExecDestroy(W.g_init);
     if (W.g_round) cudaGraphExecDestroy(W.g_round);
     W.g_init = W.g_round = nullptr;
@@ -1243,9 +1251,11 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     if (graphs) {
       const bool any_bc = d_bc != nullptr;
       SX_TRY(capture(st, &W.g_init, [&]() { return enqueue_init(M, W, any_bc, st, &W.launches_init); }));
-      SX_TRY(capture(st, &W.g_round, [&]() { return enqueue_round(M, W, n_inner, st, &W.launches_round); }));
+      SX_TRY(capture(st, &W.g_round,
+                     [&]() { return enqueue_round(M, W, n_inner, check_stop, st, &W.launches_round); }));
     }
     W.n_inner = n_inner;
+    W.check_stop = check_stop;
     W.graph_epoch = W.epoch;
   }
   // essential values: zeroed here, set from the BC lines inside g_init
@@ -1261,7 +1271,7 @@ int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &gro
     if (graphs)
       SX_CUDA(cudaGraphLaunch(W.g_round, st));
     else
-      SX_TRY(enqueue_round(M, W, n_inner, st, &W.launches_round));
+      SX_TRY(enqueue_round(M, W, n_inner, check_stop, st, &W.launches_round));
     launches += W.launches_round;
     // r2 and b2 lead the scalar block
     SX_CUDA(cudaMemcpyAsync(W.hscal.data(), W.scal.p, sizeof(double) * 2 * PP, cudaMemcpyDeviceToHost, st));
@@ -1362,13 +1372,13 @@ static int enqueue_init_multi(MxBatch &B, bool any_bc, cudaStream_t st, int *nl)
   });
 }
 
-static int enqueue_round_multi(MxBatch &B, int n_inner, cudaStream_t st, int *nl) {
+static int enqueue_round_multi(MxBatch &B, int n_inner, bool check_stop, cudaStream_t st, int *nl) {
   *nl = (int)B.cls.size() * (n_inner + 3);
   return per_class(B, st, [&](const MxBatch::Class &c, cudaStream_t s) {
     const MxTable Te = class_table(B, c, 0), Tn = class_table(B, c, 1);
     SX_NP_SWITCH_M(c.np, (k_cg_multi<N_><<<c.te, N_ * 32, cg_smem(N_), s>>>(Te, 0, CG_INIT)));
     for (int it = 0; it < n_inner; it++) {
-      const int mode = it == n_inner - 1 ? CG_LAST : CG_ITER;
+      const int mode = (it == n_inner - 1 ? CG_LAST : CG_ITER) | (check_stop ? CG_CHECK_STOP : 0);
       SX_NP_SWITCH_M(c.np, (k_cg_multi<N_><<<c.te, N_ * 32, cg_smem(N_), s>>>(Te, it, mode)));
     }
     SX_NP_SWITCH_M(c.np, (k_x_op64_multi<N_><<<c.te, N_ * 32, x64_smem(N_), s>>>(Te)));
@@ -1390,7 +1400,7 @@ static int set_smem_attrs_multi() {
 }
 
 int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, double tol_rel, int max_refine,
-                      int n_inner, bool graphs, cudaStream_t st) {
+                      int n_inner, bool check_stop, bool graphs, cudaStream_t st) {
   const int n = (int)items.size();
   if (n == 0) return SX_OK;
   for (const MxItem &it : items) {
@@ -1405,7 +1415,7 @@ int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, doub
   for (const MxItem &it : items) any_bc |= it.bc != nullptr;
   bool stale = (int)B.order.size() != n || B.epochs.size() != B.order.size();
   for (int m = 0; !stale && m < n; m++) stale = items[B.order[m]].W->epoch != B.epochs[m];
-  if (rebuild || stale || !graphs || !B.g_init || B.n_inner != n_inner) {
+  if (rebuild || stale || !graphs || !B.g_init || B.n_inner != n_inner || B.check_stop != check_stop) {
     B.reset();
     // members by element order, then item order
     B.order.resize(n);
@@ -1466,9 +1476,11 @@ int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, doub
     SX_TRY(ensure_streams(B));
     if (graphs) {
       SX_TRY(capture(st, &B.g_init, [&]() { return enqueue_init_multi(B, any_bc, st, &B.launches_init); }));
-      SX_TRY(capture(st, &B.g_round, [&]() { return enqueue_round_multi(B, n_inner, st, &B.launches_round); }));
+      SX_TRY(capture(st, &B.g_round,
+                     [&]() { return enqueue_round_multi(B, n_inner, check_stop, st, &B.launches_round); }));
     }
     B.n_inner = n_inner;
+    B.check_stop = check_stop;
   }
   // essential values: zeroed here, set from the BC lines inside the init
   for (const MxItem &it : items)
@@ -1483,7 +1495,7 @@ int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, doub
     if (graphs)
       SX_CUDA(cudaGraphLaunch(B.g_round, st));
     else
-      SX_TRY(enqueue_round_multi(B, n_inner, st, &B.launches_round));
+      SX_TRY(enqueue_round_multi(B, n_inner, check_stop, st, &B.launches_round));
     launches += B.launches_round;
     SX_CUDA(cudaMemcpyAsync(B.hnorms.data(), B.norms.p, sizeof(double) * B.hnorms.size(), cudaMemcpyDeviceToHost,
                             st));

@@ -90,6 +90,8 @@ struct MixedWork {
   // setup() counts its runs here; a captured graph (this workspace's own,
   // or a batch's) is valid while the count it was captured at still holds
   unsigned epoch = 0, graph_epoch = 0;
+  bool check_stop = false;  // the captured round reads the chunks' stop flags
+  cudaMemPool_t pool = nullptr;  // when set, setup() allocates from it
   std::vector<double> hscal;
   MxParams prm{};
   ~MixedWork() {
@@ -110,9 +112,13 @@ struct MxGroup {
 // solved by another path -- are neither read nor written).  Stops when every
 // plane's FP64 relative residual ||b - A x|| / ||b|| <= tol_rel or after
 // max_refine rounds.
+// check_stop: the FP32 iterations read each chunk's stop flag, so that
+// chunks whose planes have all stopped skip the rest of the round (worth
+// its latency when some planes need far fewer iterations than the round).
 int mixed_solve(const MeshView &M, MixedWork &W, const std::vector<MxGroup> &groups, int nz, int num_modes,
                 double *d_u, double *d_f, const double *d_bc, long long stride, bool rebuild, double tol_rel,
-                int max_refine, int n_inner, bool graphs, cudaStream_t st, sx_solve_stats *stats);
+                int max_refine, int n_inner, bool check_stop, bool graphs, cudaStream_t st,
+                sx_solve_stats *stats);
 
 // One member of a multi-mesh mixed-precision solve: a mesh, its workspace
 // and plane groups, and the caller's arrays.  `stats` is filled on return.
@@ -150,6 +156,7 @@ struct MxBatch {
   std::vector<cudaEvent_t> events;    // fork + one join per class
   cudaGraphExec_t g_init = nullptr, g_round = nullptr;
   int launches_init = 0, launches_round = 0, n_inner = 0;
+  bool check_stop = false;
   void reset();
   ~MxBatch();
 };
@@ -160,7 +167,7 @@ struct MxBatch {
 // member meets tol_rel, or max_refine.  Returns SX_WARN_STEP_LIMIT when a
 // member did not converge.
 int mixed_solve_multi(std::vector<MxItem> &items, MxBatch &B, bool rebuild, double tol_rel, int max_refine,
-                      int n_inner, bool graphs, cudaStream_t st);
+                      int n_inner, bool check_stop, bool graphs, cudaStream_t st);
 
 // Enqueue `reps` inner-iteration launches (k_cg, iteration 1) on the
 // workspace of the last mixed solve, for timing the kernel on its own.  The

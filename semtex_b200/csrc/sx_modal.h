@@ -66,6 +66,7 @@ struct sx_modal_s {
   int n_inner = 12;                  // FP32 PCG iterations per refinement round, at least
   int mixed_route = 0;               // 0 auto, 1 FP32 CG only, 2 band solve where factored
   bool use_graphs = true;
+  cudaMemPool_t pool = nullptr;      // when set, workspaces are allocated from it
   std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
   int forced_cluster = 0;
   int cluster(int nj);

@@ -23,6 +23,8 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <list>
@@ -33,6 +35,9 @@
 #include "sx_modal.h"
 
 using namespace sx;
+namespace sx {
+const char *last_error();
+}
 using Clock = std::chrono::steady_clock;
 
 namespace {
@@ -72,16 +77,23 @@ struct Req {
   double *u = nullptr;
   Clock::time_point t_submit;
   size_t reserve = 0;  // bytes reserved while in flight
+  size_t build_bytes = 0;  // estimate of the mesh and systems its build adds to the cache
   bool done = false;
   int status = SX_OK;
   double latency_ms = 0.0;
 };
 
+// Cache entries are inserted by the slot that builds them as soon as it
+// starts, so that no two slots build the same entry; `ready` is set when the
+// build is done (a mesh) or enqueued with its event recorded (a system), and
+// `failed` when it went wrong.  A slot waits for other slots' entries only
+// after marking its own ready, so waits cannot form a cycle.
 struct MeshEntry {
   std::unique_ptr<sx_mesh_s> mesh;
   size_t bytes = 0;
   int refs = 0;
   uint64_t last_use = 0;
+  bool ready = false, failed = false;
 };
 
 struct SysEntry {
@@ -90,6 +102,7 @@ struct SysEntry {
   size_t bytes = 0;
   int refs = 0;
   uint64_t last_use = 0;
+  bool ready = false, failed = false;
 };
 
 size_t mesh_estimate(const MeshCopy &m) {
@@ -115,11 +128,11 @@ size_t work_estimate(const MeshCopy &m, int nz, int precision) {
   const size_t npts = m.nglobal + (size_t)m.nel * nint;
   const size_t PP = ((nz + MX_CH - 1) / MX_CH) * MX_CH;
   size_t b = 2 * (size_t)nz * m.nel * nn * 8 + (size_t)nz * std::max(m.nbound, 1) * m.np * 8;  // I/O
-  if (precision == SX_MIXED_FP32)
-    b += PP * npts * (2 * 8 + 9 * 4) + PP * m.nel * nn * 8 + 2 * PP * m.nel * next * 4 + PP * m.nglobal * 8 +
-         npts * (nz / 2 + 1) * 4;
-  else
-    b += (size_t)nz * ((m.nsolve + NB) * 8 + (size_t)m.nel * next * 8 + (size_t)m.nglobal * 8);
+  // band-solve workspace (rhs, condensed forcing, essential values): every
+  // plane in the FP64 form, and any plane the mixed form routes to the band
+  b += (size_t)nz * ((m.nsolve + NB) * 8 + (size_t)m.nel * next * 8 + (size_t)m.nglobal * 8);
+  if (precision == SX_MIXED_FP32)  // node vectors, element vectors, FP64 element results, preconditioner
+    b += PP * npts * (2 * 8 + 4) + PP * m.nel * nn * (6 * 4 + 8 + 2) + PP * m.nglobal * 8 + npts * (nz / 2 + 1) * 4;
   return b;
 }
 
@@ -138,10 +151,42 @@ struct sx_server_s {
   size_t bytes_cached = 0, bytes_reserved = 0;
   std::unordered_map<uint64_t, MeshEntry> meshes;
   std::map<std::tuple<uint64_t, uint64_t, uint64_t, int>, SysEntry> systems;
-  std::mutex build_mu;  // serialises construction of cache entries
   std::vector<std::thread> workers;
   std::vector<double> latencies;
   sx_server_stats st{};
+  // SX_SERVER_TRACE set: one line per batch on stderr (its timeline)
+  bool trace = false;
+  Clock::time_point t_start = Clock::now();
+  // Device memory of the cached systems and the workspaces: a pool grown to
+  // the budget at creation, so that a build or a workspace sub-allocates in
+  // stream order instead of paying a cudaMalloc (~0.2-1 ms each on B200)
+  cudaMemPool_t mem_pool = nullptr;
+  // Before a batch's builds: when the pool's free
+  // reserve is below `need`, grow it by at least POOL_STEP in one allocation
+  // freed at once on `stream`, so that the batch's allocations map nothing.
+  static constexpr size_t POOL_STEP = size_t(4) << 30;
+  void grow_pool(size_t need, cudaStream_t stream) {
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(mem_pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(mem_pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    if (reserved - used >= need) return;
+    size_t step = std::max(need, POOL_STEP);
+    if (reserved + step > cfg.hbm_budget) step = cfg.hbm_budget > reserved ? cfg.hbm_budget - reserved : 0;
+    void *p = nullptr;
+    if (step > 0 && cudaMallocFromPoolAsync(&p, step, mem_pool, stream) == cudaSuccess) cudaFreeAsync(p, stream);
+    cudaGetLastError();  // best effort: the pool still grows on demand
+  }
+  ~sx_server_s() {
+    systems.clear();
+    meshes.clear();
+    if (mem_pool) {
+      cudaDeviceSynchronize();  // the frees above are stream-ordered
+      cudaMemPoolDestroy(mem_pool);
+    }
+  }
 
   // System kind of one mode (caller holds mu): SX_DIRECT for SX_FP64.  For
   // SX_MIXED_FP32 a cached factor is used when there is one; otherwise the
@@ -162,15 +207,22 @@ struct sx_server_s {
   bool admissible(Req *r, size_t &need);
   void evict_for(size_t need, uint64_t keep_mesh);
   void worker(int slot);
-  // One request's mesh and systems, looked up or built (caller holds
-  // build_mu); new band factors are appended to to_factor.
+  using SysKey = std::tuple<uint64_t, uint64_t, uint64_t, int>;
+  // One request's mesh and systems.
   struct Prep {
+    double mesh_ms = 0.0, direct_ms = 0.0, jacobi_ms = 0.0;  // host time of the builds (trace)
     sx_mesh_s *mesh = nullptr;
     std::vector<std::shared_ptr<System>> sys;
-    std::vector<std::tuple<uint64_t, uint64_t, uint64_t, int>> keys;
+    std::vector<SysKey> keys;     // every entry this request holds a reference on
+    std::vector<SysKey> built;    // entries this slot builds
+    std::vector<SysKey> foreign;  // entries another slot was still building
     bool mesh_ref = false;
   };
+  // Look up one request's mesh and systems, and enqueue on `stream`, without
+  // waiting, the builds of those the cache lacks; new band factors are
+  // appended to to_factor.
   int prepare(Req *r, Prep &p, std::vector<System *> &to_factor, cudaStream_t stream);
+  std::condition_variable cv_ready;  // a cache entry became ready
   void release(const Req *r, const Prep &p);
   // A worker's workspace for one batch member.
   struct Member {
@@ -227,31 +279,48 @@ void sx_server_s::evict_for(size_t need, uint64_t keep_mesh) {
 }
 
 int sx_server_s::prepare(Req *r, Prep &pp, std::vector<System *> &to_factor, cudaStream_t stream) {
+  auto since = [](Clock::time_point a) { return std::chrono::duration<double, std::milli>(Clock::now() - a).count(); };
+  bool build_mesh = false;
   {
-    std::lock_guard<std::mutex> lk(mu);
+    std::unique_lock<std::mutex> lk(mu);
     auto it = meshes.find(r->mesh.key);
     if (it != meshes.end()) {
-      pp.mesh = it->second.mesh.get();
       it->second.refs++;
       it->second.last_use = ++tick;
       pp.mesh_ref = true;
       st.mesh_hits++;
+      // a mesh another slot is creating: its creation waits for nothing
+      MeshEntry &e = it->second;
+      cv_ready.wait(lk, [&]() { return e.ready; });
+      if (e.failed) return SX_ERR_CUDA;
+      pp.mesh = e.mesh.get();
+    } else {
+      MeshEntry &e = meshes[r->mesh.key];
+      e.bytes = mesh_estimate(r->mesh);
+      e.refs = 1;
+      e.last_use = ++tick;
+      bytes_cached += e.bytes;
+      pp.mesh_ref = true;
+      st.mesh_misses++;
+      build_mesh = true;
     }
   }
-  if (!pp.mesh) {
+  if (build_mesh) {
+    const auto tm = Clock::now();
     const sx_mesh_desc d = r->mesh.desc();
     sx_mesh m = nullptr;
-    SX_TRY(sx_mesh_create(&d, &m));
-    std::lock_guard<std::mutex> lk(mu);
-    MeshEntry &e = meshes[r->mesh.key];
-    e.mesh.reset(m);
-    e.bytes = mesh_estimate(r->mesh);
-    e.refs = 1;
-    e.last_use = ++tick;
-    bytes_cached += e.bytes;
+    const int rc = sx_mesh_create(&d, &m);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      MeshEntry &e = meshes[r->mesh.key];
+      e.mesh.reset(m);
+      e.ready = true;
+      e.failed = rc != SX_OK;
+    }
+    cv_ready.notify_all();
+    SX_TRY(rc);
     pp.mesh = m;
-    pp.mesh_ref = true;
-    st.mesh_misses++;
+    pp.mesh_ms += since(tm);
   }
   pp.sys.resize(r->num_modes);
   for (int l = 0; l < r->num_modes; l++) {
@@ -259,7 +328,8 @@ int sx_server_s::prepare(Req *r, Prep &pp, std::vector<System *> &to_factor, cud
     uint64_t a, b;
     std::memcpy(&a, &r->lam[l], 8);
     std::memcpy(&b, &r->bk2[l], 8);
-    const auto key = std::make_tuple(r->mesh.key, a, b, kind);
+    const SysKey key = std::make_tuple(r->mesh.key, a, b, kind);
+    std::shared_ptr<System> S;
     {
       std::lock_guard<std::mutex> lk(mu);
       auto it = systems.find(key);
@@ -269,32 +339,38 @@ int sx_server_s::prepare(Req *r, Prep &pp, std::vector<System *> &to_factor, cud
         it->second.last_use = ++tick;
         pp.keys.push_back(key);
         st.system_hits++;
+        if (!it->second.ready && std::find(pp.built.begin(), pp.built.end(), key) == pp.built.end())
+          pp.foreign.push_back(key);
         continue;
       }
-    }
-    auto S = std::make_shared<System>();
-    S->mesh = pp.mesh;
-    S->lambda2 = r->lam[l];
-    S->betak2 = r->bk2[l];
-    S->method = kind;
-    if (kind == SX_DIRECT) {
-      SX_TRY(system_build_direct(*S, stream));
-      if (S->nsolve > 0) to_factor.push_back(S.get());
-      SX_TRY(system_build_jacobi_diag(*S, stream));
-    } else {
-      SX_TRY(system_build_jacobi(*S, stream));
+      S = std::make_shared<System>();
+      S->pool = mem_pool;
+      S->mesh = pp.mesh;
+      S->lambda2 = r->lam[l];
+      S->betak2 = r->bk2[l];
+      S->method = kind;
+      SysEntry &e = systems[key];
+      e.sys = S;
+      e.mesh_key = r->mesh.key;
+      e.bytes = system_estimate(r->mesh, kind);
+      e.refs = 1;
+      e.last_use = ++tick;
+      bytes_cached += e.bytes;
+      pp.keys.push_back(key);
+      pp.built.push_back(key);
+      st.system_misses++;
     }
     pp.sys[l] = S;
-    std::lock_guard<std::mutex> lk(mu);
-    SysEntry &e = systems[key];
-    e.sys = S;
-    e.mesh_key = r->mesh.key;
-    e.bytes = system_estimate(r->mesh, kind);
-    e.refs = 1;
-    e.last_use = ++tick;
-    bytes_cached += e.bytes;
-    pp.keys.push_back(key);
-    st.system_misses++;
+    const auto tb = Clock::now();
+    if (kind == SX_DIRECT) {
+      SX_TRY(system_build_direct(*S, stream, false));
+      if (S->nsolve > 0) to_factor.push_back(S.get());
+      SX_TRY(system_build_jacobi_diag(*S, stream, false));
+      pp.direct_ms += since(tb);
+    } else {
+      SX_TRY(system_build_jacobi(*S, stream, false));
+      pp.jacobi_ms += since(tb);
+    }
   }
   return SX_OK;
 }
@@ -311,6 +387,10 @@ void sx_server_s::release(const Req *r, const Prep &pp) {
   }
 }
 
+// Memory estimate (workspace plus new cache entries) up to which admitted
+// requests are gathered into one batch.
+constexpr size_t BATCH_BYTES = size_t(1) << 30;
+
 // Workspaces above this size are freed after their batch instead of kept
 // for the next one (a pool slot otherwise holds the largest request it saw).
 constexpr size_t KEEP_WS_BYTES = size_t(256) << 20;
@@ -321,16 +401,60 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
   const auto t0 = Clock::now();
   std::vector<Prep> prep(n);
   std::vector<int> rc(n, SX_OK);
+  Clock::time_point tl, tf;
+  size_t nfactor = 0;
   {
-    // look up or build the meshes and systems (one builder at a time), then
-    // factor the batch's new band systems together
-    std::lock_guard<std::mutex> bl(build_mu);
+    // look up the meshes and systems, enqueue the builds of the missing ones
+    // and one factorisation of the batch's new band systems, all on this
+    // slot's stream without waiting (other slots build theirs meanwhile); an
+    // event recorded after them marks the new systems ready for the other
+    // slots' streams
+    tl = Clock::now();
+    size_t need = 0;
+    for (int i = 0; i < n; i++) need += batch[i]->reserve + batch[i]->build_bytes;
+    grow_pool(need, stream);
     std::vector<System *> to_factor;
     for (int i = 0; i < n; i++) rc[i] = prepare(batch[i], prep[i], to_factor, stream);
-    const int fr = factor_batch(to_factor, stream);
-    if (fr != SX_OK)
-      for (int i = 0; i < n; i++) rc[i] = rc[i] == SX_OK ? fr : rc[i];
+    tf = Clock::now();
+    nfactor = to_factor.size();
+    int fr = factor_batch(to_factor, stream, false);
+    auto ev = std::make_shared<ReadyEvent>();
+    if (fr == SX_OK && (cudaEventCreateWithFlags(&ev->ev, cudaEventDisableTiming) != cudaSuccess ||
+                        cudaEventRecord(ev->ev, stream) != cudaSuccess)) {
+      set_error("serving: could not record a build event");
+      fr = SX_ERR_CUDA;
+    }
+    {
+      // this slot's new entries are ready (or failed) for everyone
+      std::lock_guard<std::mutex> lk(mu);
+      for (int i = 0; i < n; i++) {
+        if (fr != SX_OK && rc[i] == SX_OK) rc[i] = fr;
+        for (auto &k : prep[i].built) {
+          auto it = systems.find(k);
+          if (it == systems.end()) continue;
+          it->second.sys->ready = ev;
+          it->second.ready = true;
+          it->second.failed = rc[i] != SX_OK;
+        }
+      }
+    }
+    cv_ready.notify_all();
+    // then the entries other slots were building
+    std::unique_lock<std::mutex> lk(mu);
+    for (int i = 0; i < n; i++)
+      for (auto &k : prep[i].foreign) {
+        auto it = systems.find(k);
+        if (it == systems.end()) continue;
+        SysEntry &e = it->second;
+        cv_ready.wait(lk, [&]() { return e.ready; });
+        if (e.failed && rc[i] == SX_OK) rc[i] = SX_ERR_CUDA;
+      }
   }
+  // systems another slot built: wait (on the device) for their builds
+  for (int i = 0; i < n; i++)
+    for (auto &S : prep[i].sys)
+      if (S && S->ready && S->ready->ev && cudaStreamWaitEvent(stream, S->ready->ev, 0) != cudaSuccess)
+        rc[i] = SX_ERR_CUDA;
   const auto t1 = Clock::now();
   while ((int)pool.size() < n) pool.emplace_back(new Member());
   std::vector<sx_modal> mods;
@@ -347,6 +471,8 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
       m.ws->own = stream;
       m.ws->own_stream_external = true;
       m.ws->use_graphs = false;
+      m.ws->pool = mem_pool;
+      m.ws->mixed.pool = mem_pool;
     }
     sx_modal_s &ws = *m.ws;
     ws.rebind(prep[i].mesh, r->base_mode, r->num_modes, cfg.precision == SX_FP64 ? SX_DIRECT : SX_MIXED,
@@ -354,9 +480,10 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
     ws.n_inner = cfg.inner_iters;
     const size_t len = (size_t)r->nz * r->stride;
     int e = SX_OK;
-    if (m.du.n < len) e = m.du.alloc(len);
-    if (e == SX_OK && m.df.n < len) e = m.df.alloc(len);
-    if (e == SX_OK && !r->bc.empty() && m.dbc.n < r->bc.size()) e = m.dbc.alloc(r->bc.size());
+    if (m.du.n < len) e = m.du.alloc_in(len, mem_pool, stream);
+    if (e == SX_OK && m.df.n < len) e = m.df.alloc_in(len, mem_pool, stream);
+    if (e == SX_OK && !r->bc.empty() && m.dbc.n < r->bc.size())
+      e = m.dbc.alloc_in(r->bc.size(), mem_pool, stream);
     if (e == SX_OK && cudaMemcpyAsync(m.df.p, r->f.data(), len * 8, cudaMemcpyHostToDevice, stream) != cudaSuccess)
       e = SX_ERR_CUDA;
     if (e == SX_OK && !r->bc.empty() &&
@@ -397,6 +524,12 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
       set_error("serving: batch solve or device -> host copy failed");
       for (int i : idx) rc[i] = SX_ERR_CUDA;
     }
+    // the systems' build statuses (interior blocks, band factors)
+    for (size_t k = 0; k < idx.size(); k++)
+      for (auto &S : prep[idx[k]].sys) {
+        const int c = S ? system_check_status(*S) : SX_OK;
+        if (c != SX_OK) rc[idx[k]] = c;
+      }
     // the batch's device-side status words (bounded waits that ran out)
     for (size_t k = 0; k < idx.size(); k++) {
       int h = 0;
@@ -417,10 +550,28 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
     if (pool[i]->bytes > KEEP_WS_BYTES) pool[i].reset(new Member());
   std::lock_guard<std::mutex> lk(mu);
   st.batches++;
-  const double bms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-  const double sms = std::chrono::duration<double, std::milli>(t2 - t1).count();
-  st.build_ms += bms * n;
-  st.solve_ms += sms * n;
+  auto ms = [](Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  st.build_ms += ms(t0, t1) * n;
+  st.solve_ms += ms(t1, t2) * n;
+  if (trace) {
+    double mm = 0.0, dm = 0.0, jm = 0.0;
+    for (auto &p : prep) {
+      mm += p.mesh_ms;
+      dm += p.direct_ms;
+      jm += p.jacobi_ms;
+    }
+    std::fprintf(stderr,
+                 "sx_server batch %llu: %d requests, t=%.1f ms, build %.1f (meshes %.1f, band systems %.1f, "
+                 "Jacobi %.1f), factor and waits %.1f (%zu systems factored), solve %.1f\n",
+                 (unsigned long long)st.batches, n, ms(t_start, t0), ms(tl, tf), mm, dm, jm, ms(tf, t1), nfactor,
+                 ms(t1, t2));
+    for (int i = 0; i < n; i++)
+      if (rc[i] != SX_OK && rc[i] != SX_WARN_STEP_LIMIT)
+        std::fprintf(stderr, "sx_server   request %llu failed: status %d (%s)\n", (unsigned long long)batch[i]->id,
+                     rc[i], sx::last_error());
+  }
 }
 
 void sx_server_s::worker(int slot) {
@@ -438,14 +589,21 @@ void sx_server_s::worker(int slot) {
       std::unique_lock<std::mutex> lk(mu);
       for (;;) {
         if (stopping && pending.empty()) break;
-        // every admissible pending request, in arrival order, up to max_batch
+        // admissible pending requests in arrival order, up to max_batch, and
+        // while the batch's memory estimate stays under BATCH_BYTES: small
+        // requests share a batch, a large one (whose builds and iterations
+        // would hold up the small ones) is served by itself
+        size_t batch_bytes = 0;
         while (!pending.empty() && (int)batch.size() < cfg.max_batch) {
           Req *h = pending.front();
           size_t need = 0;
           if (!admissible(h, need)) evict_for(need, h->mesh.key);
           if (!(admissible(h, need) || (inflight == 0 && batch.empty()))) break;
+          if (!batch.empty() && batch_bytes + need > BATCH_BYTES) break;
+          batch_bytes += need;
           pending.pop_front();
           h->reserve = work_estimate(h->mesh, h->nz, cfg.precision);
+          h->build_bytes = need > h->reserve ? need - h->reserve : 0;
           bytes_reserved += h->reserve;
           inflight++;
           st.queue_ms += std::chrono::duration<double, std::milli>(Clock::now() - h->t_submit).count();
@@ -505,6 +663,17 @@ extern "C" int sx_server_create(const sx_server_config *cfg, sx_server *out) {
     c.hbm_budget = (unsigned long long)(0.8 * fr);
   }
   S->st.bytes_budget = c.hbm_budget;
+  {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = S->device;
+    SX_CUDA(cudaMemPoolCreate(&S->mem_pool, &props));
+    uint64_t keep = ~0ull;  // never hand memory back between requests
+    SX_CUDA(cudaMemPoolSetAttribute(S->mem_pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  S->trace = std::getenv("SX_SERVER_TRACE") != nullptr;
   sx_server_s *p = S.get();
   for (int i = 0; i < c.slots; i++) S->workers.emplace_back([p, i]() { p->worker(i); });
   *out = S.release();
