@@ -426,10 +426,75 @@ def run_ours(args, rank, world):
         l2a, mxa = rel_err(u_batched[2], sols[0])
         l2b, mxb = rel_err(u_batched[3], sols[1])
         line["batched_fp64"]["rel_err_vs_oracle_mode1"] = [max(l2a, l2b), max(mxa, mxb)]
+    if rank == 0 and world == 1:
+        line["multi_mesh"] = run_multi()
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_multi(n_meshes=24, reps=5):
+    """Form (a) on many small meshes (workloads.small_mesh_mix: orders 4-10,
+    4 to 144 elements, 1-12 modes): the same solves (i) one mesh after
+    another with the single-mesh batched form and (ii) as one multi-mesh
+    batch, mixed precision to 1e-12, device-resident inputs, CUDA events on
+    one stream, median of `reps` after a warm-up (graph capture)."""
+    import torch
+    import semtex_b200 as sx
+    from semtex_b200.workloads import small_mesh_mix
+    torch.cuda.set_device(0)
+    reqs = small_mesh_mix(n_meshes)
+    st = torch.cuda.Stream()
+    sptr = st.cuda_stream
+    mem = []
+    for r in reqs:
+        S = sx.ModalMatrixSys(sx.Mesh(r.mesh), num_modes=len(r.lambda2), method=sx.AUTO,
+                              lambda2_modes=r.lambda2, betak2_modes=r.betak2)
+        f0 = torch.tensor(r.forcing, device="cuda")
+        mem.append((S, f0, torch.empty_like(f0), torch.zeros_like(f0), r))
+    dofs = sum(r.dof_solves for r in reqs)
+    B = sx.Batch()
+
+    def one_by_one():
+        for S, _, f, u, r in mem:
+            S.solve_batched(u.data_ptr(), f.data_ptr(), 0, r.nz, r.mesh.nplane, sx.MIXED_FP32, 1e-12,
+                            max_refine=30, stream=sptr)
+
+    def batched():
+        B.solve([(S, u.data_ptr(), f.data_ptr(), None, r.nz, r.mesh.nplane) for S, _, f, u, r in mem],
+                sx.MIXED_FP32, 1e-12, max_refine=30, stream=sptr)
+
+    def timed(fn):
+        out = []
+        for k in range(reps + 1):
+            with torch.cuda.stream(st):
+                for _, f0, f, _, _ in mem:
+                    f.copy_(f0)  # the band-routed modes overwrite their forcing
+            st.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            if k > 0:
+                out.append(e0.elapsed_time(e1))
+        return float(np.median(out))
+
+    t_one = timed(one_by_one)
+    u_one = [u.cpu().numpy() for _, _, _, u, _ in mem]
+    t_bat = timed(batched)
+    worst = 0.0
+    for (_, _, _, u, r), a in zip(mem, u_one):
+        sp = [0] + list(range(2, r.nz)) if r.nz > 1 else [0]
+        worst = max(worst, rel_err(u.cpu().numpy()[sp], a[sp])[0])
+    return {"meshes": n_meshes, "orders": sorted({r.mesh.np - 1 for r in reqs}),
+            "elements": [min(r.mesh.nel for r in reqs), max(r.mesh.nel for r in reqs)],
+            "dof_solves": dofs, "one_by_one_ms": t_one, "batch_ms": t_bat,
+            "one_by_one_dof_solves_per_s": dofs / (t_one * 1e-3),
+            "batch_dof_solves_per_s": dofs / (t_bat * 1e-3), "speedup": t_one / t_bat,
+            "batch_vs_one_by_one_rel_l2": worst,
+            "note": "mixed precision to 1e-12; routing per mode (SX_AUTO); CUDA events on one stream"}
 
 
 def run_serving(n_requests, check_oracle=True):
@@ -533,6 +598,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--serve-only", type=int, default=0, metavar="N",
+                    help="run only the serving loop on the first N requests of the config-4 stream "
+                         "and print its JSON (not a bench line)")
     ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
@@ -542,6 +610,9 @@ def main():
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.serve_only > 0:
+        print(json.dumps({"serving_only": run_serving(args.serve_only, check_oracle=False)}), flush=True)
+        return
     if args.profile:
         run_profile(args)
         return

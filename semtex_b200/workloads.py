@@ -202,6 +202,26 @@ def serving_trace(n_requests, seed=4, rate=2000.0):
     return out
 
 
+def small_mesh_mix(n_meshes=24, seed=9):
+    """Many small meshes of uneven size and order, the case a multi-mesh
+    batch is for: straight-sided E_x x E_y quads of [0,1]^2 with E_x, E_y
+    uniform in [2, 12], order N uniform in {4..10}, a mode count uniform in
+    [1, 12], lambda2 log-uniform in [1e3, 1e5] (plus k^2 per mode), seeded
+    Gaussian Fourier forcing, Dirichlet on every side."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_meshes):
+        ex, ey = (int(v) for v in rng.integers(2, 13, size=2))
+        order = int(rng.integers(4, 11))
+        modes = int(rng.integers(1, 13))
+        lam = float(np.exp(rng.uniform(np.log(1e3), np.log(1e5))))
+        m = rect_mesh(ex, ey, order + 1, 0.0, 1.0, 0.0, 1.0)
+        nz = 1 if modes == 1 else 2 * modes
+        out.append(ServeRequest(0.0, m, np.full(modes, lam), np.arange(modes, dtype=np.float64) ** 2,
+                                fourier_forcing(m, nz, rng)))
+    return out
+
+
 def small_channel(nx=8, ny=6, np_=9, nz=16, lam=1e6, seed=7, jitter=0.15):
     """Small config-2-shaped case for parity tests."""
     m = _jittered_channel(nx, ny, np_, jitter, seed)
