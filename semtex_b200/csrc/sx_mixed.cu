@@ -81,8 +81,8 @@ __device__ __forceinline__ size_t ye_index(const MeshView &M, int e, int a, int 
 // of RED_GROUP blocks (an integer counter per chunk and group) sums the
 // group's partials in block order into part[G + group]; the last group to
 // finish sums the group totals in group order.  Returns true in warp 0 of
-// that last block, with the chunk's totals in fa, fb.  part holds
-// (G + ceil(G / RED_GROUP)) * PP double2; cnt holds nch * (1 + ceil(G /
+// that last block, with the chunk's totals in fa, fb.  part holds (G +
+// ceil(G / RED_GROUP)) * PP double2; cnt holds nch * (1 + ceil(G /
 // RED_GROUP)) counters, zero on entry and left zero.
 constexpr int RED_GROUP = 32;
 inline int red_groups(int G) { return (G + RED_GROUP - 1) / RED_GROUP; }
@@ -98,7 +98,8 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
   const int g0 = grp * RED_GROUP, gn = min(RED_GROUP, G - g0);
   double2 *P1 = reinterpret_cast<double2 *>(part), *P2 = P1 + (size_t)G * PPc;
   unsigned *cg = cnt + nch + (size_t)y * ngrp;
-  // ---- the block's total
+  // ---- the block's total (warp 0 writes it and alone needs the fence
+  // that orders it before the counter)
   sa[row][lane] = a;
   sb[row][lane] = b;
   __syncthreads();
@@ -109,10 +110,9 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
       tb += sb[r][lane];
     }
     P1[(size_t)blk * PPc + p] = make_double2(ta, tb);
+    __threadfence();
+    if (lane == 0) last = (atomicAdd(&cg[grp], 1u) == (unsigned)gn - 1u);
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&cg[grp], 1u) == (unsigned)gn - 1u);
   __syncthreads();
   if (!last) return false;
   // ---- the group's total, over its blocks in order
@@ -133,11 +133,10 @@ __device__ __forceinline__ bool chunk_sum(double a, double b, double *part, unsi
       tb += sb[r][lane];
     }
     P2[(size_t)grp * PPc + p] = make_double2(ta, tb);
+    if (lane == 0) cg[grp] = 0;
+    __threadfence();
+    if (lane == 0) last = (atomicAdd(&cnt[y], 1u) == (unsigned)ngrp - 1u);
   }
-  if (threadIdx.x == 0) cg[grp] = 0;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&cnt[y], 1u) == (unsigned)ngrp - 1u);
   __syncthreads();
   if (!last) return false;
   // ---- the chunk's total, over the groups in order
@@ -617,9 +616,9 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
     beta = (float)beta_in[p];
   }
   const unsigned long long own = M.owner[e];
-  __syncthreads();
-  // the staged spans: thread 0 waits (bounded) and tells the block; the
-  // others then pass the completed phase, which orders the TMA writes for them
+  // the staged spans: thread 0 waits (bounded) before the block's first
+  // barrier, which then also publishes the tables; the others pass the
+  // completed phase after it, which orders the TMA writes for them
   if (threadIdx.x == 0) {
     bool ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);
     if (!ok) {
