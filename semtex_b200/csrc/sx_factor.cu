@@ -201,54 +201,66 @@ __device__ __forceinline__ void tile_store(double *dst, const double *src) {
 }
 
 // Factor the diagonal tile of block column k and store its inverse.
-__global__ void k_potrf(const SysDesc *__restrict__ sys, int k) {
+// Factor the diagonal tile of block column k, A = U^T U (upper), and form
+// D_k = U^-1, one CTA of 256 threads per system.
+//   Cholesky, right-looking: thread t owns column j = t % 64 at rows i = t /
+//   64 (mod 4).  Step c takes d = sqrt(A[c][c]), r = 1/d (every thread, from
+//   the same shared value) and updates A[i][j] -= (A[c][i] r)(A[c][j] r)
+//   for c < i <= j; row c itself is scaled by its owners at step c + 1, when
+//   no thread reads it any more.  One barrier per step.
+//   Inverse, by rows from the bottom: X[i][i] = 1/U[i][i], X[i][j] =
+//   -(sum_{l=i+1..j} U[i][l] X[l][j]) / U[i][i]; four consecutive lanes
+//   split each sum and combine it with two shuffles.  One barrier per row.
+__global__ void __launch_bounds__(256) k_potrf(const SysDesc *__restrict__ sys, int k) {
   const SysDesc S = sys[blockIdx.x];
   if (k >= S.nblk) return;
   extern __shared__ __align__(16) double smp[];
   double *A = smp, *X = smp + TSZ;
   __shared__ int bad;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x;
   double *T = S.tiles + ((size_t)k * (S.J + 1)) * TSZ;
   if (tid == 0) bad = 0;
   tile_load(A, T);
+  for (int idx = tid; idx < TSZ; idx += 256) X[idx] = 0.0;
   __syncthreads();
+  const int j = tid & (NB - 1), rg = tid >> 6;
+  double d_prev = 1.0, r_prev = 1.0;
   for (int c = 0; c < NB; c++) {
-    double d = A[c * LDT + c];
-    if (!(d > 0.0)) {
+    double a = A[c * LDT + c];
+    if (!(a > 0.0)) {
       if (tid == 0) bad = 1;
-      d = 1.0;
+      a = 1.0;
     }
-    d = sqrt(d);
-    __syncthreads();
-    const double rd = 1.0 / d;
-    for (int j = c + 1 + tid; j < NB; j += nt) A[c * LDT + j] *= rd;
-    if (tid == 0) A[c * LDT + c] = d;
-    __syncthreads();
-    const int w = NB - c - 1;
-    for (int idx = tid; idx < w * w; idx += nt) {
-      const int i = c + 1 + idx / w, j = c + 1 + idx % w;
-      if (j >= i) A[i * LDT + j] -= A[c * LDT + i] * A[c * LDT + j];
+    const double d = sqrt(a), r = 1.0 / d;
+    // row c - 1 is final: its owners scale it (and set its diagonal)
+    if (c > 0 && ((c - 1) & 3) == rg && j >= c - 1)
+      A[(c - 1) * LDT + j] = j == c - 1 ? d_prev : A[(c - 1) * LDT + j] * r_prev;
+    if (j > c) {
+      const double ucj = A[c * LDT + j] * r;
+      for (int i = c + 1 + ((rg - (c + 1)) & 3); i <= j; i += 4) A[i * LDT + j] -= (A[c * LDT + i] * r) * ucj;
     }
+    d_prev = d;
+    r_prev = r;
     __syncthreads();
   }
-  for (int idx = tid; idx < NB * NB; idx += nt) {
-    const int i = idx / NB, j = idx % NB;
-    if (j < i) A[i * LDT + j] = 0.0;
+  if (rg == ((NB - 1) & 3) && j == NB - 1) A[(NB - 1) * LDT + NB - 1] = d_prev;
+  __syncthreads();
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int ii = idx / NB, jj = idx % NB;
+    if (jj < ii) A[ii * LDT + jj] = 0.0;
   }
   __syncthreads();
   tile_store(T, A);
-  // X = U^-1 (upper triangular), one column per thread, back substitution.
-  for (int idx = tid; idx < TSZ; idx += nt) X[idx] = 0.0;
-  __syncthreads();
-  for (int j = tid; j < NB; j += nt) {
-    X[j * LDT + j] = 1.0 / A[j * LDT + j];
-    for (int i = j - 1; i >= 0; i--) {
-      double s = 0.0;
-      for (int l = i + 1; l <= j; l++) s += A[i * LDT + l] * X[l * LDT + j];
-      X[i * LDT + j] = -s / A[i * LDT + i];
-    }
+  const int jc = tid >> 2, q = tid & 3;
+  for (int i = NB - 1; i >= 0; i--) {
+    double s = 0.0;
+    if (jc > i)
+      for (int l = i + 1 + q; l <= jc; l += 4) s += A[i * LDT + l] * X[l * LDT + jc];
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (q == 0 && jc >= i) X[i * LDT + jc] = jc == i ? 1.0 / A[i * LDT + i] : -s / A[i * LDT + i];
+    __syncthreads();
   }
-  __syncthreads();
   tile_store(S.dinv + (size_t)k * TSZ, X);
   if (tid == 0 && bad) atomicOr(S.status, 1 << SX_ERR_NOT_SPD);
 }
