@@ -242,6 +242,17 @@ SX_API int sx_profile_band_sweeps(sx_modal modal, int reps, void *stream);
  * the next solve starts afresh. */
 SX_API int sx_profile_mixed_iterations(sx_modal modal, int reps, void *stream);
 
+/* ---- z-direction transform: replaces dDFTr as AuxField::transform uses it --
+ * femlib/fourier.c:47-171, src/auxfield.cpp:1133-1170.  In place on device
+ * data: nz planes plane_stride doubles apart, the first npts points of each
+ * plane transformed along z.  sign = +1: physical -> Fourier, scaled by 1/nz,
+ * planes ordered mode 0, Nyquist (real), then Re/Im of modes 1 .. nz/2 - 1
+ * (the layout every solve entry point takes); sign = -1: back, unscaled.
+ * nz = 1 is a no-op; otherwise nz must be even with prime factors 2, 3, 5.
+ * Enqueued on `stream`; nz = 2, 4, ..., 64 run as one kernel and return at
+ * once, other lengths (which share a workspace) are waited for. */
+SX_API int sx_transform_z(double *d_data, int nz, int plane_stride, int npts, int sign, void *stream);
+
 /* ---- multi-mesh batch (no reference counterpart) --------------------------
  * Solves the planes of several modal systems -- different meshes, element
  * counts, orders and mode sets -- together, on device buffers.  Each is the

@@ -187,3 +187,40 @@ def solve_planes(mesh: OracleMesh, lambda2, beta, forcing, bc, method=DIRECT,
         u0 = None if unknown is None else unknown[k]
         out[k], iters[k] = systems[mode].solve_plane(forcing[k], bc[k], u0, tol_rel, step_max)
     return out, iters
+
+
+def transform_z(data, sign):
+    """dDFTr (femlib/fourier.c:47-171) restated as a direct DFT along axis 0
+    of `data` (nz planes x points), the checker for sx_transform_z.
+
+    Forward (sign=+1): X_k = (1/nz) sum_j x_j exp(-2 pi i j k / nz) -- the
+    sign of DMPFFT's DGPFA call (femlib/temfftd.F:218-238) -- stored as
+    plane 0 = Re X_0, plane 1 = Re X_{nz/2}, planes 2k, 2k+1 = Re X_k,
+    Im X_k (fourier.c:58-63).  Inverse (sign=-1): the unscaled sum back.
+    """
+    x = np.asarray(data, dtype=np.float64)
+    nz = x.shape[0]
+    if nz == 1:
+        return x.copy()
+    assert nz % 2 == 0
+    nh = nz // 2
+    j = np.arange(nz)
+    out = np.empty_like(x)
+    if sign == 1:
+        for k in range(nh + 1):
+            ang = 2.0 * np.pi * ((j * k) % nz) / nz
+            re = (np.cos(ang) @ x) / nz
+            im = (-np.sin(ang) @ x) / nz
+            if k == 0:
+                out[0] = re
+            elif k == nh:
+                out[1] = re
+            else:
+                out[2 * k] = re
+                out[2 * k + 1] = im
+        return out
+    out[:] = x[0] + np.where(j % 2 == 0, 1.0, -1.0)[:, None] * x[1]
+    for k in range(1, nh):
+        ang = 2.0 * np.pi * ((j * k) % nz) / nz
+        out += 2.0 * (np.cos(ang)[:, None] * x[2 * k] - np.sin(ang)[:, None] * x[2 * k + 1])
+    return out

@@ -127,6 +127,7 @@ def _load():
     L.sx_modal_status.argtypes = [vp]
     L.sx_modal_tune.argtypes = [vp, ip, ip]
     L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
+    L.sx_transform_z.argtypes = [vp, ip, ip, ip, ip, vp]
     L.sx_batch_create.argtypes = [P(vp)]
     L.sx_batch_destroy.argtypes = [vp]
     L.sx_batch_solve.argtypes = [vp, ip, P(vp), P(vp), P(vp), P(vp), P(ip), P(ip), ip, dp, ip, vp,
@@ -342,6 +343,14 @@ class ModalMatrixSys:
 
     def __del__(self):
         self.close()
+
+
+def transform_z(d_data, nz, plane_stride, npts=None, sign=1, stream=0):
+    """z-direction transform of nz device planes in place (dDFTr,
+    femlib/fourier.c:47-171): sign=+1 physical -> Fourier (1/nz, semtex
+    plane order), sign=-1 back."""
+    _check(lib.sx_transform_z(d_data, nz, plane_stride, plane_stride if npts is None else npts, sign, stream),
+           "sx_transform_z")
 
 
 class Batch:
