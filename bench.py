@@ -606,11 +606,26 @@ def run_profile(args):
            nz = 16 (8 systems, ~0.5 GB of factors, larger than L2)
     mixed: the mixed-precision batched form on the full config-2 workload
            with Jacobi systems only (no band factors, ~0.3 GB resident)
+    transform: the z-direction transform of the config-2 field (nz = 64,
+           82,944 points, 42 MB), forward and inverse, `steps` times each,
+           a 256 MB write between calls
     """
     import torch
     import semtex_b200 as sx
     from semtex_b200.workloads import config2
     torch.cuda.set_device(0)
+    if args.profile == "transform":
+        w = config2()
+        d = torch.tensor(w.forcing, device="cuda")
+        l2 = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+        sptr = torch.cuda.current_stream().cuda_stream
+        for _ in range(max(1, args.steps)):
+            for sign in (+1, -1):
+                l2.zero_()
+                sx.transform_z(d.data_ptr(), w.nz, w.mesh.nplane, w.mesh.nplane, sign, sptr)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "transform", "nz": w.nz, "points": w.mesh.nplane}), flush=True)
+        return
     if args.profile == "band":
         w = config2(ny=16, nz=16)
         method = sx.DIRECT
@@ -652,7 +667,7 @@ def main():
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
-    ap.add_argument("--profile", choices=["band", "mixed"], default=None,
+    ap.add_argument("--profile", choices=["band", "mixed", "transform"], default=None,
                     help="bounded run of one kernel family for ncu (no bench line)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
