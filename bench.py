@@ -541,6 +541,24 @@ def run_transform(reps=20):
                 "round_trip_max_rel_err": float(np.abs(back - w.forcing).max() / np.abs(w.forcing).max()),
                 "l2": "flushed between timed calls (256 MB written)",
                 "kernel": "k_z_fwd<64> / k_z_inv<64>: one pass, each point's z-line in registers"})
+    # config 3 and 5 field shapes: one pass through shared memory
+    for name, nz2, pts in (("nz128_config3", 128, 64 * 64 * 121), ("nz256_config5", 256, 128 * 64 * 121)):
+        x = torch.randn((nz2, pts), dtype=torch.float64, device="cuda")
+        sx.transform_z(x.data_ptr(), nz2, pts, pts, +1, sptr)
+        ts = []
+        for _ in range(max(3, reps // 4)):
+            l2.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sx.transform_z(x.data_ptr(), nz2, pts, pts, +1, sptr)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        gbs = 2.0 * nz2 * pts * 8 / (ms * 1e-3) / 1e9
+        out[name] = {"forward_ms": ms, "achieved_gbs": gbs, "frac": gbs / peak,
+                     "kernel": f"k_z_fwd_s<{nz2}>"}
+        del x
     return out
 
 

@@ -11,7 +11,8 @@
 //   inverse (sign = -1): x_j = X_0 + (-1)^j X_{nz/2} + 2 sum_{k=1}^{nz/2-1}
 //     Re(X_k exp(+2 pi i j k / nz)), unscaled, so that inverse(forward(x))
 //     = x.
-// Lengths 2, 4, ..., 64 (config 2 uses 64): one pass, k_z_fwd / k_z_inv.
+// Lengths 2, 4, ..., 64 (config 2 uses 64): one pass, k_z_fwd / k_z_inv;
+// 128, 256, 512: one pass through shared memory, k_z_fwd_s / k_z_inv_s.
 // A thread holds one point's whole z-line in registers: the real transform
 // of length N is a complex FFT of length M = N/2 on z_m = x_2m + i x_2m+1
 // (radix-2, decimation in time, every index a compile-time constant), then
@@ -84,8 +85,10 @@ bool factors_235(int n) {
 
 }  // namespace
 
-// exp(-2 pi i t / 64), t = 0 .. 32, from the host's cos / sin in FP64.
-__constant__ double c_twr[33], c_twi[33];
+// exp(-2 pi i t / TWN), t = 0 .. TWN/2, from the host's cos / sin in FP64;
+// a length-L stage uses t = j * (TWN / L).
+constexpr int TWN = 512;
+__constant__ double c_twr[TWN / 2 + 1], c_twi[TWN / 2 + 1];
 
 static int ensure_twiddles() {
   static std::mutex mu;
@@ -94,16 +97,16 @@ static int ensure_twiddles() {
   SX_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 256 && done[dev]) return SX_OK;
-  double wr[33], wi[33];
-  for (int t = 0; t <= 32; t++) {
-    const double a = 2.0 * M_PI * t / 64.0;
+  double wr[TWN / 2 + 1], wi[TWN / 2 + 1];
+  for (int t = 0; t <= TWN / 2; t++) {
+    const double a = 2.0 * M_PI * t / TWN;
     wr[t] = std::cos(a);
     wi[t] = -std::sin(a);
   }
-  wr[16] = 0.0;   // exact at the quarter and half turns
-  wi[16] = -1.0;
-  wr[32] = -1.0;
-  wi[32] = 0.0;
+  wr[TWN / 4] = 0.0;  // exact at the quarter and half turns
+  wi[TWN / 4] = -1.0;
+  wr[TWN / 2] = -1.0;
+  wi[TWN / 2] = 0.0;
   SX_CUDA(cudaMemcpyToSymbol(c_twr, wr, sizeof(wr)));
   SX_CUDA(cudaMemcpyToSymbol(c_twi, wi, sizeof(wi)));
   if (dev < 256) done[dev] = 1;
@@ -131,7 +134,7 @@ struct FftStage {
     for (int i = 0; i < M; i += LEN) {
 #pragma unroll
       for (int j = 0; j < LEN / 2; j++) {
-        const int t = j * (64 / LEN);
+        const int t = j * (TWN / LEN);
         const double wr = c_twr[t], wi = INV ? -c_twi[t] : c_twi[t];
         const int a = i + j, b = i + j + LEN / 2;
         const double vr = re[b] * wr - im[b] * wi, vi = re[b] * wi + im[b] * wr;
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(128) k_z_fwd(double *__restrict__ data, int np
     const double yr = re[M - k], yi = -im[M - k];  // conj Z_{M-k}
     const double er = 0.5 * (re[k] + yr), ei = 0.5 * (im[k] + yi);
     const double orr = 0.5 * (im[k] - yi), oi = -0.5 * (re[k] - yr);  // (Z_k - conj Z_{M-k}) / 2i
-    const int t = k * (64 / N);
+    const int t = k * (TWN / N);
     const double wr = c_twr[t], wi = c_twi[t];
     data[(2 * k) * stride + p] = (er + (orr * wr - oi * wi)) * scale;
     data[(2 * k + 1) * stride + p] = (ei + (orr * wi + oi * wr)) * scale;
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(128) k_z_inv(double *__restrict__ data, int np
       const double cr = side ? ar : br, ci = side ? -ai : -bi;  // conj X_{M-q}
       const double er = 0.5 * (xr + cr), ei = 0.5 * (xi + ci);
       const double dr = 0.5 * (xr - cr), di = 0.5 * (xi - ci);
-      const int t = q * (64 / N);
+      const int t = q * (TWN / N);
       const double wr = c_twr[t], wi = -c_twi[t];  // conj W^q
       const double orr = dr * wr - di * wi, oi = dr * wi + di * wr;
       re[bitrev(q, LB)] = er - oi;  // E + i O
@@ -222,6 +225,136 @@ __global__ void __launch_bounds__(128) k_z_inv(double *__restrict__ data, int np
     data[(2 * m) * stride + p] = 2.0 * re[m];
     data[(2 * m + 1) * stride + p] = 2.0 * im[m];
   }
+}
+
+// Lengths 128, 256, 512: a block of four warps takes 32 points (lane =
+// point); the half-length complex sequence of each point lies in shared
+// memory, Zr/Zi[m][32], and the warps share each radix-2 stage's
+// butterflies, a barrier between stages.  Same steps as the register
+// kernels; loads and stores of a plane are 32 consecutive doubles.
+constexpr size_t zsmem(int nz) { return (size_t)nz * 32 * sizeof(double); }
+
+template <int N>
+__device__ __forceinline__ void smem_stages(double *Zr, double *Zi, bool inv) {
+  constexpr int M = N / 2;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int len = 2; len <= M; len <<= 1) {
+    const int h = len >> 1;
+    for (int b = w; b < M / 2; b += 4) {
+      const int j = b & (h - 1), a = (b - j) * 2 + j, c = a + h;
+      const int t = j * (TWN / len);
+      const double wr = c_twr[t], wi = inv ? -c_twi[t] : c_twi[t];
+      const double br = Zr[c * 32 + lane], bi = Zi[c * 32 + lane];
+      const double vr = br * wr - bi * wi, vi = br * wi + bi * wr;
+      const double ar = Zr[a * 32 + lane], ai = Zi[a * 32 + lane];
+      Zr[c * 32 + lane] = ar - vr;
+      Zi[c * 32 + lane] = ai - vi;
+      Zr[a * 32 + lane] = ar + vr;
+      Zi[a * 32 + lane] = ai + vi;
+    }
+    __syncthreads();
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_z_fwd_s(double *__restrict__ data, int npts, long long stride,
+                                                  double scale) {
+  constexpr int M = N / 2, LB = ilog2c(M);
+  extern __shared__ __align__(16) double zs[];
+  double *Zr = zs, *Zi = zs + M * 32;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * 32 + lane;
+  const bool ok = p < npts;
+  for (int m = w; m < M; m += 4) {
+    const int r = (int)(__brev((unsigned)m) >> (32 - LB));
+    Zr[r * 32 + lane] = ok ? data[(2 * m) * stride + p] : 0.0;
+    Zi[r * 32 + lane] = ok ? data[(2 * m + 1) * stride + p] : 0.0;
+  }
+  __syncthreads();
+  smem_stages<N>(Zr, Zi, false);
+  if (!ok) return;  // no barrier follows
+  for (int k = w; k <= M / 2; k += 4) {
+    if (k == 0) {
+      data[p] = (Zr[lane] + Zi[lane]) * scale;
+      data[stride + p] = (Zr[lane] - Zi[lane]) * scale;
+      continue;
+    }
+    // X_k from Z_k and conj Z_{M-k}; and X_{M-k} from the same pair
+    const int kk = M - k;
+    const double zr = Zr[k * 32 + lane], zi = Zi[k * 32 + lane];
+    const double qr = Zr[kk * 32 + lane], qi = Zi[kk * 32 + lane];
+    for (int side = 0; side < (k == kk ? 1 : 2); side++) {
+      const int q = side ? kk : k;
+      const double ar = side ? qr : zr, ai = side ? qi : zi;   // Z_q
+      const double yr = side ? zr : qr, yi = side ? -zi : -qi;  // conj Z_{M-q}
+      const double er = 0.5 * (ar + yr), ei = 0.5 * (ai + yi);
+      const double orr = 0.5 * (ai - yi), oi = -0.5 * (ar - yr);
+      const int t = q * (TWN / N);
+      const double wr = c_twr[t], wi = c_twi[t];
+      data[(2 * q) * stride + p] = (er + (orr * wr - oi * wi)) * scale;
+      data[(2 * q + 1) * stride + p] = (ei + (orr * wi + oi * wr)) * scale;
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_z_inv_s(double *__restrict__ data, int npts, long long stride) {
+  constexpr int M = N / 2, LB = ilog2c(M);
+  extern __shared__ __align__(16) double zs[];
+  double *Zr = zs, *Zi = zs + M * 32;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * 32 + lane;
+  const bool ok = p < npts;
+  auto rev = [](int v) { return (int)(__brev((unsigned)v) >> (32 - LB)); };
+  for (int k = w; k <= M / 2; k += 4) {
+    if (k == 0) {
+      const double x0 = ok ? data[p] : 0.0, xm = ok ? data[stride + p] : 0.0;
+      Zr[0 * 32 + lane] = 0.5 * (x0 + xm);
+      Zi[0 * 32 + lane] = 0.5 * (x0 - xm);
+      continue;
+    }
+    const int kk = M - k;
+    const double ar = ok ? data[(2 * k) * stride + p] : 0.0, ai = ok ? data[(2 * k + 1) * stride + p] : 0.0;
+    const double br = ok ? data[(2 * kk) * stride + p] : 0.0, bi = ok ? data[(2 * kk + 1) * stride + p] : 0.0;
+    for (int side = 0; side < (k == kk ? 1 : 2); side++) {
+      const int q = side ? kk : k;
+      const double xr = side ? br : ar, xi = side ? bi : ai;
+      const double cr = side ? ar : br, ci = side ? -ai : -bi;
+      const double er = 0.5 * (xr + cr), ei = 0.5 * (xi + ci);
+      const double dr = 0.5 * (xr - cr), di = 0.5 * (xi - ci);
+      const int t = q * (TWN / N);
+      const double wr = c_twr[t], wi = -c_twi[t];
+      const double orr = dr * wr - di * wi, oi = dr * wi + di * wr;
+      Zr[rev(q) * 32 + lane] = er - oi;
+      Zi[rev(q) * 32 + lane] = ei + orr;
+    }
+  }
+  __syncthreads();
+  smem_stages<N>(Zr, Zi, true);
+  if (!ok) return;
+  for (int m = w; m < M; m += 4) {
+    data[(2 * m) * stride + p] = 2.0 * Zr[m * 32 + lane];
+    data[(2 * m + 1) * stride + p] = 2.0 * Zi[m * 32 + lane];
+  }
+}
+
+template <int N>
+static int launch_smem(double *d, int npts, long long stride, int sign, cudaStream_t st) {
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, []() {
+    attr = cudaFuncSetAttribute(k_z_fwd_s<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem(N));
+    if (attr == cudaSuccess)
+      attr = cudaFuncSetAttribute(k_z_inv_s<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem(N));
+  });
+  SX_CUDA(attr);
+  const int grid = (npts + 31) / 32;
+  if (sign == 1)
+    k_z_fwd_s<N><<<grid, 128, zsmem(N), st>>>(d, npts, stride, 1.0 / N);
+  else
+    k_z_inv_s<N><<<grid, 128, zsmem(N), st>>>(d, npts, stride);
+  return SX_OK;
 }
 
 template <int N>
@@ -294,6 +427,18 @@ extern "C" int sx_transform_z(double *d_data, int nz, int plane_stride, int npts
       case 16: launch_reg<16>(d_data, npts, plane_stride, sign, st); break;
       case 32: launch_reg<32>(d_data, npts, plane_stride, sign, st); break;
       default: launch_reg<64>(d_data, npts, plane_stride, sign, st); break;
+    }
+    SX_CUDA(cudaGetLastError());
+    return SX_OK;
+  }
+  if (nz <= TWN && (nz & (nz - 1)) == 0) {
+    // one pass through shared memory, enqueued without waiting
+    SX_TRY(ensure_twiddles());
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (nz) {
+      case 128: SX_TRY(launch_smem<128>(d_data, npts, plane_stride, sign, st)); break;
+      case 256: SX_TRY(launch_smem<256>(d_data, npts, plane_stride, sign, st)); break;
+      default: SX_TRY(launch_smem<512>(d_data, npts, plane_stride, sign, st)); break;
     }
     SX_CUDA(cudaGetLastError());
     return SX_OK;

@@ -375,15 +375,31 @@ int sx_server_s::prepare(Req *r, Prep &pp, std::vector<System *> &to_factor, cud
   return SX_OK;
 }
 
+// Drop the request's references (caller has synchronised the slot's
+// stream, so no work of this batch is in flight); an entry whose build
+// failed leaves the cache with its last reference, so that a later request
+// builds it again.
 void sx_server_s::release(const Req *r, const Prep &pp) {
   std::lock_guard<std::mutex> lk(mu);
-  if (pp.mesh_ref) {
-    auto mi = meshes.find(r->mesh.key);
-    if (mi != meshes.end()) mi->second.refs--;
-  }
   for (auto &k : pp.keys) {
     auto si = systems.find(k);
-    if (si != systems.end()) si->second.refs--;
+    if (si == systems.end()) continue;
+    if (--si->second.refs == 0 && si->second.failed) {
+      bytes_cached -= si->second.bytes;
+      systems.erase(si);
+    }
+  }
+  if (pp.mesh_ref) {
+    auto mi = meshes.find(r->mesh.key);
+    if (mi != meshes.end() && --mi->second.refs == 0 && mi->second.failed) {
+      bool used = false;
+      for (auto &s : systems)
+        if (s.second.mesh_key == mi->first) used = true;
+      if (!used) {
+        bytes_cached -= mi->second.bytes;
+        meshes.erase(mi);
+      }
+    }
   }
 }
 
@@ -540,6 +556,9 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
       }
     }
   }
+  // builds enqueued for requests that failed before the solve may still run
+  if (cudaStreamSynchronize(stream) != cudaSuccess)
+    for (int i = 0; i < n; i++) rc[i] = rc[i] == SX_OK ? SX_ERR_CUDA : rc[i];
   const auto t2 = Clock::now();
   for (int i = 0; i < n; i++) {
     release(batch[i], prep[i]);

@@ -4,8 +4,9 @@ CPU: the oracle's direct-DFT restatement against a known answer (a single
 cosine and sine mode), against an independent FFT-based computation of the
 same packing, and for its own round trip.  GPU: sx_transform_z against the
 oracle for even lengths with factors 2, 3, 5 and ragged point counts, and
-the forward-inverse round trip in place -- both the one-pass register
-kernels (2, 4, ..., 64) and the cuFFT path (other lengths).
+the forward-inverse round trip in place -- the one-pass register kernels
+(2, 4, ..., 64), the shared-memory kernels (128, 256, 512) and the cuFFT
+path (other lengths).
 """
 import numpy as np
 import pytest
@@ -46,8 +47,9 @@ def test_oracle_matches_fft_packing_and_round_trip(nz):
 @pytest.mark.gpu
 @pytest.mark.parametrize("nz,npts,stride", [(2, 33, 34), (4, 130, 130), (8, 129, 132), (16, 82944, 82944),
                                             (32, 300, 300), (64, 4096, 4100), (64, 82944, 82944),
-                                            (6, 1000, 1000), (30, 257, 260), (128, 999, 1000),
-                                            (256, 2050, 2050)])
+                                            (128, 999, 1000), (256, 2050, 2050), (256, 410240, 410240),
+                                            (512, 100, 100), (6, 1000, 1000), (30, 257, 260),
+                                            (96, 333, 340), (160, 70, 72)])
 def test_transform_matches_oracle(nz, npts, stride):
     import torch
     import semtex_b200 as sx
