@@ -179,3 +179,42 @@ def test_multi_rejects_duplicate_member(sx, torch):
     B = sx.Batch()
     with pytest.raises(sx.SolverError):
         B.solve([m.args(), m.args()], sx.MIXED_FP32)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_multi_with_boundary_values(sx, torch, precision):
+    """Members with essential and natural boundary data (the reference
+    goldens laplace1: sin(2 pi x) on the top wall; laplace4: du/dn on the
+    top) beside a channel member without any: each member's essential
+    values and <h, w> terms come from its own BC lines inside the batch,
+    within the form's bar of the oracle."""
+    from tests.problems import build_2d
+    from semtex_b200.workloads import Workload, small_channel
+    prec = sx.MIXED_FP32 if precision == "mixed" else sx.FP64
+    tol = MIXED_TOL if precision == "mixed" else 1e-12
+    members, oracles = [], []
+    for name in ("laplace1", "laplace4"):
+        m, p, f, bc, _ = build_2d(name)
+        w = Workload(name, m, 1, 0.0, np.array([p["lambda2"]]), np.array([0.0]), f)
+        mem = Member(sx, torch, w)
+        mem.bc = torch.tensor(bc, device="cuda")
+        members.append(mem)
+        uo, _ = solve_planes(OracleMesh(m), p["lambda2"], 0.0, f, bc)
+        oracles.append(uo)
+    wc = small_channel(nx=4, ny=3, np_=7, nz=4, lam=1e4, seed=17)
+    mc = Member(sx, torch, wc)
+    mc.bc = None
+    members.append(mc)
+    oracles.append(mc.oracle())
+    for m in members:
+        if precision == "mixed":
+            m.S.tune(mixed_route=sx.ROUTE_CG, inner_iters=200)
+    B = sx.Batch()
+    args = [(m.S, m.u.data_ptr(), m.f.data_ptr(), m.bc.data_ptr() if m.bc is not None else None,
+             m.w.nz, m.w.mesh.nplane) for m in members]
+    B.solve(args, prec, 1e-13, max_refine=40)
+    torch.cuda.synchronize()
+    for m, uo in zip(members, oracles):
+        sp = solved_planes(m.w.nz)
+        l2, mx = rel_errs(m.u.cpu().numpy()[sp], uo[sp])
+        assert l2 <= tol and mx <= tol, (m.w.name, precision, l2, mx)
