@@ -691,24 +691,114 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   return SX_OK;
 }
 
+sx_modal_s::HostPipe::~HostPipe() {
+  views.clear();
+  for (cudaEvent_t e : in) cudaEventDestroy(e);
+  for (cudaEvent_t e : done) cudaEventDestroy(e);
+  if (h2d) cudaStreamDestroy(h2d);
+  if (d2h) cudaStreamDestroy(d2h);
+}
+
+// Modes per chunk of the pipelined host entry: 32 planes, one full lane
+// chunk of the mixed form's kernels.
+constexpr int HOST_CHUNK_MODES = 16;
+
 extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *f, const double *bc,
                                            int nz, int plane_stride, int precision, double tol_rel,
                                            int max_refine, sx_solve_stats *stats) {
   if (!s || !u || !f || nz <= 0 || plane_stride <= 0) return SX_ERR_ARG;
   const size_t n = (size_t)nz * plane_stride;
-  const size_t nbc = (size_t)nz * std::max(s->mesh->nbound, 1) * s->mesh->np;
+  const size_t bcp = (size_t)std::max(s->mesh->nbound, 1) * s->mesh->np;  // bc values per plane
+  const size_t nbc = (size_t)nz * bcp;
   if (s->hu.n < n) SX_TRY(s->hu.alloc(n));
   if (s->hf.n < n) SX_TRY(s->hf.alloc(n));
   if (bc && s->hbc.n < nbc) SX_TRY(s->hbc.alloc(nbc));
   if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
   cudaStream_t st = s->own;
-  SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));
-  if (bc) SX_CUDA(cudaMemcpyAsync(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice, st));
-  const int rc = solve_batched_on(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride, precision,
-                                  tol_rel, max_refine, st, stats);
-  if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
-  SX_TRY(copy_solved_planes(u, s->hu.p, nz, plane_stride, s->base_mode, st));
-  SX_TRY(take_status(s, true, st, false));
+  const int nmodes = nz == 1 ? 1 : nz / 2;
+  const int nchunks = (nmodes + HOST_CHUNK_MODES - 1) / HOST_CHUNK_MODES;
+  if (nchunks < 2 || nz % 2 || nmodes > s->num_modes) {
+    SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));
+    if (bc) SX_CUDA(cudaMemcpyAsync(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice, st));
+    const int rc = solve_batched_on(s, s->hu.p, s->hf.p, bc ? s->hbc.p : nullptr, nz, plane_stride, precision,
+                                    tol_rel, max_refine, st, stats);
+    if (rc != SX_OK && rc != SX_WARN_STEP_LIMIT) return rc;
+    SX_TRY(copy_solved_planes(u, s->hu.p, nz, plane_stride, s->base_mode, st));
+    SX_TRY(take_status(s, true, st, false));
+    return rc;
+  }
+  // Pipelined: every chunk's forcing goes up on one stream at once; the
+  // chunks are solved in turn on `st`, each after its copy has landed; a
+  // chunk's solution goes down on a third stream while the next one is
+  // solved.  Chunk c covers modes [16c, 16c + 16), planes [32c, 32c + 32)
+  // (chunk 0 keeps the Nyquist plane 1 in place).
+  if (!s->pipe) s->pipe.reset(new sx_modal_s::HostPipe());
+  sx_modal_s::HostPipe &P = *s->pipe;
+  if (!P.h2d) SX_CUDA(cudaStreamCreateWithFlags(&P.h2d, cudaStreamNonBlocking));
+  if (!P.d2h) SX_CUDA(cudaStreamCreateWithFlags(&P.d2h, cudaStreamNonBlocking));
+  while ((int)P.in.size() < nchunks) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    SX_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    SX_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    P.in.push_back(a);
+    P.done.push_back(b);
+  }
+  while ((int)P.views.size() < nchunks) P.views.emplace_back(new sx_modal_s());
+  // the views share the system objects; their workspaces are their own
+  SX_CUDA(cudaEventRecord(P.in[0], st));  // the device buffers are free once st's earlier work is done
+  SX_CUDA(cudaStreamWaitEvent(P.h2d, P.in[0], 0));
+  for (int c = 0; c < nchunks; c++) {
+    const int m0 = c * HOST_CHUNK_MODES, m1 = std::min(nmodes, m0 + HOST_CHUNK_MODES);
+    const size_t off = (size_t)2 * m0 * plane_stride, len = (size_t)2 * (m1 - m0) * plane_stride;
+    SX_CUDA(cudaMemcpyAsync(s->hf.p + off, f + off, len * 8, cudaMemcpyHostToDevice, P.h2d));
+    if (bc)
+      SX_CUDA(cudaMemcpyAsync(s->hbc.p + 2 * m0 * bcp, bc + 2 * m0 * bcp, 2 * (m1 - m0) * bcp * 8,
+                              cudaMemcpyHostToDevice, P.h2d));
+    SX_CUDA(cudaEventRecord(P.in[c], P.h2d));
+  }
+  int rc = SX_OK;
+  sx_solve_stats tot{};
+  for (int c = 0; c < nchunks; c++) {
+    const int m0 = c * HOST_CHUNK_MODES, m1 = std::min(nmodes, m0 + HOST_CHUNK_MODES);
+    sx_modal_s &v = *P.views[c];
+    const std::vector<std::shared_ptr<System>> sub(s->sys.begin() + m0, s->sys.begin() + m1);
+    if (v.mesh != s->mesh || v.base_mode != s->base_mode + m0 || v.num_modes != m1 - m0 || v.sys != sub)
+      v.rebind(s->mesh, s->base_mode + m0, m1 - m0, s->method, sub);
+    v.own = st;
+    v.own_stream_external = true;
+    v.n_inner = s->n_inner;
+    v.mixed_route = s->mixed_route;
+    if (v.forced_cluster != s->forced_cluster) {
+      v.forced_cluster = s->forced_cluster;
+      v.fp64.reset();
+      v.hyb.reset();
+    }
+    if (!v.dstatus.p) {
+      SX_TRY(v.dstatus.alloc(1));
+      SX_TRY(v.dstatus.zero(st));
+    }
+    const size_t off = (size_t)2 * m0 * plane_stride;
+    SX_CUDA(cudaStreamWaitEvent(st, P.in[c], 0));
+    sx_solve_stats cs{};
+    const int r = solve_batched_on(&v, s->hu.p + off, s->hf.p + off, bc ? s->hbc.p + 2 * m0 * bcp : nullptr,
+                                   2 * (m1 - m0), plane_stride, precision, tol_rel, max_refine, st, &cs);
+    if (r != SX_OK && r != SX_WARN_STEP_LIMIT) return r;
+    if (r == SX_WARN_STEP_LIMIT) rc = r;
+    SX_CUDA(cudaEventRecord(P.done[c], st));
+    SX_CUDA(cudaStreamWaitEvent(P.d2h, P.done[c], 0));
+    SX_TRY(copy_solved_planes(u + off, s->hu.p + off, 2 * (m1 - m0), plane_stride, v.base_mode, P.d2h));
+    tot.planes_solved += cs.planes_solved;
+    tot.planes_direct += cs.planes_direct;
+    tot.iterations_max = std::max(tot.iterations_max, cs.iterations_max);
+    tot.iterations_total += cs.iterations_total;
+    tot.refinements = std::max(tot.refinements, cs.refinements);
+    tot.final_rel_residual = std::max(tot.final_rel_residual, cs.final_rel_residual);
+    tot.kernel_launches += cs.kernel_launches;
+  }
+  SX_CUDA(cudaStreamSynchronize(P.d2h));
+  for (auto &v : P.views)
+    if (v->dstatus.p) SX_TRY(take_status(v.get(), true, st, false));
+  if (stats) *stats = tot;
   return rc;
 }
 

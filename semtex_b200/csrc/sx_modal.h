@@ -70,6 +70,15 @@ struct sx_modal_s {
   std::map<int, int> cluster_for;    // jobs per launch -> band-sweep cluster size
   int forced_cluster = 0;
   int cluster(int nj);
+  // host-buffer entry, pipelined: per-chunk views of this system (16 modes
+  // each, sharing its systems) and the copy streams and events
+  struct HostPipe {
+    std::vector<std::unique_ptr<sx_modal_s>> views;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    std::vector<cudaEvent_t> in, done;
+    ~HostPipe();
+  };
+  std::unique_ptr<HostPipe> pipe;
   // Point this object at another mesh and set of systems, keeping the
   // workspace buffers (the serving loop reuses one object per slot).
   void rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vector<std::shared_ptr<sx::System>> s);

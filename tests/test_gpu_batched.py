@@ -189,3 +189,24 @@ def test_batched_host_entry(sx, torch):
     uh = S.solve_batched_host(w.forcing)
     sp = solved_planes(w.nz)
     assert np.array_equal(uh[sp], ud[sp])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_host_entry_pipelined(sx, torch, precision):
+    """More than 16 modes: the host entry solves chunks of 16 modes with
+    their copies overlapped; every plane matches the single device-side
+    batched solve (FP64: to rounding; mixed: within the 1e-10 bar), and the
+    Nyquist plane is left as the caller passed it."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=4, ny=3, np_=6, nz=40, lam=1e5, seed=23)
+    _, S = _setup(sx, w)
+    prec = sx.FP64 if precision == "fp64" else sx.MIXED_FP32
+    ud, _ = _run_device(torch, S, w, batched=True, precision=prec, tol=1e-12)
+    out = np.full_like(w.forcing, 7.0)
+    uh = S.solve_batched_host(w.forcing, out=out, precision=prec, tol_rel=1e-12, max_refine=40)
+    sp = solved_planes(w.nz)
+    l2, mx = rel_errs(uh[sp], ud[sp])
+    tol = 1e-13 if precision == "fp64" else MIXED_TOL
+    assert l2 <= tol and mx <= tol, (precision, l2, mx)
+    assert np.all(uh[1] == 7.0)
+    assert S.last_stats["planes_solved"] == len(sp)
