@@ -909,7 +909,10 @@ __device__ __forceinline__ void unpack_body(const MxMember &B, int e, int y) {
   const MeshView &M = B.M;
   const MxParams &P = B.P;
   const double *__restrict__ x64 = B.V.x64;
-  __shared__ double V[NN * MX_CH];
+  // [NN][33]: the store loop reads a column (one plane) across threads, and
+  // the odd row length keeps those reads on distinct banks
+  constexpr int VS = MX_CH + 1;
+  __shared__ double V[NN * VS];
   __shared__ int emap[NN];
   const int tid = threadIdx.x, row = tid >> 5, lane = tid & 31;
   const int p0 = y * MX_CH, p = p0 + lane, PP = P.PP;
@@ -924,14 +927,14 @@ __device__ __forceinline__ void unpack_body(const MxMember &B, int e, int y) {
     } else {
       v = x64[((size_t)M.nglobal + (size_t)e * M.nint + (a - NE)) * PP + p];
     }
-    V[emap[a] * MX_CH + lane] = v;
+    V[emap[a] * VS + lane] = v;
   }
   __syncthreads();
-  for (int q = 0; q < MX_CH; q++) {
-    const int pl = p0 + q;
-    if (!real_plane(P, pl)) continue;
-    double *u = P.u + (size_t)pl * P.stride + (size_t)e * NN;
-    for (int k = tid; k < NN; k += 256) u[k] = V[k * MX_CH + q];
+  // plane q's NN values are contiguous in the caller's array: all threads
+  // over (plane, node) pairs
+  for (int i = tid; i < MX_CH * NN; i += 256) {
+    const int q = i / NN, k = i - q * NN, pl = p0 + q;
+    if (real_plane(P, pl)) P.u[(size_t)pl * P.stride + (size_t)e * NN + k] = V[k * VS + q];
   }
 }
 
