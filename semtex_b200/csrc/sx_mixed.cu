@@ -616,9 +616,23 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
     beta = (float)beta_in[p];
   }
   const unsigned long long own = M.owner[e];
-  // the staged spans: thread 0 waits (bounded) before the block's first
-  // barrier, which then also publishes the tables; the others pass the
-  // completed phase after it, which orders the TMA writes for them
+  __syncthreads();  // the tables
+  // Global loads of phase A -- A u of the previous launch at the element's
+  // boundary nodes through their holders (or r at INIT) -- issued now, so
+  // that their latency overlaps the staging instead of following it.
+  float gv[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    const int a = w + k * NP, g = gtab[a];
+    gv[k] = 0.0f;
+    if (!(a >= NE || g < ns)) continue;
+    if (init)
+      gv[k] = V.r0[(size_t)g * PP + p];
+    else if (!last && a < NE)
+      gv[k] = gather_we<NN>(M, Win, w4[a], g, nch, y, lane, emt);
+  }
+  // the staged spans: thread 0 waits (bounded) and tells the block; the
+  // others then pass the completed phase, which orders the TMA writes for them
   if (threadIdx.x == 0) {
     bool ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);
     if (!ok) {
@@ -631,20 +645,8 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   if (!staged) return;  // block-uniform
   if (threadIdx.x != 0) mbar_wait(&bar, 0, CG_WAIT_LIMIT);
 
-  // ---- phase A: vector updates at the element's nodes, u = PC r -> B0.
-  // Global loads first (the boundary gathers, or r at INIT), all in flight
-  // together; then the updates on the staged spans.
-  float gv[NP];
-#pragma unroll
-  for (int k = 0; k < NP; k++) {
-    const int a = w + k * NP, g = gtab[a];
-    gv[k] = 0.0f;
-    if (!(a >= NE || g < ns)) continue;
-    if (init)
-      gv[k] = V.r0[(size_t)g * PP + p];
-    else if (!last && a < NE)
-      gv[k] = gather_we<NN>(M, Win, w4[a], g, nch, y, lane, emt);
-  }
+  // ---- phase A: vector updates at the element's nodes on the staged
+  // spans, u = PC r -> B0
   double gam = 0.0;
 #pragma unroll
   for (int k = 0; k < NP; k++) {
