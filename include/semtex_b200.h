@@ -207,16 +207,20 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
  *                         bytes than three band solves go to the FP64 band
  *                         Cholesky, when the mode is factored), 1 = FP32 CG
  *                         for every mode, 2 = band Cholesky for every
- *                         factored mode                                   */
-enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3 };
+ *                         factored mode
+ *   SX_TUNE_BAND_STAGES   band-sweep tiles in flight per CTA, 2..4 (auto:
+ *                         4, or 2 when that lets a larger cluster stay
+ *                         resident -- two CTAs then share an SM)          */
+enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3, SX_TUNE_BAND_STAGES = 4 };
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 
 /* Autotuner (no reference counterpart): times the batched form on the
  * caller's own data for each candidate schedule and keeps the fastest in the
  * modal system, as sx_modal_tune would set it --
  *   the band-sweep cluster size (CTAs sharing one system's tiles; sizes the
- *   SM groups cannot hold are skipped), for SX_FP64 and for the modes that
- *   SX_MIXED_FP32 routes to the band Cholesky;
+ *   SM groups cannot hold are skipped) and ring depth (4 or 2 tiles in
+ *   flight per CTA), for SX_FP64 and for the modes that SX_MIXED_FP32
+ *   routes to the band Cholesky;
  *   the floor on FP32 iterations per refinement round, for SX_MIXED_FP32.
  * d_f is only read (each trial solves a copy, allocated for the duration);
  * d_u holds the last trial's solution.  Candidates whose solve does not
@@ -226,6 +230,7 @@ typedef struct {
   int inner_iters;  /* chosen floor on FP32 iterations per round (0: FP64 form) */
   double ms;        /* one solve with the chosen schedule                     */
   int trials;       /* schedules timed                                        */
+  int band_stages;  /* chosen band-sweep ring depth (0: no band sweeps)       */
 } sx_tune_result;
 SX_API int sx_modal_autotune(sx_modal modal, double *d_u, const double *d_f, const double *d_bc, int nz,
                              int plane_stride, int precision, double tol_rel, int max_refine, void *stream,

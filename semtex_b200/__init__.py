@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libsemtex_b200.so")
 DIRECT, JACPCG, MIXED_SOLVER, AUTO = 0, 1, 2, 3
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
-TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE = 1, 2, 3
+TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE, TUNE_BAND_STAGES = 1, 2, 3, 4
 ROUTE_AUTO, ROUTE_CG, ROUTE_BAND = 0, 1, 2
 STATIC_SCRATCH_BYTES = 4 << 20  # SX_STATIC_SCRATCH_BYTES
 
@@ -63,7 +63,7 @@ class SolveStats(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("band_cluster", C.c_int), ("inner_iters", C.c_int), ("ms", C.c_double),
-                ("trials", C.c_int)]
+                ("trials", C.c_int), ("band_stages", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -307,7 +307,7 @@ class ModalMatrixSys:
         self.last_stats = st.as_dict()
         return u
 
-    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None):
+    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None, band_stages=None):
         """Schedule knobs of the batched forms (None leaves a knob alone, 0
         restores its default).  mixed_route: ROUTE_AUTO (by cost), ROUTE_CG
         (FP32 CG for every mode), ROUTE_BAND (band Cholesky for every
@@ -318,6 +318,8 @@ class ModalMatrixSys:
             _check(lib.sx_modal_tune(self.h, TUNE_BAND_CLUSTER, int(band_cluster)), "sx_modal_tune")
         if mixed_route is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_MIXED_ROUTE, int(mixed_route)), "sx_modal_tune")
+        if band_stages is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_BAND_STAGES, int(band_stages)), "sx_modal_tune")
 
     def autotune(self, d_u, d_f, d_bc, nz, stride, precision=FP64, tol_rel=1e-12, max_refine=20, stream=0):
         """Time the batched form's candidate schedules on this data (device

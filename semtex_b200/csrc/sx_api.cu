@@ -14,16 +14,23 @@ using namespace sx;
 // sx_modal_s
 // ---------------------------------------------------------------------------
 
-int sx_modal_s::cluster(int nj) {
-  if (forced_cluster > 0) return forced_cluster;
-  auto it = cluster_for.find(nj);
-  if (it != cluster_for.end()) return it->second;
-  int J = 1;
-  for (auto &s : uniq) J = std::max(J, s->J);
-  // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
-  const int c = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2);
-  cluster_for[nj] = c;
-  return c;
+int sx_modal_s::cluster(int nj, int *stages) {
+  int S = forced_stages > 0 ? forced_stages : BAND_STAGES_MAX, C = forced_cluster;
+  if (C <= 0) {
+    auto it = cluster_for.find(nj);
+    if (it != cluster_for.end()) {
+      C = it->second.first;
+      S = it->second.second;
+    } else {
+      int J = 1;
+      for (auto &s : uniq) J = std::max(J, s->J);
+      // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
+      C = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2, &S, forced_stages);
+      cluster_for[nj] = std::make_pair(C, S);
+    }
+  }
+  if (stages) *stages = S;
+  return C;
 }
 
 void sx_modal_s::rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vector<std::shared_ptr<System>> s) {
@@ -232,6 +239,13 @@ extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
       if (value < 0 || value > 2) return SX_ERR_ARG;
       s->mixed_route = value;
       return SX_OK;
+    case SX_TUNE_BAND_STAGES:
+      if (value == 1 || value > BAND_STAGES_MAX) return SX_ERR_ARG;
+      s->forced_stages = value > 0 ? value : 0;
+      s->cluster_for.clear();
+      s->fp64.reset();
+      s->hyb.reset();
+      return SX_OK;
     default:
       return SX_ERR_ARG;
   }
@@ -349,7 +363,9 @@ extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const
     std::vector<Job> one(1, jobs[i]);
     if (S.method == SX_DIRECT) {
       int nl = 0;
-      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st, s->cluster(1), &nl));
+      int S = BAND_STAGES_MAX;
+      const int C = s->cluster(1, &S);
+      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st, C, &nl, S));
       loc.kernel_launches += nl;
     } else {
       int iters = 0;
@@ -423,13 +439,13 @@ static int direct_batched(sx_modal_s *s, DirectBatch &B, const std::vector<Group
     SX_CUDA(cudaMemcpyAsync(B.djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
     SX_CUDA(cudaStreamSynchronize(st));
     SX_TRY(prepare_direct_kernels(M));
-    B.C = s->cluster((int)jobs.size());
+    B.C = s->cluster((int)jobs.size(), &B.S);
     B.jobs = jobs;
     B.modes = modes;
-    if (!s->use_graphs) return direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches);
+    if (!s->use_graphs) return direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches, B.S);
     cudaGraph_t g = nullptr;
     SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches);
+    const int rc = direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches, B.S);
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc != SX_OK) {
       if (g) cudaGraphDestroy(g);
@@ -615,11 +631,13 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   }
   int J = 1;
   for (auto &u : s->uniq) J = std::max(J, u->J);
-  std::vector<int> clusters, inners;
+  std::vector<std::pair<int, int>> clusters;  // (cluster size, ring depth)
+  std::vector<int> inners;
   if (band)
-    for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
-      if (C <= J && band_active_clusters(C, 2, J + 2) > 0) clusters.push_back(C);
-  if (clusters.empty()) clusters.push_back(0);
+    for (int S : {BAND_STAGES_MAX, 2})
+      for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
+        if (C <= J && band_active_clusters(C, 2, J + 2, S) > 0) clusters.push_back(std::make_pair(C, S));
+  if (clusters.empty()) clusters.push_back(std::make_pair(0, 0));
   if (precision == SX_MIXED_FP32)
     inners = {8, 12, 16, 24};
   else
@@ -630,15 +648,16 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   SX_CUDA(cudaEventCreate(&e0));
   SX_CUDA(cudaEventCreate(&e1));
-  const int saved_cluster = s->forced_cluster, saved_inner = s->n_inner;
+  const int saved_cluster = s->forced_cluster, saved_stages = s->forced_stages, saved_inner = s->n_inner;
   double best = INFINITY;
   bool best_ok = false;
-  int bc = saved_cluster, bi = saved_inner, trials = 0, rc = SX_OK;
-  for (int C : clusters)
+  int bc = saved_cluster, bs = saved_stages, bi = saved_inner, trials = 0, rc = SX_OK;
+  for (auto CS : clusters)
     for (int I : inners) {
-      s->forced_cluster = C;
+      s->forced_cluster = CS.first;
+      s->forced_stages = CS.second;
       if (I > 0) s->n_inner = I;
-      s->fp64.reset();  // the captured graphs bake in the cluster size
+      s->fp64.reset();  // the captured graphs bake in the cluster size and ring depth
       s->hyb.reset();
       double t_min = INFINITY;
       int r = SX_OK;
@@ -664,7 +683,8 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
       if ((ok && !best_ok) || (ok == best_ok && t_min < best)) {
         best = t_min;
         best_ok = ok;
-        bc = C;
+        bc = CS.first;
+        bs = CS.second;
         bi = I > 0 ? I : saved_inner;
       }
     }
@@ -675,7 +695,9 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   s->hyb.reset();
   s->mkey[0] = s->mkey[1] = s->mkey[2] = nullptr;
   s->forced_cluster = trials ? bc : saved_cluster;
+  s->forced_stages = trials ? bs : saved_stages;
   s->n_inner = trials ? bi : saved_inner;
+  s->cluster_for.clear();
   SX_CUDA(cudaStreamSynchronize(st));
   if (rc != SX_OK) return rc;
   if (!trials) {
@@ -684,6 +706,7 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   }
   if (out) {
     out->band_cluster = band ? s->forced_cluster : 0;
+    out->band_stages = band ? std::max(s->forced_stages, 0) : 0;
     out->inner_iters = precision == SX_MIXED_FP32 ? s->n_inner : 0;
     out->ms = best;
     out->trials = trials;
@@ -819,7 +842,8 @@ int sx::copy_solved_planes(double *h_u, const double *d_u, int nz, int plane_str
 extern "C" int sx_profile_band_sweeps(sx_modal s, int reps, void *stream) {
   if (!s || reps <= 0 || s->fp64.jobs.empty()) return SX_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  for (int r = 0; r < reps; r++) SX_TRY(band_sweep_jobs(s->fp64.djobs.p, s->fp64.jobs, s->fp64.C, st));
+  for (int r = 0; r < reps; r++)
+    SX_TRY(band_sweep_jobs(s->fp64.djobs.p, s->fp64.jobs, s->fp64.C, st, s->fp64.S));
   return SX_OK;
 }
 
@@ -888,6 +912,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
     key.push_back(q.nz);
     key.push_back(q.stride);
     key.push_back(q.s->forced_cluster);
+    key.push_back(q.s->forced_stages);
     for (auto &g : q.gd) key.push_back(g.mode);
     key.push_back(-1);
   }
@@ -901,7 +926,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
   b->dkey.clear();
   std::vector<Job> jobs;
   std::vector<size_t> j0;
-  int maxJ = 1, maxP = 1, forced = 0;
+  int maxJ = 1, maxP = 1, forced = 0, fstages = 0;
   for (Part &q : parts) {
     j0.push_back(jobs.size());
     if (q.gd.empty()) continue;
@@ -914,6 +939,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
       slot += g.P;
     }
     forced = std::max(forced, q.s->forced_cluster);
+    fstages = std::max(fstages, q.s->forced_stages);
     SX_TRY(prepare_direct_kernels(q.s->mesh->view()));
   }
   j0.push_back(jobs.size());
@@ -921,8 +947,11 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
   SX_CUDA(cudaMemcpyAsync(b->djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
   SX_CUDA(cudaStreamSynchronize(st));
   b->jobs = jobs;
+  b->S = BAND_STAGES_MAX;
   b->C = forced > 0 ? forced
-                    : pick_cluster((int)jobs.size(), std::min(16, std::max(1, maxJ)), maxP <= 2 ? 2 : 8, maxJ + 2);
+                    : pick_cluster((int)jobs.size(), std::min(16, std::max(1, maxJ)), maxP <= 2 ? 2 : 8, maxJ + 2,
+                                   &b->S, fstages);
+  if (forced > 0 && fstages > 0) b->S = fstages;
   auto body = [&]() -> int {
     int nl = 0;
     for (size_t i = 0; i < parts.size(); i++) {
@@ -930,7 +959,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
       const std::vector<Job> slice(jobs.begin() + j0[i], jobs.begin() + j0[i + 1]);
       SX_TRY(direct_rhs_jobs(parts[i].s->mesh->view(), b->djobs.p + j0[i], slice, st, &nl));
     }
-    SX_TRY(band_sweep_jobs(b->djobs.p, jobs, b->C, st));
+    SX_TRY(band_sweep_jobs(b->djobs.p, jobs, b->C, st, b->S));
     nl++;
     for (size_t i = 0; i < parts.size(); i++) {
       if (parts[i].gd.empty()) continue;

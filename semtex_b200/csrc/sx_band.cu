@@ -20,6 +20,8 @@
 // Every wait is bounded (clock64); on timeout the kernel records
 // SX_ERR_TIMEOUT in the status word, drains its own bulk copies (bounded),
 // meets the other CTAs at a final cluster barrier and returns.
+#include <algorithm>
+
 #include "sx_kernels.cuh"
 #include "sx_ptx.cuh"
 #include "sx_solve.cuh"
@@ -281,7 +283,7 @@ static int smem_optin() {
 }
 
 // Launch both sweeps for every job: cluster size C per job.
-int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st) {
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st, int smax) {
   const int nj = (int)hjobs.size();
   if (nj == 0) return SX_OK;
   int maxP = 0, Wmax = 0;
@@ -292,7 +294,7 @@ int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cuda
   if (maxP > 8) return SX_ERR_UNSUPPORTED;
   const int pmax = maxP <= 2 ? 2 : 8;
   const int limit = smem_optin();
-  int S = 4;
+  int S = std::max(2, std::min(smax, BAND_STAGES_MAX));
   while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)limit) S--;
   const size_t sm = sweep_smem(pmax, C, S, Wmax);
   if (sm > (size_t)limit) {
@@ -329,8 +331,8 @@ int prepare_band_kernels() {
 
 // Largest cluster size (<= cmax) for which `nj` clusters can be resident at
 // once; at least 1.
-int band_active_clusters(int C, int pmax, int Wmax) {
-  int S = 4;
+int band_active_clusters(int C, int pmax, int Wmax, int smax) {
+  int S = std::max(2, std::min(smax, BAND_STAGES_MAX));
   while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
   if (sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) return 0;
   cudaLaunchConfig_t cfg = {};
@@ -354,32 +356,44 @@ int band_active_clusters(int C, int pmax, int Wmax) {
   return n;
 }
 
-int pick_cluster(int nj, int cmax, int pmax, int Wmax) {
-  int best = 1;
-  for (int C = 1; C <= cmax; C++) {
-    int S = 4;
-    while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(C * nj, 1, 1);
-    cfg.blockDim = dim3(256, 1, 1);
-    cfg.dynamicSmemBytes = sweep_smem(pmax, C, S, Wmax);
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int n = 0;
-    const cudaError_t e = pmax == 2 ? cudaOccupancyMaxActiveClusters(&n, k_band_sweep<2>, &cfg)
-                                    : cudaOccupancyMaxActiveClusters(&n, k_band_sweep<8>, &cfg);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      continue;
+// Largest cluster size C <= cmax (and ring depth) for which all nj clusters
+// are resident at once, over the ring depths 4 and 2 (a shallower ring
+// halves a CTA's shared memory, so that two fit an SM); the deeper ring on
+// a tie.  stages_forced > 0 fixes the depth.
+int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out, int stages_forced) {
+  int bestC = 1, bestS = BAND_STAGES_MAX;
+  for (int S0 : {BAND_STAGES_MAX, 2}) {
+    if (stages_forced > 0 && S0 != stages_forced) continue;
+    for (int C = 1; C <= cmax; C++) {
+      int S = S0;
+      while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(C * nj, 1, 1);
+      cfg.blockDim = dim3(256, 1, 1);
+      cfg.dynamicSmemBytes = sweep_smem(pmax, C, S, Wmax);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = C;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int n = 0;
+      const cudaError_t e = pmax == 2 ? cudaOccupancyMaxActiveClusters(&n, k_band_sweep<2>, &cfg)
+                                      : cudaOccupancyMaxActiveClusters(&n, k_band_sweep<8>, &cfg);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      if (n >= nj && C > bestC) {
+        bestC = C;
+        bestS = S0;
+      }
     }
-    if (n >= nj) best = C;
   }
-  return best;
+  if (stages_forced > 0) bestS = stages_forced;
+  if (stages_out) *stages_out = bestS;
+  return bestC;
 }
 
 }  // namespace sx

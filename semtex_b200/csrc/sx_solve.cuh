@@ -70,8 +70,11 @@ __device__ __forceinline__ void helm_op(const T *D, const T *Q1, const T *Q2, co
 
 // Direct solve of all jobs; the band sweeps run one cluster of C CTAs per job.
 // Returns the number of kernels launched through *launches when non-null.
+// Ring depth (tiles in flight per CTA) of the band sweeps: at most 4; 2
+// lets two CTAs share an SM, so that larger clusters stay resident.
+constexpr int BAND_STAGES_MAX = 4;
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st, int C, int *launches = nullptr);
+                      cudaStream_t st, int C, int *launches = nullptr, int stages = BAND_STAGES_MAX);
 // The phases of direct_solve_jobs, for batches whose band sweeps run in one
 // launch across meshes: essential values, condensed RHS (element kernels
 // and direct-stiffness sum); then, after the sweeps, the interior
@@ -79,12 +82,13 @@ int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job
 int direct_rhs_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs, cudaStream_t st,
                     int *launches);
 int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_t st, int *launches);
-int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st);
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st,
+                    int stages = BAND_STAGES_MAX);
 int prepare_band_kernels();
-int pick_cluster(int nj, int cmax, int pmax, int Wmax);
+int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out = nullptr, int stages_forced = 0);
 // Clusters of C band-sweep CTAs that can be resident at once (0: C does not
 // fit an SM group, so a launch with it would fail).
-int band_active_clusters(int C, int pmax, int Wmax);
+int band_active_clusters(int C, int pmax, int Wmax, int stages = BAND_STAGES_MAX);
 size_t sweep_smem(int pmax, int C, int S, int Wmax);
 // Set kernel attributes (max dynamic smem) ahead of any stream capture.
 int prepare_direct_kernels(const MeshView &M);

@@ -108,7 +108,8 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
   cudaStream_t st = (cudaStream_t)stream;
   const MeshView M = s->mesh->view();
   SX_TRY(prepare_direct_kernels(M));
-  const int C = s->cluster(1);
+  int stages = BAND_STAGES_MAX;
+  const int C = s->cluster(1, &stages);
   const long long bcstride = (long long)std::max(Mh.nbound, 1) * Mh.np;
   // one host Job, reused: the 1-element vector is allocated once per thread
   thread_local std::vector<Job> one(1);
@@ -149,7 +150,7 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
     // in full by k_rhs_dss / k_rhs_elem before anything reads them.
     SX_CUDA(cudaMemcpyAsync(djob, &j, sizeof(Job), cudaMemcpyHostToDevice, st));
     int nl = 0;
-    SX_TRY(direct_solve_jobs(M, djob, one, st, C, &nl));
+    SX_TRY(direct_solve_jobs(M, djob, one, st, C, &nl, stages));
     loc.kernel_launches += nl;
     loc.planes_solved += g.P;
   }

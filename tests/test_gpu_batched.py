@@ -64,12 +64,14 @@ def _run_device(torch, S, w, batched=True, precision=0, tol=1e-12, bc=None):
     return u.cpu().numpy(), st
 
 
-@pytest.mark.parametrize("cluster", [0, 1, 2, 3, 5])
-def test_batched_fp64_equals_plain(sx, torch, cluster):
+@pytest.mark.parametrize("cluster,stages", [(0, 0), (1, 0), (2, 0), (3, 0), (5, 0), (2, 2), (5, 2), (3, 3)])
+def test_batched_fp64_equals_plain(sx, torch, cluster, stages):
+    """Every band-sweep cluster size and ring depth (tiles in flight per
+    CTA) gives the plain form's answer to rounding."""
     from semtex_b200.workloads import small_channel
     w = small_channel(nx=8, ny=8, np_=9, nz=12, lam=1e6, seed=11)
     _, S = _setup(sx, w)
-    S.tune(band_cluster=cluster)
+    S.tune(band_cluster=cluster, band_stages=stages)
     up, _ = _run_device(torch, S, w, batched=False)
     ub, st = _run_device(torch, S, w, batched=True)
     sp = solved_planes(w.nz)
@@ -170,6 +172,7 @@ def test_autotune_keeps_results(sx, torch):
     u = torch.zeros_like(f)
     r64 = S.autotune(u.data_ptr(), f.data_ptr(), 0, w.nz, w.mesh.nplane, sx.FP64)
     assert r64["trials"] >= 1 and r64["band_cluster"] >= 1 and r64["ms"] > 0.0
+    assert r64["band_stages"] in (2, 3, 4)
     assert np.array_equal(f.cpu().numpy(), w.forcing)
     ub2, _ = _run_device(torch, S, w, batched=True)
     sp = solved_planes(w.nz)
