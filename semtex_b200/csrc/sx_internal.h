@@ -269,12 +269,18 @@ int cg_round_iters(double kratio, double hcon);
 // mode is charged only for its bytes):
 //   CG:     rounds of max(n_inner, cg_round_iters) iterations, one round per
 //           1e-6 of tol_rel; each iteration streams 4 (8 npts + 2 nel np^2)
-//           bytes per plane at 2.1 TB/s (k_cg, measured)
-//   band:   the factor twice plus hbi/hii at 1.9 TB/s (k_band_sweep with 32
-//           systems, measured)
+//           bytes per plane at 2.1 TB/s
+//   band:   the factor twice plus hbi/hii at 1.9 TB/s
 //   factor: nsolve nband^2 flops at 3.9 TFLOP/s (config-2 set-up,
 //           measured), divided by `reuse`, the solves expected per factored
 //           system (0: already factored, no cost).
+// The two streaming rates are calibration constants: k_cg's and
+// k_band_sweep's rates when the rule was set up.  Both kernels are faster
+// now (about 2.7 and 2.8 TB/s); with those rates the rule sends more modes
+// of a serving request to the band, and a request's factorisation, whose
+// block-column steps are latency-bound, costs more than the flop estimate
+// above -- the serving stream ran slower (makespan 7.2-7.7 s against
+// 5.3-7.8 s in an A/B on one box), so the calibrated pair stays.
 // A mode whose rounds would exceed CG_ROUND_CAP iterations, or whose CG would
 // need more than max_refine rounds, goes to the band.
 bool band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon, int n_inner,
