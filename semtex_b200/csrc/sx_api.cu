@@ -631,6 +631,8 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   }
   int J = 1;
   for (auto &u : s->uniq) J = std::max(J, u->J);
+  // the occupancy queries below need the sweep kernels' shared-memory limit
+  if (band) SX_TRY(prepare_direct_kernels(s->mesh->view()));
   std::vector<std::pair<int, int>> clusters;  // (cluster size, ring depth)
   std::vector<int> inners;
   if (band)

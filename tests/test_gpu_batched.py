@@ -159,6 +159,18 @@ def test_mixed_hybrid_route_vs_oracle(sx, torch, method):
         assert l2 <= MIXED_TOL and mx <= MIXED_TOL, (p, l2, mx, st)
 
 
+def test_autotune_first_call_finds_clusters(sx, torch):
+    """The autotuner as the first band-sweep call of the process-fresh
+    system: it still finds (and times) several cluster schedules."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=8, ny=8, np_=10, nz=12, lam=1e6, seed=29)
+    _, S = _setup(sx, w)
+    f = torch.tensor(w.forcing, device="cuda")
+    u = torch.zeros_like(f)
+    r = S.autotune(u.data_ptr(), f.data_ptr(), 0, w.nz, w.mesh.nplane, sx.FP64)
+    assert r["trials"] > 1 and r["band_cluster"] >= 1, r
+
+
 def test_autotune_keeps_results(sx, torch):
     """The autotuner picks a schedule among the candidates, leaves the
     forcing untouched, and the batched forms give the same answers after it:
