@@ -129,7 +129,12 @@ __global__ void k_elem_condense(MeshView M, double hCon, double *__restrict__ hb
   double *ob = hbi_out + (size_t)e * next * nint;
   for (int i = tid; i < next * nint; i += nt) ob[i] = t[i];
   double *oi = hii_out + (size_t)e * nint * nint;
-  for (int i = tid; i < nint * nint; i += nt) oi[i] = hii[i];
+  // column-major, (r, c) at c * nint + r: the back-substitution's threads
+  // own rows and read a column per step
+  for (int o = tid; o < nint * nint; o += nt) {
+    const int c = o / nint, r = o - c * nint;
+    oi[o] = hii[r * nint + c];
+  }
   double *oh = hbb_out + (size_t)e * next * next;
   for (int i = tid; i < next * next; i += nt) oh[i] = hbb[i];
   if (tid == 0 && bad) atomicOr(status, 1 << SX_ERR_SINGULAR_HII);

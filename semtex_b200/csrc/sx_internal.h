@@ -229,7 +229,7 @@ struct System {
   DBuf<double> tiles;      // nblk*(J+1)*TSZ
   DBuf<double> dinv;       // nblk*TSZ: inverse of the diagonal U tiles
   DBuf<double> hbi;        // nel*next*nint  (hbi hii^-1, row-major next x nint)
-  DBuf<double> hii;        // nel*nint*nint  (hii^-1, row-major)
+  DBuf<double> hii;        // nel*nint*nint  (hii^-1, column-major)
   DBuf<float> hbif, hiif;  // FP32 copies for the mixed form
   DBuf<double> pc;         // npts: inverse Jacobi diagonal (JACPCG)
   DBuf<float> pcf;         // FP32 copy

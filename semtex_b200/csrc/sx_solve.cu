@@ -54,56 +54,97 @@ __global__ void k_essential(MeshView M, const Job *__restrict__ jobs) {
 // Element forcing and condensation
 // ---------------------------------------------------------------------------
 
+// One block of ELEM_WARPS warps per (element, job); both planes of the job in
+// one pass, so the element's hbi block is read once per job.  Warp w owns
+// rows b = w, w + ELEM_WARPS, ... of hbi (hbi hii^-1), its lanes the row's
+// NI columns: the whole block is loaded into registers, coalesced and
+// evict-first (it is not read again before the band sweeps have streamed
+// the factor through L2), before anything else, so that it arrives while
+// the forcing and the element operator are computed.  The geometric factors
+// of the operator are read only for elements that hold essential nodes.
+constexpr int ELEM_WARPS = 4;
+
 template <int NP>
-__global__ void __launch_bounds__(128) k_rhs_elem(MeshView M, const Job *__restrict__ jobs) {
+__global__ void __launch_bounds__(ELEM_WARPS * 32) k_rhs_elem(MeshView M, const Job *__restrict__ jobs) {
   constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
+  constexpr int NT = ELEM_WARPS * 32, RW = (NE + ELEM_WARPS - 1) / ELEM_WARPS, QL = (NI + 31) / 32;
   const Job J = jobs[blockIdx.y];
-  const int e = blockIdx.x, tid = threadIdx.x;
-  __shared__ double D[NN], Q[5][NN], u[NN], R[NN], S[NN], F[NN], Fe[NN];
-  __shared__ double hb[NE * (NI > 0 ? NI : 1)];
+  const int e = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int P = J.P;
+  const double *hbi = J.hbi + (size_t)e * NE * NI;
+  double h[RW][QL];
+#pragma unroll
+  for (int k = 0; k < RW; k++)
+#pragma unroll
+    for (int j = 0; j < QL; j++) {
+      const int b = w + ELEM_WARPS * k, q = lane + 32 * j;
+      h[k][j] = (b < NE && q < NI) ? __ldcs(hbi + b * NI + q) : 0.0;
+    }
+  __shared__ double F[2][NN], Fe[2][NN];
+  __shared__ double D[NN], Q[4][NN], u[NN], R[NN], S[NN], T[NN];
   __shared__ int emap[NN];
   const size_t eo = (size_t)e * NN;
-  for (int i = tid; i < NN; i += 128) {
-    D[i] = M.D[i];
-    Q[0][i] = M.Q1[eo + i];
-    Q[1][i] = M.Q2[eo + i];
-    Q[2][i] = M.Q3[eo + i];
-    Q[3][i] = M.Q4[eo + i];
-    Q[4][i] = M.Q8[eo + i];
+  const bool masked = M.emask[e] != 0;
+  for (int i = tid; i < NN; i += NT) {
     emap[i] = M.emap[i];
+    const double q8 = M.Q8[eo + i];
+    for (int p = 0; p < P; p++) F[p][i] = q8 * J.f[(size_t)p * J.fstride + eo + i];
   }
-  const double *hbi = J.hbi + (size_t)e * NE * NI;
-  for (int i = tid; i < NE * NI; i += 128) hb[i] = hbi[i];
-  const bool q3 = M.hasQ3[e], masked = M.emask[e] != 0;
-  const int *bt = M.btog + (size_t)e * NE;
-  __syncthreads();
-  for (int p = 0; p < J.P; p++) {
-    double *f = J.f + (size_t)p * J.fstride + eo;
-    for (int i = tid; i < NN; i += 128) F[i] = Q[4][i] * f[i];
-    if (masked) {
+  if (masked) {
+    // f <- M f + H g: the operator applied to the element's essential values
+    for (int i = tid; i < NN; i += NT) {
+      D[i] = M.D[i];
+      Q[0][i] = M.Q1[eo + i];
+      Q[1][i] = M.Q2[eo + i];
+      Q[2][i] = M.Q3[eo + i];
+      Q[3][i] = M.Q4[eo + i];
+    }
+    const bool q3 = M.hasQ3[e];
+    const int *bt = M.btog + (size_t)e * NE;
+    for (int p = 0; p < P; p++) {
       const double *g = J.gess + (size_t)p * M.nglobal;
-      for (int i = tid; i < NN; i += 128) u[i] = 0.0;
       __syncthreads();
-      for (int i = tid; i < NE; i += 128) u[emap[i]] = g[bt[i]];
+      for (int i = tid; i < NN; i += NT) u[i] = 0.0;
       __syncthreads();
-      helm_op<NP, double>(D, Q[0], Q[1], Q[2], Q[3], q3, J.hCon, u, R, S, Fe, 128);
-      for (int i = tid; i < NN; i += 128) F[i] += Fe[i];
+      for (int i = tid; i < NE; i += NT) u[emap[i]] = g[bt[i]];
+      __syncthreads();
+      helm_op<NP, double>(D, Q[0], Q[1], Q[2], Q[3], q3, J.hCon, u, R, S, T, NT);
+      for (int i = tid; i < NN; i += NT) F[p][i] += T[i];
     }
-    __syncthreads();
-    for (int a = tid; a < NN; a += 128) Fe[a] = -F[emap[a]];
-    __syncthreads();
-    double *fb = J.Fb + ((size_t)p * M.nel + e) * NE;
-    for (int b = tid; b < NE; b += 128) {
-      double s = 0.0;
-#pragma unroll 7
-      for (int q = 0; q < NI; q++) s += hb[b * NI + q] * Fe[NE + q];
-      const double v = Fe[b] - s;
-      fb[b] = v;
-      f[b] = v;
-    }
-    for (int i = NE + tid; i < NN; i += 128) f[i] = Fe[i];
-    __syncthreads();
   }
+  __syncthreads();
+  // boundary-first element ordering, negated: f <- -(M f + H g)
+  for (int a = tid; a < NN; a += NT)
+    for (int p = 0; p < P; p++) Fe[p][a] = -F[p][emap[a]];
+  __syncthreads();
+  // F_b -= (hbi hii^-1) F_i: row b of the block against the interior values
+#pragma unroll
+  for (int k = 0; k < RW; k++) {
+    const int b = w + ELEM_WARPS * k;
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int j = 0; j < QL; j++) {
+      const int q = lane + 32 * j;
+      if (q < NI) {
+        s0 += h[k][j] * Fe[0][NE + q];
+        if (P > 1) s1 += h[k][j] * Fe[1][NE + q];
+      }
+    }
+    s0 = warp_sum(s0);
+    if (P > 1) s1 = warp_sum(s1);
+    if (lane == 0 && b < NE) {
+      const double v0 = Fe[0][b] - s0;
+      J.Fb[(size_t)e * NE + b] = v0;
+      J.f[eo + b] = v0;
+      if (P > 1) {
+        const double v1 = Fe[1][b] - s1;
+        J.Fb[((size_t)M.nel + e) * NE + b] = v1;
+        J.f[(size_t)J.fstride + eo + b] = v1;
+      }
+    }
+  }
+  for (int i = NE + tid; i < NN; i += NT)
+    for (int p = 0; p < P; p++) J.f[(size_t)p * J.fstride + eo + i] = Fe[p][i];
 }
 
 // ---------------------------------------------------------------------------
@@ -138,48 +179,71 @@ __global__ void k_rhs_dss(MeshView M, const Job *__restrict__ jobs) {
 // Interior back-substitution + essential values
 // ---------------------------------------------------------------------------
 
+// Threads of k_backsub: one per interior row, rounded up to whole warps.
 template <int NP>
-__global__ void __launch_bounds__(128) k_backsub(MeshView M, const Job *__restrict__ jobs) {
-  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
+__host__ __device__ constexpr int back_threads() {
+  return ((NP * NP - 4 * (NP - 1) + 31) / 32) * 32;
+}
+
+// One block per (element, job), both planes in one pass.  Thread r owns
+// interior row r: u_i[r] = sum_c hii^-1[r][c] F_i[c] - sum_b (hbi hii^-1)[b][r] u_b[b].
+// hii^-1 is stored column-major, so that for each c the block reads one
+// contiguous column (lanes along r), as it reads the rows of hbi hii^-1:
+// the element's 8 (NI + NE) NI bytes stream once from HBM, coalesced and
+// evict-first, straight into the FMA chains; nothing is staged in shared
+// memory but the two right-hand vectors, so many blocks share an SM and
+// keep enough loads in flight.
+template <int NP>
+__global__ void __launch_bounds__(back_threads<NP>()) k_backsub(MeshView M, const Job *__restrict__ jobs) {
+  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE, NT = back_threads<NP>();
   const Job J = jobs[blockIdx.y];
   const int e = blockIdx.x, tid = threadIdx.x;
-  extern __shared__ __align__(16) double smk[];
-  double *hii = smk, *hb = hii + NI * NI;
-  __shared__ double ub[NE], fi[NI > 0 ? NI : 1];
-  __shared__ int emap[NN], bt[NE], bm[NE];
-  const double *gi = J.hii + (size_t)e * NI * NI;
-  for (int i = tid; i < NI * NI; i += 128) hii[i] = gi[i];
-  const double *gb = J.hbi + (size_t)e * NE * NI;
-  for (int i = tid; i < NE * NI; i += 128) hb[i] = gb[i];
-  for (int i = tid; i < NN; i += 128) emap[i] = M.emap[i];
-  for (int i = tid; i < NE; i += 128) {
-    bt[i] = M.btog[(size_t)e * NE + i];
-    bm[i] = M.bmask[(size_t)e * NE + i];
-  }
-  const bool masked = M.emask[e] != 0;
+  const int P = J.P;
+  __shared__ double ub[2][NE], fi[2][NI];
   const size_t eo = (size_t)e * NN;
+  const int *bt = M.btog + (size_t)e * NE;
+  for (int b = tid; b < NE; b += NT) {
+    const int g = bt[b];
+    for (int p = 0; p < P; p++) ub[p][b] = (g < J.nsolve) ? J.rhs[(size_t)p * J.rhs_stride + g] : 0.0;
+  }
+  for (int i = tid; i < NI; i += NT)
+    for (int p = 0; p < P; p++) fi[p][i] = J.f[(size_t)p * J.fstride + eo + NE + i];
   __syncthreads();
-  for (int p = 0; p < J.P; p++) {
-    const double *rhs = J.rhs + (size_t)p * J.rhs_stride;
-    const double *f = J.f + (size_t)p * J.fstride + eo;
-    double *u = J.u + (size_t)p * J.ustride + eo;
-    for (int b = tid; b < NE; b += 128) ub[b] = (bt[b] < J.nsolve) ? rhs[bt[b]] : 0.0;
-    for (int i = tid; i < NI; i += 128) fi[i] = f[NE + i];
-    __syncthreads();
-    for (int b = tid; b < NE; b += 128) u[emap[b]] = ub[b];
-    for (int r = tid; r < NI; r += 128) {
-      double s = 0.0;
-      for (int c = 0; c < NI; c++) s += hii[r * NI + c] * fi[c];
-      double t = 0.0;
-      for (int b = 0; b < NE; b++) t += hb[b * NI + r] * ub[b];
-      u[emap[NE + r]] = s - t;
+  // boundary values: the solved ones, then setEssential on masked nodes
+  const bool masked = M.emask[e] != 0;
+  for (int b = tid; b < NE; b += NT) {
+    const int n = M.emap[b];
+    const bool ess = masked && M.bmask[(size_t)e * NE + b];
+    for (int p = 0; p < P; p++)
+      J.u[(size_t)p * J.ustride + eo + n] = ess ? J.gess[(size_t)p * M.nglobal + bt[b]] : ub[p][b];
+  }
+  if (tid < NI) {
+    const int r = tid;
+    const double *hc = J.hii + (size_t)e * NI * NI + r;
+    const double *hb = J.hbi + (size_t)e * NE * NI + r;
+    double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
+    if (P > 1) {
+#pragma unroll 9
+      for (int c = 0; c < NI; c++) {
+        const double v = __ldcs(hc + c * NI);
+        s0 += v * fi[0][c];
+        s1 += v * fi[1][c];
+      }
+#pragma unroll 8
+      for (int b = 0; b < NE; b++) {
+        const double v = __ldcs(hb + b * NI);
+        t0 += v * ub[0][b];
+        t1 += v * ub[1][b];
+      }
+    } else {
+#pragma unroll 9
+      for (int c = 0; c < NI; c++) s0 += __ldcs(hc + c * NI) * fi[0][c];
+#pragma unroll 8
+      for (int b = 0; b < NE; b++) t0 += __ldcs(hb + b * NI) * ub[0][b];
     }
-    if (masked) {
-      const double *g = J.gess + (size_t)p * M.nglobal;
-      for (int b = tid; b < NE; b += 128)
-        if (bm[b]) u[emap[b]] = g[bt[b]];
-    }
-    __syncthreads();
+    const int n = M.emap[NE + r];
+    J.u[eo + n] = s0 - t0;
+    if (P > 1) J.u[(size_t)J.ustride + eo + n] = s1 - t1;
   }
 }
 
@@ -189,22 +253,11 @@ __global__ void __launch_bounds__(128) k_backsub(MeshView M, const Job *__restri
 
 template <int NP>
 static void launch_elem(const MeshView &M, const Job *djobs, int njobs, bool rhs, cudaStream_t st) {
-  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
   dim3 grid(M.nel, njobs);
-  if (rhs) {
-    k_rhs_elem<NP><<<grid, 128, 0, st>>>(M, djobs);
-  } else {
-    const size_t sm = sizeof(double) * (NI * NI + NE * NI);
-    k_backsub<NP><<<grid, 128, sm, st>>>(M, djobs);
-  }
-}
-
-template <int NP>
-static int prepare_np() {
-  constexpr int NN = NP * NP, NE = 4 * (NP - 1), NI = NN - NE;
-  const size_t sm = sizeof(double) * (NI * NI + NE * NI);
-  SX_CUDA(cudaFuncSetAttribute(k_backsub<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  return SX_OK;
+  if (rhs)
+    k_rhs_elem<NP><<<grid, ELEM_WARPS * 32, 0, st>>>(M, djobs);
+  else
+    k_backsub<NP><<<grid, back_threads<NP>(), 0, st>>>(M, djobs);
 }
 
 static void dispatch_elem(const MeshView &M, const Job *djobs, int njobs, bool rhs, cudaStream_t st) {
@@ -219,14 +272,7 @@ static void dispatch_elem(const MeshView &M, const Job *djobs, int njobs, bool r
 }
 
 int prepare_direct_kernels(const MeshView &M) {
-  switch (M.np) {
-#define SX_CASE(n) \
-  case n: SX_TRY(prepare_np<n>()); break;
-    SX_CASE(3) SX_CASE(4) SX_CASE(5) SX_CASE(6) SX_CASE(7) SX_CASE(8) SX_CASE(9) SX_CASE(10)
-    SX_CASE(11) SX_CASE(12)
-#undef SX_CASE
-    default: return SX_ERR_UNSUPPORTED;
-  }
+  if (M.np < 3 || M.np > 12) return SX_ERR_UNSUPPORTED;
   return prepare_band_kernels();
 }
 
