@@ -796,7 +796,7 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
     const unsigned live = __ballot_sync(0xffffffffu, real_plane(P, p) && (an != 0.0 || bn != 0.0));
     if (lane == 0) V.skip[y] = live == 0u;
   }
-  if (threadIdx.x == 0) bulk_wait_all();  // the stores read shared memory
+  if (threadIdx.x == 0) bulk_wait_read_all();  // the stores have read shared memory
 }
 
 template <int NP>

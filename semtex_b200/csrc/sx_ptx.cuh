@@ -78,9 +78,12 @@ __device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t by
 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
-// Wait until every bulk group this thread committed has completed (global
-// writes done, shared-memory sources free).
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Wait until every committed bulk store has read its shared-memory source;
+// the writes to global memory may still be in flight (they are performed by
+// the time the grid completes), so the block may exit or reuse the buffers.
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
 
 // Make this thread's generic-proxy shared-memory writes visible to the async
 // proxy (TMA) before a bulk store reads them.
