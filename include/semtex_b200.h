@@ -208,9 +208,9 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
  *                         Cholesky, when the mode is factored), 1 = FP32 CG
  *                         for every mode, 2 = band Cholesky for every
  *                         factored mode
- *   SX_TUNE_BAND_STAGES   band-sweep tiles in flight per CTA, 2..4 (auto:
- *                         4, or 2 when that lets a larger cluster stay
- *                         resident -- two CTAs then share an SM)          */
+ *   SX_TUNE_BAND_STAGES   band-sweep tiles in flight per CTA, 1..4 (auto:
+ *                         4, or 2 or 1 when that lets a larger cluster
+ *                         stay resident -- two CTAs then share an SM)     */
 enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3, SX_TUNE_BAND_STAGES = 4 };
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 

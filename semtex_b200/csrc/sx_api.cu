@@ -240,7 +240,7 @@ extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
       s->mixed_route = value;
       return SX_OK;
     case SX_TUNE_BAND_STAGES:
-      if (value == 1 || value > BAND_STAGES_MAX) return SX_ERR_ARG;
+      if (value < 0 || value > BAND_STAGES_MAX) return SX_ERR_ARG;
       s->forced_stages = value > 0 ? value : 0;
       s->cluster_for.clear();
       s->fp64.reset();
@@ -636,7 +636,7 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   std::vector<std::pair<int, int>> clusters;  // (cluster size, ring depth)
   std::vector<int> inners;
   if (band)
-    for (int S : {BAND_STAGES_MAX, 2})
+    for (int S : {BAND_STAGES_MAX, 2, 1})
       for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
         if (C <= J && band_active_clusters(C, 2, J + 2, S) > 0) clusters.push_back(std::make_pair(C, S));
   if (clusters.empty()) clusters.push_back(std::make_pair(0, 0));

@@ -294,8 +294,8 @@ int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cuda
   if (maxP > 8) return SX_ERR_UNSUPPORTED;
   const int pmax = maxP <= 2 ? 2 : 8;
   const int limit = smem_optin();
-  int S = std::max(2, std::min(smax, BAND_STAGES_MAX));
-  while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)limit) S--;
+  int S = std::max(1, std::min(smax, BAND_STAGES_MAX));
+  while (S > 1 && sweep_smem(pmax, C, S, Wmax) > (size_t)limit) S--;
   const size_t sm = sweep_smem(pmax, C, S, Wmax);
   if (sm > (size_t)limit) {
     set_error("band sweep needs %zu B of shared memory (limit %d)", sm, limit);
@@ -332,8 +332,8 @@ int prepare_band_kernels() {
 // Largest cluster size (<= cmax) for which `nj` clusters can be resident at
 // once; at least 1.
 int band_active_clusters(int C, int pmax, int Wmax, int smax) {
-  int S = std::max(2, std::min(smax, BAND_STAGES_MAX));
-  while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
+  int S = std::max(1, std::min(smax, BAND_STAGES_MAX));
+  while (S > 1 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
   if (sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) return 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C, 1, 1);
@@ -357,16 +357,23 @@ int band_active_clusters(int C, int pmax, int Wmax, int smax) {
 }
 
 // Largest cluster size C <= cmax (and ring depth) for which all nj clusters
-// are resident at once, over the ring depths 4 and 2 (a shallower ring
-// halves a CTA's shared memory, so that two fit an SM); the deeper ring on
-// a tie.  stages_forced > 0 fixes the depth.
+// are resident at once, over the ring depths 4, 2 and 1 (a shallower ring
+// shrinks a CTA's shared memory, so that two share an SM); the deeper ring
+// on a tie.  Depth 1 puts the leader's load of D_k on each block column's
+// critical path: it pays where the deeper rings leave at most 2 CTAs per
+// system (many large systems, one CTA per SM, throughput-bound) and lets
+// twice as many stay resident, and is slower where a system's block-column
+// chain is the bound (measured: 64 systems with a 37-tile band, 80.5 ->
+// 57.9 ms at 4 CTAs; 32 systems with a 17-tile band, 2.9 -> 3.1 ms at 8).
+// stages_forced > 0 fixes the depth.
 int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out, int stages_forced) {
   int bestC = 1, bestS = BAND_STAGES_MAX;
-  for (int S0 : {BAND_STAGES_MAX, 2}) {
+  for (int S0 : {BAND_STAGES_MAX, 2, 1}) {
     if (stages_forced > 0 && S0 != stages_forced) continue;
+    if (S0 == 1 && stages_forced != 1 && bestC > 2) continue;
     for (int C = 1; C <= cmax; C++) {
       int S = S0;
-      while (S > 2 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
+      while (S > 1 && sweep_smem(pmax, C, S, Wmax) > (size_t)smem_optin()) S--;
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(C * nj, 1, 1);
       cfg.blockDim = dim3(256, 1, 1);

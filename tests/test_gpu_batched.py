@@ -64,7 +64,8 @@ def _run_device(torch, S, w, batched=True, precision=0, tol=1e-12, bc=None):
     return u.cpu().numpy(), st
 
 
-@pytest.mark.parametrize("cluster,stages", [(0, 0), (1, 0), (2, 0), (3, 0), (5, 0), (2, 2), (5, 2), (3, 3)])
+@pytest.mark.parametrize("cluster,stages", [(0, 0), (1, 0), (2, 0), (3, 0), (5, 0), (2, 2), (5, 2), (3, 3), (1, 1),
+                                            (4, 1)])
 def test_batched_fp64_equals_plain(sx, torch, cluster, stages):
     """Every band-sweep cluster size and ring depth (tiles in flight per
     CTA) gives the plain form's answer to rounding."""
@@ -184,7 +185,7 @@ def test_autotune_keeps_results(sx, torch):
     u = torch.zeros_like(f)
     r64 = S.autotune(u.data_ptr(), f.data_ptr(), 0, w.nz, w.mesh.nplane, sx.FP64)
     assert r64["trials"] >= 1 and r64["band_cluster"] >= 1 and r64["ms"] > 0.0
-    assert r64["band_stages"] in (2, 3, 4)
+    assert r64["band_stages"] in (1, 2, 3, 4)
     assert np.array_equal(f.cpu().numpy(), w.forcing)
     ub2, _ = _run_device(torch, S, w, batched=True)
     sp = solved_planes(w.nz)
