@@ -12,10 +12,12 @@
 // own the older tiles j >= 2 round-robin, so they run ahead while the
 // leader finishes the previous block.  Tiles stream into each CTA through a
 // ring of 1-D TMA bulk copies (cp.async.bulk + mbarrier complete_tx).
-// Partial sums go to the leader, and each solved block goes back to every
-// rank's ring of recent blocks, over distributed shared memory with
-// mbarrier release/acquire at cluster scope.  Partials are combined in rank
-// order, so the result does not depend on timing.
+// Partial sums go to the leader over distributed shared memory; each solved
+// block goes to the RHS array in global memory (where it stays in L2), and
+// the leader's release at cluster scope on every rank's mbarrier for that
+// block lets the ranks fetch it from there (cp.async through L2, one block
+// per tile, issued under the previous tile's work).  Partials are combined
+// in rank order, so the result does not depend on timing.
 //
 // Every wait is bounded (clock64); on timeout the kernel records
 // SX_ERR_TIMEOUT in the status word, drains its own bulk copies (bounded),
@@ -73,8 +75,8 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
   const int P = Jb.P, nblk = Jb.nblk, W = Jb.J + 2;
   extern __shared__ __align__(128) unsigned char smraw[];
   double *ring = reinterpret_cast<double *>(smraw);      // S * TSZ
-  double *ybuf = ring + (size_t)S * TSZ;                 // Wmax * PMAX * NB
-  double *pbuf = ybuf + (size_t)Wmax * PMAX * NB;        // 2 * (C-1) * PMAX * NB
+  double *ysl = ring + (size_t)S * TSZ;                  // 2 * PMAX * NB: y of this tile and the next
+  double *pbuf = ysl + (size_t)2 * PMAX * NB;            // 2 * (C-1) * PMAX * NB
   double *qpart = pbuf + (size_t)2 * max(C - 1, 1) * PMAX * NB;  // 4 * PMAX * NB
   double *acc = qpart + 4 * PMAX * NB;                   // PMAX * NB
   double *yk = acc + PMAX * NB;                          // PMAX * NB
@@ -118,6 +120,24 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
   };
   if (tid == 0) produce(S);
 
+  // The block a tile (t, j >= 2) multiplies -- the one solved at step
+  // t - j -- from the RHS array into ysl[b]: every thread waits (bounded) for
+  // the leader's release of it (a rank of a larger cluster), then threads
+  // tid < P NB / 2 copy one 16-byte chunk each through L2.  False if the wait
+  // ran out (nothing is copied then).
+  auto fetch_y = [&](int t, int j, int b) -> bool {
+    const int src = t - j;
+    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) return false;
+    if (tid < P * (NB / 2)) {
+      const int p = tid / (NB / 2), ch = tid - p * (NB / 2);
+      const int blk = src < nblk ? src : 2 * nblk - 1 - src;
+      cp_async16_cg(ysl + ((size_t)b * PMAX + p) * NB + 2 * ch,
+                    Jb.rhs + (size_t)p * Jb.rhs_stride + (size_t)blk * NB + 2 * ch);
+    }
+    cp_async_commit();
+    return true;
+  };
+
   for (int t = 0; t < T; t++) {
     const bool fwd = t < nblk;
     const int k = fwd ? t : 2 * nblk - 1 - t;
@@ -126,18 +146,25 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
 #pragma unroll
     for (int p = 0; p < PMAX; p++) s[p] = 0.0;
     bool bad = false;
+    // the step's first tile's block; each later one is fetched under the
+    // work of the tile before it (j = 1 uses the leader's own yk, D_k none)
+    int jn = n > 0 ? G.jat(t, 0) : 0;
+    if (jn >= 2 && !fetch_y(t, jn, 0)) bad = true;
     for (int idx = 0; idx < n; idx++) {
-      const int j = G.jat(t, idx);
+      const int j = jn;
       if (j == 0) break;  // D_k: handled below by the leader
       const int slot = (int)(ncons % S);
       if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), WAIT_LIMIT)) bad = true;
-      const int src = t - j, w = src % W;
-      if (rank != 0 && !mbar_wait(&ybar[w], (uint32_t)((src / W) & 1), WAIT_LIMIT)) bad = true;
+      cp_async_wait_all();  // this thread's chunks of the tile's block
       if (bad) abort_flag = 1;
       __syncthreads();
       if (abort_flag) break;
+      jn = idx + 1 < n ? G.jat(t, idx + 1) : 0;
+      // ysl[(idx + 1) & 1] was last read by tile idx - 1, before the barrier
+      // that ended it; a failed wait is seen after this tile's barrier
+      if (jn >= 2 && !fetch_y(t, jn, (idx + 1) & 1)) abort_flag = 1;
       const double *Tt = ring + (size_t)slot * TSZ;
-      const double *yv = ybuf + (size_t)w * PMAX * NB;
+      const double *yv = j == 1 ? yk : ysl + (size_t)(idx & 1) * PMAX * NB;
       if (fwd) {
 #pragma unroll 4
         for (int rr = q * 16; rr < q * 16 + 16; rr++) {
@@ -232,24 +259,16 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
         yk[p * NB + c] = v;
         Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] = v;
       }
-    __syncthreads();
-    // broadcast block t into slot t % W of every rank's ring
-    const int w = t % W;
-    const int tot = C * P * NB;
-    for (int i = tid; i < tot; i += 256) {
-      const int r = i / (P * NB), rem = i - r * P * NB, p = rem / NB, cc = rem - p * NB;
-      double *dst = ybuf + ((size_t)w * PMAX + p) * NB + cc;
-      if (r == 0)
-        *dst = yk[p * NB + cc];
-      else
-        st_cluster_f64(map_rank(dst, (uint32_t)r), yk[p * NB + cc]);
-    }
+    // block t is in rhs (and yk): release it to every other rank (slot
+    // t % W of their barriers); the fence orders the writers' stores before
+    // the arrivals that follow the barrier
     fence_acq_rel_cluster();
     __syncthreads();
-    if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[w], (uint32_t)tid));
+    if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[t % W], (uint32_t)tid));
   }
 
   if (abort_flag) {
+    cp_async_wait_all();
     if (tid == 0) {
       atomicOr(Jb.status, 1 << SX_ERR_TIMEOUT);
       // drain this CTA's bulk copies still in flight (bounded)
@@ -261,7 +280,7 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
 }
 
 size_t sweep_smem(int pmax, int C, int S, int Wmax) {
-  return sizeof(double) * ((size_t)S * TSZ + (size_t)Wmax * pmax * NB +
+  return sizeof(double) * ((size_t)S * TSZ + (size_t)2 * pmax * NB +
                            (size_t)2 * std::max(C - 1, 1) * pmax * NB + 6 * (size_t)pmax * NB) +
          sizeof(uint64_t) * (S + Wmax + 2);
 }
@@ -360,11 +379,10 @@ int band_active_clusters(int C, int pmax, int Wmax, int smax) {
 // are resident at once, over the ring depths 4, 2 and 1 (a shallower ring
 // shrinks a CTA's shared memory, so that two share an SM); the deeper ring
 // on a tie.  Depth 1 puts the leader's load of D_k on each block column's
-// critical path: it pays where the deeper rings leave at most 2 CTAs per
-// system (many large systems, one CTA per SM, throughput-bound) and lets
-// twice as many stay resident, and is slower where a system's block-column
-// chain is the bound (measured: 64 systems with a 37-tile band, 80.5 ->
-// 57.9 ms at 4 CTAs; 32 systems with a 17-tile band, 2.9 -> 3.1 ms at 8).
+// critical path; it is taken only where the deeper rings leave at most 2
+// CTAs per system resident (measured at 4 CTAs on 64 systems with a 37-tile
+// band: depth 2, two CTAs per SM, 46 ms; depth 1 61 ms; and at 8 CTAs on 32
+// systems with a 17-tile band: depth 2 2.9 ms, depth 1 3.1 ms).
 // stages_forced > 0 fixes the depth.
 int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out, int stages_forced) {
   int bestC = 1, bestS = BAND_STAGES_MAX;

@@ -66,6 +66,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// 16-byte asynchronous copy global -> this CTA's shared memory through L2
+// only (no L1 line that could be stale), in the calling thread's cp.async
+// group.  Both addresses 16-B aligned.
+__device__ __forceinline__ void cp_async16_cg(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until every cp.async group of the calling thread has landed.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // 1-D TMA bulk copy this CTA's shared memory -> global, in the calling
 // thread's bulk group.  dst/src 16-B aligned, bytes a multiple of 16.  The
 // shared-memory source must have been written before a
