@@ -138,6 +138,16 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
     return true;
   };
 
+  // the leader's right-hand side of the next block column, loaded a step
+  // ahead (threads q == 0: column c, each plane); the first backward step's
+  // is the forward sweep's last block, taken from the registers that solve it
+  double bnext[PMAX];
+  if (rank == 0 && q == 0) {
+#pragma unroll
+    for (int p = 0; p < PMAX; p++)
+      if (p < P) bnext[p] = Jb.rhs[(size_t)p * Jb.rhs_stride + c];
+  }
+
   for (int t = 0; t < T; t++) {
     const bool fwd = t < nblk;
     const int k = fwd ? t : 2 * nblk - 1 - t;
@@ -226,11 +236,13 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
     __syncthreads();
     if (abort_flag) break;
     if (q == 0) {
-      for (int p = 0; p < P; p++) {
+#pragma unroll
+      for (int p = 0; p < PMAX; p++) {
+        if (p >= P) continue;
         double v = qpart[(0 * PMAX + p) * NB + c] + qpart[(1 * PMAX + p) * NB + c] +
                    qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
         for (int r = 1; r < C; r++) v += pbuf[((size_t)((t & 1) * (C - 1) + (r - 1)) * PMAX + p) * NB + c];
-        acc[p * NB + c] = Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] - v;
+        acc[p * NB + c] = bnext[p] - v;
       }
     }
     __syncthreads();
@@ -252,13 +264,21 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
     for (int p = 0; p < PMAX; p++)
       if (p < P) qpart[(q * PMAX + p) * NB + c] = s[p];
     __syncthreads();
-    if (q == 0)
-      for (int p = 0; p < P; p++) {
+    if (q == 0) {
+      const int kn = t + 1 < nblk ? t + 1 : 2 * nblk - 2 - t;  // next step's block column
+#pragma unroll
+      for (int p = 0; p < PMAX; p++) {
+        if (p >= P) continue;
         const double v = qpart[(0 * PMAX + p) * NB + c] + qpart[(1 * PMAX + p) * NB + c] +
                          qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
         yk[p * NB + c] = v;
         Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] = v;
+        if (t + 1 == nblk)
+          bnext[p] = v;  // backward from the last block: its y is its right-hand side
+        else if (t + 1 < T)
+          bnext[p] = Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)kn * NB + c];
       }
+    }
     // block t is in rhs (and yk): release it to every other rank (slot
     // t % W of their barriers); the fence orders the writers' stores before
     // the arrivals that follow the barrier
