@@ -280,9 +280,9 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
       }
     }
     // block t is in rhs (and yk): release it to every other rank (slot
-    // t % W of their barriers); the fence orders the writers' stores before
-    // the arrivals that follow the barrier
-    fence_acq_rel_cluster();
+    // t % W of their barriers); the writers' fence orders their stores
+    // before the arrivals that follow the barrier
+    if (q == 0) fence_acq_rel_cluster();
     __syncthreads();
     if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[t % W], (uint32_t)tid));
   }
