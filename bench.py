@@ -429,7 +429,8 @@ def run_ours(args, rank, world):
     if rank == 0 and world == 1:
         line["multi_mesh"] = run_multi()
         line["transform_z"] = run_transform()
-        line["config3_full"] = run_config3_full()
+        if not args.no_config3:
+            line["config3_full"] = run_config3_full()
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu)
     if rank == 0:
@@ -740,6 +741,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip config 3 at full size (121 GB of band factors; keep it out of profiler runs)")
     ap.add_argument("--serve-only", type=int, default=0, metavar="N",
                     help="run only the serving loop on the first N requests of the config-4 stream "
                          "and print its JSON (not a bench line)")
