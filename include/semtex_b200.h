@@ -218,7 +218,7 @@ SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
  * caller's own data for each candidate schedule and keeps the fastest in the
  * modal system, as sx_modal_tune would set it --
  *   the band-sweep cluster size (CTAs sharing one system's tiles; sizes the
- *   SM groups cannot hold are skipped) and ring depth (4 or 2 tiles in
+ *   SM groups cannot hold are skipped) and ring depth (4, 2 or 1 tiles in
  *   flight per CTA), for SX_FP64 and for the modes that SX_MIXED_FP32
  *   routes to the band Cholesky;
  *   the floor on FP32 iterations per refinement round, for SX_MIXED_FP32.
