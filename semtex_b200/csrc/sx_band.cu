@@ -68,8 +68,10 @@ __device__ __forceinline__ const double *tile_src(const Job &Jb, int t, int j) {
   return j ? Jb.tiles + ((size_t)(k + j) * J1 + j) * TSZ : Jb.dinv + (size_t)k * TSZ;
 }
 
+// Two CTAs per SM for up to two planes (128 registers a thread), one for more.
 template <int PMAX>
-__global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ jobs, int C, int S, int Wmax) {
+__global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
+    k_band_sweep(const Job *__restrict__ jobs, int C, int S, int Wmax) {
   const int rank = (int)cluster_ctarank();
   const Job Jb = jobs[blockIdx.x / C];
   const int P = Jb.P, nblk = Jb.nblk, W = Jb.J + 2;
@@ -125,9 +127,7 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
   // the leader's release of it (a rank of a larger cluster), then threads
   // tid < P NB / 2 copy one 16-byte chunk each through L2.  False if the wait
   // ran out (nothing is copied then).
-  auto fetch_y = [&](int t, int j, int b) -> bool {
-    const int src = t - j;
-    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) return false;
+  auto copy_y = [&](int src, int b) {
     if (tid < P * (NB / 2)) {
       const int p = tid / (NB / 2), ch = tid - p * (NB / 2);
       const int blk = src < nblk ? src : 2 * nblk - 1 - src;
@@ -135,8 +135,20 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
                     Jb.rhs + (size_t)p * Jb.rhs_stride + (size_t)blk * NB + 2 * ch);
     }
     cp_async_commit();
+  };
+  auto fetch_y = [&](int t, int j, int b) -> bool {
+    const int src = t - j;
+    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) return false;
+    copy_y(src, b);
     return true;
   };
+  // Tiles that multiply a fetched block alternate between the two halves of
+  // ysl (ytile counts them, the same in every thread).  The next step's
+  // first such block is fetched under the current step's last one when its
+  // release is already visible to this thread (one probe, no wait): each
+  // thread copies its own chunk, so each may decide alone (pre).
+  long long ytile = 0;
+  bool pre = false;
 
   // the leader's right-hand side of the next block column, loaded a step
   // ahead (threads q == 0: column c, each plane); the first backward step's
@@ -159,7 +171,8 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
     // the step's first tile's block; each later one is fetched under the
     // work of the tile before it (j = 1 uses the leader's own yk, D_k none)
     int jn = n > 0 ? G.jat(t, 0) : 0;
-    if (jn >= 2 && !fetch_y(t, jn, 0)) bad = true;
+    if (jn >= 2 && !pre && !fetch_y(t, jn, (int)(ytile & 1))) bad = true;
+    pre = false;
     for (int idx = 0; idx < n; idx++) {
       const int j = jn;
       if (j == 0) break;  // D_k: handled below by the leader
@@ -169,12 +182,21 @@ __global__ void __launch_bounds__(256, 1) k_band_sweep(const Job *__restrict__ j
       if (bad) abort_flag = 1;
       __syncthreads();
       if (abort_flag) break;
+      const double *yv = yk;
+      if (j >= 2) yv = ysl + (size_t)(ytile++ & 1) * PMAX * NB;
       jn = idx + 1 < n ? G.jat(t, idx + 1) : 0;
-      // ysl[(idx + 1) & 1] was last read by tile idx - 1, before the barrier
-      // that ended it; a failed wait is seen after this tile's barrier
-      if (jn >= 2 && !fetch_y(t, jn, (idx + 1) & 1)) abort_flag = 1;
+      // ysl[ytile & 1] was last read two fetched tiles ago, before the
+      // barrier that ended it; a failed wait is seen after this tile's barrier
+      if (jn >= 2) {
+        if (!fetch_y(t, jn, (int)(ytile & 1))) abort_flag = 1;
+      } else if (t + 1 < T) {
+        const int n1 = G.count(t + 1), j1 = n1 > 0 ? G.jat(t + 1, 0) : 0, src = t + 1 - j1;
+        if (j1 >= 2 && (rank == 0 || mbar_test_cluster(&ybar[src % W], (uint32_t)((src / W) & 1)))) {
+          copy_y(src, (int)(ytile & 1));
+          pre = true;
+        }
+      }
       const double *Tt = ring + (size_t)slot * TSZ;
-      const double *yv = j == 1 ? yk : ysl + (size_t)(idx & 1) * PMAX * NB;
       if (fwd) {
 #pragma unroll 4
         for (int rr = q * 16; rr < q * 16 + 16; rr++) {

@@ -47,6 +47,20 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t pa
   return ok != 0;
 }
 
+// One non-blocking probe of the phase with the given parity (acquire at
+// cluster scope when it has completed).
+__device__ __forceinline__ bool mbar_test_cluster(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait on the phase with the given parity; false if it ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit_cycles) {
   if (mbar_try_wait_cluster(bar, parity)) return true;
