@@ -287,7 +287,6 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       if (p < P) qpart[(q * PMAX + p) * NB + c] = s[p];
     __syncthreads();
     if (q == 0) {
-      const int kn = t + 1 < nblk ? t + 1 : 2 * nblk - 2 - t;  // next step's block column
 #pragma unroll
       for (int p = 0; p < PMAX; p++) {
         if (p >= P) continue;
@@ -295,10 +294,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
                          qpart[(2 * PMAX + p) * NB + c] + qpart[(3 * PMAX + p) * NB + c];
         yk[p * NB + c] = v;
         Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)k * NB + c] = v;
-        if (t + 1 == nblk)
-          bnext[p] = v;  // backward from the last block: its y is its right-hand side
-        else if (t + 1 < T)
-          bnext[p] = Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)kn * NB + c];
+        if (t + 1 == nblk) bnext[p] = v;  // backward from the last block: its y is its right-hand side
       }
     }
     // block t is in rhs (and yk): release it to every other rank (slot
@@ -307,6 +303,14 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     if (q == 0) fence_acq_rel_cluster();
     __syncthreads();
     if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[t % W], (uint32_t)tid));
+    // the next step's right-hand side, issued after the fence (which would
+    // wait for it) and used a step later
+    if (q == 0 && t + 1 < T && t + 1 != nblk) {
+      const int kn = t + 1 < nblk ? t + 1 : 2 * nblk - 2 - t;  // next step's block column
+#pragma unroll
+      for (int p = 0; p < PMAX; p++)
+        if (p < P) bnext[p] = Jb.rhs[(size_t)p * Jb.rhs_stride + (size_t)kn * NB + c];
+    }
   }
 
   if (abort_flag) {
