@@ -122,11 +122,8 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   };
   if (tid == 0) produce(S);
 
-  // The block a tile (t, j >= 2) multiplies -- the one solved at step
-  // t - j -- from the RHS array into ysl[b]: every thread waits (bounded) for
-  // the leader's release of it (a rank of a larger cluster), then threads
-  // tid < P NB / 2 copy one 16-byte chunk each through L2.  False if the wait
-  // ran out (nothing is copied then).
+  // Block src (the one solved at step src) from the RHS array into ysl[b]:
+  // threads tid < P NB / 2 copy one 16-byte chunk each through L2.
   auto copy_y = [&](int src, int b) {
     if (tid < P * (NB / 2)) {
       const int p = tid / (NB / 2), ch = tid - p * (NB / 2);
@@ -136,6 +133,9 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     }
     cp_async_commit();
   };
+  // The block a tile (t, j >= 2) multiplies, solved at step t - j: every
+  // thread of a rank waits (bounded) for the leader's release of it, then
+  // copies its chunk.  False if the wait ran out (nothing is copied then).
   auto fetch_y = [&](int t, int j, int b) -> bool {
     const int src = t - j;
     if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) return false;
