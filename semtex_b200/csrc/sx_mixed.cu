@@ -546,9 +546,9 @@ __device__ __forceinline__ float gather_we(const MeshView &M, const float *__res
 constexpr int cg_min_blocks(int np) { return np <= 9 ? 3 : (np <= 11 ? 2 : 1); }
 constexpr long long CG_WAIT_LIMIT = 2000000000LL;  // clock cycles: about a second
 
-// Dynamic shared memory of k_cg: six [NN][32] spans and the [NN][16]
-// preconditioner pairs.
-constexpr size_t cg_smem(int np) { return (size_t)np * np * (6 * MX_CH + 16) * sizeof(float); }
+// Dynamic shared memory of k_cg: six [NN][32] spans, the [NN][16]
+// preconditioner pairs and the element's geometry (one float4 a node).
+constexpr size_t cg_smem(int np) { return (size_t)np * np * ((6 * MX_CH + 16) * sizeof(float) + 16); }
 
 template <int NP>
 __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it, int mode) {
@@ -560,10 +560,14 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   // shared spans, NN * 32 floats each: r, s, p, d (updated in place); B1 =
   // the element's own A u, then the column results (and r on curved
   // elements); B0 = u, then s on curved elements, then the A u to store;
-  // then the preconditioner pairs [NN][16]
+  // then the preconditioner pairs [NN][16], then the geometry (Q1..Q4 of
+  // each node, staged with the spans so that the operator reads no global
+  // memory)
   extern __shared__ __align__(128) float smc[];
   float *Rs = smc, *Ss = Rs + NN * MX_CH, *Ps = Ss + NN * MX_CH, *Ds = Ps + NN * MX_CH;
   float *B1 = Ds + NN * MX_CH, *B0 = B1 + NN * MX_CH, *PCs = B0 + NN * MX_CH;
+  float4 *Gs = reinterpret_cast<float4 *>(PCs + NN * 16);
+  constexpr uint32_t GSPAN = NN * sizeof(float4);
   __shared__ int gtab[NN], emt[NN], tsl[NN];
   __shared__ int4 w4[NE];
   __shared__ __align__(8) uint64_t bar;
@@ -587,10 +591,11 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init_cluster();
-    const uint32_t bytes =
-        PSPAN + (init ? 0u : SPAN) + (!init && !last ? SPAN : 0u) + (warm ? (last ? 2u : 3u) * SPAN : 0u);
+    const uint32_t bytes = PSPAN + (last ? 0u : GSPAN) + (init ? 0u : SPAN) + (!init && !last ? SPAN : 0u) +
+                           (warm ? (last ? 2u : 3u) * SPAN : 0u);
     mbar_arrive_expect_tx(&bar, bytes);
     bulk_g2s(PCs, V.pcE + pbase, PSPAN, &bar);
+    if (!last) bulk_g2s(Gs, M.Gf + (size_t)e * NN, GSPAN, &bar);
     if (!init) bulk_g2s(Rs, V.rE + base, SPAN, &bar);
     if (!init && !last) bulk_g2s(B1, Win + base, SPAN, &bar);
     if (warm) {
@@ -715,7 +720,7 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
       S[j] = s;
     }
   }
-  const float4 *G = M.Gf + (size_t)e * NN;
+  const float4 *G = Gs;
   if (M.hasQ3[e]) {
     // curved: R = Q1 r + Q3 s, S = Q2 s + Q3 r need both at every node
     __syncthreads();  // every warp has its u lines: B0 is free
