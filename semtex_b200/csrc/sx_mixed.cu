@@ -568,7 +568,7 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   float *B1 = Ds + NN * MX_CH, *B0 = B1 + NN * MX_CH, *PCs = B0 + NN * MX_CH;
   float4 *Gs = reinterpret_cast<float4 *>(PCs + NN * 16);
   constexpr uint32_t GSPAN = NN * sizeof(float4);
-  __shared__ int gtab[NN], emt[NN], tsl[NN];
+  __shared__ int gtab[NN], emt[NN];
   __shared__ int4 w4[NE];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int staged;
@@ -607,7 +607,6 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   for (int a = threadIdx.x; a < NN; a += NP * 32) {
     gtab[a] = a < NE ? M.btog[(size_t)e * NE + a] : M.nglobal + e * NI + (a - NE);
     emt[a] = M.emap[a];
-    tsl[a] = M.pmap[a];
     if (a < NE) w4[a] = M.e2w4[(size_t)e * NE + a];
   }
   const double *gam_in = cur ? V.gam[1] : V.gam[0], *alpha_in = cur ? V.alpha[1] : V.alpha[0];
