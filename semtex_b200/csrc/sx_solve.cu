@@ -282,6 +282,11 @@ int direct_rhs_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> 
   int maxpad = 0;
   bool any_bc = false;
   for (const Job &j : hjobs) {
+    // the element kernels take both planes of a mode in one pass, no more
+    if (j.P < 1 || j.P > 2) {
+      set_error("direct solve: a job of %d planes (the element kernels take 1 or 2)", j.P);
+      return SX_ERR_UNSUPPORTED;
+    }
     maxpad = std::max(maxpad, j.npad);
     any_bc |= j.bc != nullptr;
     SX_CUDA(cudaMemsetAsync(j.gess, 0, sizeof(double) * (size_t)j.P * M.nglobal, st));

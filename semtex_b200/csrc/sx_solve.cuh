@@ -6,8 +6,8 @@
 
 namespace sx {
 
-// A set of P planes sharing one system.  Plane p of u / f / bc is at
-// u + p*ustride etc.
+// A set of P planes sharing one system (P = 1 or 2: a Fourier mode's one
+// or two planes).  Plane p of u / f / bc is at u + p*ustride etc.
 struct Job {
   double *u;
   double *f;
