@@ -107,6 +107,15 @@ SX_API const char *sx_status_string(int status);
 SX_API const char *sx_last_error(void);
 /* Device used by subsequent calls from this host thread (cudaSetDevice). */
 SX_API int sx_set_device(int device);
+/* Limit of the bounded device-side waits on the current device (no
+ * reference counterpart): the band sweeps' waits for tiles and for solved
+ * blocks, and the FP32 iterations' wait for their staged copies.  A wait that
+ * runs out records SX_ERR_TIMEOUT, which the entry point (or
+ * sx_modal_status) returns; the kernel still returns normally and the
+ * context stays usable.  ms < 0 restores the defaults (about 2 s for the
+ * sweeps, 1 s for the iterations); ms = 0 makes every such wait give up at
+ * its first unsuccessful probe (to exercise the error path). */
+SX_API int sx_set_wait_limit(double ms);
 
 /* ---- mesh: replaces Element construction + BCmgr numbering ---------------
  * Element::Element / Element::mapping (src/element.cpp:30-100, 1281-1436),
@@ -134,14 +143,14 @@ SX_API int sx_modal_create_ex(sx_mesh mesh, int base_mode, int num_modes, const 
                        const double *betak2, int method, sx_modal *out);
 /* ModalMatrixSys::~ModalMatrixSys, src/matrix.cpp:113-130. */
 SX_API int sx_modal_destroy(sx_modal modal);
-/* Band factor of local mode m, in LAPACK "U" band storage
- * (ldab = nband, veclib/lapack.h:107-108): nsolve*nband doubles. */
 /* Status of the device work enqueued so far on this system: synchronises
  * the device, returns SX_OK or the first recorded device-side error (e.g.
  * SX_ERR_TIMEOUT from a bounded wait) and clears it. */
 SX_API int sx_modal_status(sx_modal modal);
 /* Device memory held by the modal system (factors, element matrices). */
 SX_API unsigned long long sx_modal_device_bytes(sx_modal modal);
+/* Band factor of local mode m, in LAPACK "U" band storage
+ * (ldab = nband, veclib/lapack.h:107-108): nsolve*nband doubles. */
 SX_API int sx_modal_band(sx_modal modal, int m, double *ab, int *nsolve, int *singular);
 
 /* ---- solve: replaces Field::solve (src/field.cpp:509-725) ----------------
@@ -150,7 +159,9 @@ SX_API int sx_modal_band(sx_modal modal, int m, double *ab, int *nsolve, int *si
  *   f   nz planes: forcing, overwritten (as src/field.cpp:525-526)
  *   bc  nz * nbound * np boundary-line values (NULL = all zero)
  * tol_rel / step_max: TOL_REL / STEP_MAX for JACPCG (femlib/defaults.h:29,89).
- * Host pointers; the copies are part of the call. */
+ * Host pointers; the copies are part of the call.  Every solve entry point
+ * returns SX_ERR_ARG when the calling thread's current device is not the
+ * one the mesh was created on (its systems live there). */
 SX_API int sx_field_solve(sx_modal modal, double *u, double *f, const double *bc, int nz,
                    int plane_stride, double tol_rel, int step_max, sx_solve_stats *stats);
 /* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
@@ -172,7 +183,11 @@ SX_API int sx_field_solve_device(sx_modal modal, double *d_u, double *d_f, const
  *     module; make that first call before any stream capture.
  *   - SX_ERR_CAPACITY when one mode needs more than SX_STATIC_SCRATCH_BYTES
  *     (sx_last_error() gives the bytes needed); SX_ERR_UNSUPPORTED when a
- *     mode's system is not DIRECT.
+ *     mode's system is not DIRECT; SX_ERR_ARG when the current device is not
+ *     the mesh's (the array used is the current device's).
+ *   - Each mode's job record is written into the array by a one-thread
+ *     kernel that takes the record as its argument, so no host memory is
+ *     read after the call returns.
  *   - The array is shared by all calls on a device: calls that overlap in
  *     time (two threads or two streams) race on it; serialise them.
  *   - Results equal sx_field_solve_device's bit for bit (same kernels). */

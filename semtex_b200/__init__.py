@@ -11,7 +11,10 @@ the reference's solve interface:
                       overwritten, the solution returned.
 
 The compute path is the compiled CUDA library; there is no CPU fallback.
-If ``libsemtex_b200.so`` is missing or cannot be loaded, import fails.
+If ``libsemtex_b200.so`` is missing, import fails; the library is mapped on
+the first call into it (so that the mesh and workload builders can be used
+without it, e.g. by a CPU-only timing of the oracle), and a library that
+cannot be loaded fails that call.
 """
 from __future__ import annotations
 
@@ -95,10 +98,12 @@ class ServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python -m semtex_b200.build` "
+                      "(no CPU fallback exists)")
+
+
 def _load():
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m semtex_b200.build` "
-                          "(no CPU fallback exists)")
     L = C.CDLL(LIB_PATH)
     vp, ip, dp = C.c_void_p, C.c_int, C.c_double
     P = C.POINTER
@@ -107,6 +112,7 @@ def _load():
     L.sx_status_string.argtypes = [ip]
     L.sx_last_error.restype = C.c_char_p
     L.sx_set_device.argtypes = [ip]
+    L.sx_set_wait_limit.argtypes = [dp]
     L.sx_mesh_create.argtypes = [P(MeshDesc), P(vp)]
     L.sx_mesh_destroy.argtypes = [vp]
     L.sx_mesh_geometry.argtypes = [vp, ip] + [P(dp)] * 5
@@ -140,7 +146,22 @@ def _load():
     return L
 
 
-lib = _load()
+class _Library:
+    """The C ABI, mapped on first use (``lib.sx_*``)."""
+
+    _handle = None
+
+    def __getattr__(self, name):
+        if _Library._handle is None:
+            _Library._handle = _load()
+        return getattr(_Library._handle, name)
+
+    @property
+    def loaded(self):
+        return _Library._handle is not None
+
+
+lib = _Library()
 
 
 def status_string(s):

@@ -86,6 +86,19 @@ extern "C" int sx_set_device(int device) {
   return SX_OK;
 }
 
+extern "C" int sx_set_wait_limit(double ms) {
+  long long sweep = SWEEP_WAIT_DEFAULT, cg = CG_WAIT_DEFAULT;
+  if (ms >= 0.0) {
+    int dev = 0, khz = 0;
+    SX_CUDA(cudaGetDevice(&dev));
+    SX_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+    sweep = cg = (long long)(ms * (double)khz);  // clock64 counts SM cycles
+  }
+  SX_TRY(set_sweep_wait_limit(sweep));
+  SX_TRY(set_cg_wait_limit(cg));
+  return SX_OK;
+}
+
 static bool same_constants(const System &S, double lambda2, double betak2, int method) {
   // MatrixSys::match, src/matrix.cpp:326-347 (same mesh numbering implied).
   return std::fabs(S.lambda2 - lambda2) < EPSDP && std::fabs(S.betak2 - betak2) < EPSDP &&
@@ -338,6 +351,7 @@ extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const
                                      int plane_stride, double tol_rel, int step_max, void *stream,
                                      sx_solve_stats *stats) {
   if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
+  SX_TRY(check_mesh_device(*s->mesh, "sx_field_solve_device"));
   cudaStream_t st = (cudaStream_t)stream;
   std::vector<Group> groups;
   SX_TRY(plane_groups(*s, nz, groups));
@@ -388,6 +402,7 @@ extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const
 extern "C" int sx_field_solve(sx_modal s, double *u, double *f, const double *bc, int nz, int plane_stride,
                               double tol_rel, int step_max, sx_solve_stats *stats) {
   if (!s || !u || !f || nz <= 0) return SX_ERR_ARG;
+  SX_TRY(check_mesh_device(*s->mesh, "sx_field_solve"));
   const size_t n = (size_t)nz * plane_stride;
   const size_t nbc = (size_t)nz * std::max(s->mesh->nbound, 1) * s->mesh->np;
   if (s->hu.n < n) SX_TRY(s->hu.alloc(n));
@@ -604,6 +619,7 @@ extern "C" int sx_field_solve_batched(sx_modal s, double *d_u, double *d_f, cons
                                       void *stream, sx_solve_stats *stats) {
   if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
   if (precision != SX_FP64 && precision != SX_MIXED_FP32) return SX_ERR_ARG;
+  SX_TRY(check_mesh_device(*s->mesh, "sx_field_solve_batched"));
   if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
   cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
   const int rc = solve_batched_on(s, d_u, d_f, d_bc, nz, plane_stride, precision, tol_rel, max_refine, st,
@@ -732,6 +748,7 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
                                            int nz, int plane_stride, int precision, double tol_rel,
                                            int max_refine, sx_solve_stats *stats) {
   if (!s || !u || !f || nz <= 0 || plane_stride <= 0) return SX_ERR_ARG;
+  SX_TRY(check_mesh_device(*s->mesh, "sx_field_solve_batched_host"));
   const size_t n = (size_t)nz * plane_stride;
   const size_t bcp = (size_t)std::max(s->mesh->nbound, 1) * s->mesh->np;  // bc values per plane
   const size_t nbc = (size_t)nz * bcp;
@@ -825,6 +842,16 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
     if (v->dstatus.p) SX_TRY(take_status(v.get(), true, st, false));
   if (stats) *stats = tot;
   return rc;
+}
+
+int sx::check_mesh_device(const sx_mesh_s &M, const char *who) {
+  int dev = -1;
+  SX_CUDA(cudaGetDevice(&dev));
+  if (dev != M.device) {
+    set_error("%s: the current device is %d, but the mesh and its systems live on device %d", who, dev, M.device);
+    return SX_ERR_ARG;
+  }
+  return SX_OK;
 }
 
 int sx::copy_solved_planes(double *h_u, const double *d_u, int nz, int plane_stride, int base_mode,

@@ -30,7 +30,19 @@
 
 namespace sx {
 
-constexpr long long WAIT_LIMIT = 4000000000LL;  // ~2 s at 1.9 GHz
+constexpr long long WAIT_LIMIT = SWEEP_WAIT_DEFAULT;  // ~2 s at 1.9 GHz
+
+// Cycles a wait of the sweep loop may take before the kernel gives up
+// (SX_ERR_TIMEOUT); per device, set by sx_set_wait_limit.  The drain of a
+// CTA's own bulk copies on the way out always uses WAIT_LIMIT: those copies
+// read valid memory and land within microseconds, and a CTA must not leave
+// with copies into its shared memory still in flight.
+__device__ long long g_sweep_wait = WAIT_LIMIT;
+
+int set_sweep_wait_limit(long long cycles) {
+  SX_CUDA(cudaMemcpyToSymbol(g_sweep_wait, &cycles, sizeof(cycles)));
+  return SX_OK;
+}
 
 struct SweepGeom {
   int nblk, J, C, rank;
@@ -89,6 +101,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
 
   const int tid = threadIdx.x, c = tid & (NB - 1), q = tid >> 6;
   const SweepGeom G{nblk, Jb.J, C, rank};
+  const long long lim = g_sweep_wait;
   if (tid == 0) {
     for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
     for (int w = 0; w < Wmax; w++) mbar_init(&ybar[w], 1);
@@ -138,7 +151,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   // copies its chunk.  False if the wait ran out (nothing is copied then).
   auto fetch_y = [&](int t, int j, int b) -> bool {
     const int src = t - j;
-    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) return false;
+    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), lim)) return false;
     copy_y(src, b);
     return true;
   };
@@ -177,7 +190,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       const int j = jn;
       if (j == 0) break;  // D_k: handled below by the leader
       const int slot = (int)(ncons % S);
-      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), WAIT_LIMIT)) bad = true;
+      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), lim)) bad = true;
       cp_async_wait_all();  // this thread's chunks of the tile's block
       if (bad) abort_flag = 1;
       __syncthreads();
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       // t-2; seeing that block means the slot is free again.
       if (t >= 2) {
         const int src = t - 2;
-        if (!mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), WAIT_LIMIT)) abort_flag = 1;
+        if (!mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), lim)) abort_flag = 1;
         __syncthreads();
         if (abort_flag) break;
       }
@@ -249,11 +262,11 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     }
     // ---- leader: combine partials, apply D_k, broadcast ----
     if (C > 1) {
-      if (!mbar_wait(&pbar[t & 1], (uint32_t)((t >> 1) & 1), WAIT_LIMIT)) abort_flag = 1;
+      if (!mbar_wait(&pbar[t & 1], (uint32_t)((t >> 1) & 1), lim)) abort_flag = 1;
     }
     {
       const int slot = (int)(ncons % S);
-      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), WAIT_LIMIT)) abort_flag = 1;
+      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), lim)) abort_flag = 1;
     }
     __syncthreads();
     if (abort_flag) break;

@@ -98,9 +98,13 @@ __global__ void k_elem_condense(MeshView M, double hCon, double *__restrict__ hb
   for (int k = 0; k < nint; k++) {
     const double p = hii[k * nint + k];
     for (int i = tid; i < nint; i += nt) colk[i] = hii[i * nint + k];
-    if (tid == 0 && !(p > 0.0)) bad = 1;
+    // a zero (or NaN) pivot: hii is singular (src/element.cpp:212-216); a
+    // negative one: hii, a principal block of H, is not positive definite,
+    // so neither is H -- the reference's getrf/getri go on with an
+    // indefinite hii and its dpbtrf then fails (src/matrix.cpp:259-261)
+    if (tid == 0) bad |= (p < 0.0) ? 2 : (!(p > 0.0) ? 1 : 0);
     __syncthreads();
-    const double rp = (p > 0.0) ? 1.0 / p : 1.0;
+    const double rp = (p != 0.0 && p == p) ? 1.0 / p : 1.0;
     for (int j = tid; j < nint; j += nt) hii[k * nint + j] = ((j == k) ? 1.0 : hii[k * nint + j]) * rp;
     __syncthreads();
     for (int idx = tid; idx < nint * nint; idx += nt) {
@@ -137,7 +141,8 @@ __global__ void k_elem_condense(MeshView M, double hCon, double *__restrict__ hb
   }
   double *oh = hbb_out + (size_t)e * next * next;
   for (int i = tid; i < next * next; i += nt) oh[i] = hbb[i];
-  if (tid == 0 && bad) atomicOr(status, 1 << SX_ERR_SINGULAR_HII);
+  if (tid == 0 && bad)
+    atomicOr(status, ((bad & 1) ? 1 << SX_ERR_SINGULAR_HII : 0) | ((bad & 2) ? 1 << SX_ERR_NOT_SPD : 0));
 }
 
 // ---------------------------------------------------------------------------
@@ -392,7 +397,7 @@ static int check_status(DBuf<int> &st) {
   int h = 0;
   SX_CUDA(cudaMemcpy(&h, st.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (h & (1 << SX_ERR_SINGULAR_HII)) {
-    set_error("interior matrix hii is not positive definite");
+    set_error("interior matrix hii is singular");
     return SX_ERR_SINGULAR_HII;
   }
   if (h & (1 << SX_ERR_BAND)) {

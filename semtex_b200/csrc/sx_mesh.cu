@@ -305,6 +305,24 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       set_error("btog[%zu] = %d outside [0, nglobal)", i, M->btog[i]);
       return SX_ERR_ARG;
     }
+  // Every pair of solve nodes of an element is coupled in H: their numbers
+  // must lie within the declared band (the reference's assembly,
+  // src/matrix.cpp:236-241, writes band_addr(m, n, nband) unchecked)
+  for (int e = 0; e < nel; e++) {
+    int lo = d->nglobal, hi = -1;
+    for (int i = 0; i < next; i++) {
+      const int g = M->btog[(size_t)e * next + i];
+      if (g < d->nsolve) {
+        lo = std::min(lo, g);
+        hi = std::max(hi, g);
+      }
+    }
+    if (hi >= 0 && hi - lo >= d->nband) {
+      set_error("element %d couples solve nodes %d and %d, further apart than nband - 1 = %d", e, lo, hi,
+                d->nband - 1);
+      return SX_ERR_BAND;
+    }
+  }
   M->emask.assign(nel, 0);
   for (int e = 0; e < nel; e++)
     for (int i = 0; i < next; i++) M->emask[e] |= M->bmask[(size_t)e * next + i] != 0;

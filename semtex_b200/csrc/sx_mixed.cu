@@ -544,7 +544,18 @@ __device__ __forceinline__ float gather_we(const MeshView &M, const float *__res
 // Resident blocks per SM that the register budget is set for (shared memory
 // allows 3 at np <= 9 and 2 at np <= 11).
 constexpr int cg_min_blocks(int np) { return np <= 9 ? 3 : (np <= 11 ? 2 : 1); }
-constexpr long long CG_WAIT_LIMIT = 2000000000LL;  // clock cycles: about a second
+constexpr long long CG_WAIT_LIMIT = CG_WAIT_DEFAULT;  // clock cycles: about a second
+
+// Cycles the first wait for a block's staged spans may take before the
+// block records SX_ERR_TIMEOUT; per device, set by sx_set_wait_limit.  The
+// block then waits again with CG_WAIT_LIMIT for its copies to land (they
+// read valid memory), so it never leaves with copies in flight.
+__device__ long long g_cg_wait = CG_WAIT_LIMIT;
+
+int set_cg_wait_limit(long long cycles) {
+  SX_CUDA(cudaMemcpyToSymbol(g_cg_wait, &cycles, sizeof(cycles)));
+  return SX_OK;
+}
 
 // Dynamic shared memory of k_cg: six [NN][32] spans, the [NN][16]
 // preconditioner pairs and the element's geometry (one float4 a node).
@@ -638,7 +649,7 @@ __device__ __forceinline__ void cg_body(const MxMember &B, int e, int y, int it,
   // the staged spans: thread 0 waits (bounded) and tells the block; the
   // others then pass the completed phase, which orders the TMA writes for them
   if (threadIdx.x == 0) {
-    bool ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);
+    bool ok = mbar_wait(&bar, 0, g_cg_wait);
     if (!ok) {
       atomicOr(V.status, 1 << SX_ERR_TIMEOUT);
       ok = mbar_wait(&bar, 0, CG_WAIT_LIMIT);  // let the copies land before leaving

@@ -119,6 +119,10 @@ int modal_populate(sx_modal_s &M, const double *lam, const double *bk2, const Sy
 int solve_batched_on(sx_modal_s *s, double *d_u, double *d_f, const double *d_bc, int nz, int plane_stride,
                      int precision, double tol_rel, int max_refine, cudaStream_t st, sx_solve_stats *stats);
 
+// SX_ERR_ARG (with a message naming `who`) unless the current device is the
+// one the mesh -- and so every system built on it -- lives on.
+int check_mesh_device(const sx_mesh_s &M, const char *who);
+
 // Device -> host copy of the solved planes of a field (plane_stride doubles
 // a plane).  The Nyquist plane (plane 1 when the base mode is 0 and nz > 1)
 // is not solved and not copied: the caller's host plane stays as it was, as

@@ -62,7 +62,10 @@ __device__ __forceinline__ bool mbar_test_cluster(uint64_t *bar, uint32_t parity
 }
 
 // Bounded wait on the phase with the given parity; false if it ran out.
+// limit_cycles <= 0: one non-blocking probe (false unless the phase has
+// already completed).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit_cycles) {
+  if (limit_cycles <= 0) return mbar_test_cluster(bar, parity);
   if (mbar_try_wait_cluster(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait_cluster(bar, parity))

@@ -85,6 +85,12 @@ int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_
 int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st,
                     int stages = BAND_STAGES_MAX);
 int prepare_band_kernels();
+// Bounded device-side waits on the current device (sx_set_wait_limit): the
+// band sweeps' and the FP32 iterations' limits in clock cycles (<= 0: one
+// probe).
+constexpr long long SWEEP_WAIT_DEFAULT = 4000000000LL, CG_WAIT_DEFAULT = 2000000000LL;
+int set_sweep_wait_limit(long long cycles);
+int set_cg_wait_limit(long long cycles);
 int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out = nullptr, int stages_forced = 0);
 // Clusters of C band-sweep CTAs that can be resident at once (0: C does not
 // fit an SM group, so a launch with it would fail).

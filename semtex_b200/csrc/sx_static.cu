@@ -70,12 +70,24 @@ PlaneGroup plane_group(int base_mode, int nz, int l) {
   return {l, 2 * l, 2};
 }
 
+// Stores one mode's job record into the scratch array.  The record travels
+// as a kernel argument, which the runtime copies when the launch is
+// enqueued, so the host record can be rewritten for the next mode at once
+// (a pageable host-to-device copy would instead be read whenever the
+// runtime gets to it).
+__global__ void k_put_job(Job *dst, Job j) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = j;
+}
+
 }  // namespace
 
 extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f, const double *d_bc, int nz,
                                             int plane_stride, void *stream, sx_solve_stats *stats) {
   if (!s || !d_u || !d_f || plane_stride < s->mesh->nel * s->mesh->npnp) return SX_ERR_ARG;
   if (nz <= 0 || (nz > 1 && (nz % 2 || nz / 2 > s->num_modes))) return SX_ERR_ARG;
+  // the factors and element matrices live on the mesh's device; the scratch
+  // array is taken on the current one: they must be the same device
+  SX_TRY(check_mesh_device(*s->mesh, "sx_field_solve_device_static"));
   const sx_mesh_s &Mh = *s->mesh;
   const int ngroups = nz == 1 ? 1 : nz / 2;
   // Scratch layout: [one Job][rhs: P * npad][Fb: P * nel * next][gess: P * nglobal],
@@ -112,6 +124,7 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
   const int C = s->cluster(1, &stages);
   const long long bcstride = (long long)std::max(Mh.nbound, 1) * Mh.np;
   // one host Job, reused: the 1-element vector is allocated once per thread
+  // (direct_solve_jobs reads the host copy only while it enqueues)
   thread_local std::vector<Job> one(1);
   sx_solve_stats loc{};
   for (int l = 0; l < ngroups; l++) {
@@ -148,10 +161,11 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
     // direct_solve_jobs clears it with cudaMemsetAsync before k_essential
     // writes the boundary values.  rhs (padding included) and Fb are written
     // in full by k_rhs_dss / k_rhs_elem before anything reads them.
-    SX_CUDA(cudaMemcpyAsync(djob, &j, sizeof(Job), cudaMemcpyHostToDevice, st));
+    k_put_job<<<1, 32, 0, st>>>(djob, j);
+    SX_CUDA(cudaGetLastError());
     int nl = 0;
     SX_TRY(direct_solve_jobs(M, djob, one, st, C, &nl, stages));
-    loc.kernel_launches += nl;
+    loc.kernel_launches += nl + 1;
     loc.planes_solved += g.P;
   }
   SX_CUDA(cudaGetLastError());

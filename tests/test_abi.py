@@ -43,8 +43,60 @@ def test_mesh_numbering_invariants():
     for e in range(m.nel):
         g = m.btog[e][m.bmask[e] == 0]
         assert g.max() - g.min() < m.nband
-    # periodic: x = 0 and x = 2 pi share global nodes
-    assert m.nglobal == 6 * 4 * 4 * 2 + 6 * 4 + 0 - 0 or m.nglobal > 0
+    # periodic: x = 0 and x = 2 pi share global nodes, so every row of
+    # vertices and horizontal edges has nx entries (not nx + 1): vertices
+    # 6 x 5, horizontal edges 6 x 5 and vertical edges 6 x 4 with np - 2 = 3
+    # interior nodes each
+    nx, ny, ni = 6, 4, 3
+    assert m.nglobal == nx * (ny + 1) + nx * (ny + 1) * ni + nx * ny * ni == 192
+    mo = rect_mesh(6, 4, 5, 0, 2 * np.pi, 0, 1, jitter=0.15, seed=2, periodic_x=False,
+                   bc={"bottom": "D", "top": "D"})
+    assert mo.nglobal == m.nglobal + (ny + 1) + ny * ni  # the x = 2 pi column of its own
     ptr, idx = m.global_to_element()
     assert ptr[-1] == m.nel * m.next
     assert (np.diff(ptr) >= 1).all()
+
+
+def _desc(m, **over):
+    import semtex_b200 as sx
+    d, keep = sx.mesh_desc(m)
+    for k, v in over.items():
+        setattr(d, k, v)
+    return d, keep
+
+
+def test_mesh_create_rejects_flipped_element():
+    """A clockwise (mirrored) element has a negative Jacobian: SX_ERR_JACOBIAN,
+    as Element::mapping stops (src/element.cpp:1349-1352).  Found on the host
+    before anything touches a device."""
+    import semtex_b200 as sx
+    from semtex_b200.mesh import rect_mesh
+    m = rect_mesh(3, 2, 5, 0.0, 1.0, 0.0, 1.0)
+    e = 4
+    x = m.x.reshape(m.nel, m.np, m.np).copy()
+    x[e] = x[e][:, ::-1]  # reverse the element's r direction: orientation flips
+    m.x = x.reshape(m.x.shape)
+    d, keep = _desc(m)
+    h = C.c_void_p()
+    st = sx.lib.sx_mesh_create(C.byref(d), C.byref(h))
+    assert st == 4, sx.status_string(st)  # SX_ERR_JACOBIAN
+    assert f"element {e + 1}" in sx.last_error()
+
+
+def test_mesh_create_rejects_band_too_narrow():
+    """A declared band narrower than the numbering's couplings: SX_ERR_BAND
+    (the reference's assembly would write outside its band,
+    src/matrix.cpp:236-241)."""
+    import semtex_b200 as sx
+    from semtex_b200.mesh import rect_mesh
+    m = rect_mesh(4, 4, 5, 0.0, 1.0, 0.0, 1.0)
+    d, keep = _desc(m, nband=m.nband - 1)
+    h = C.c_void_p()
+    st = sx.lib.sx_mesh_create(C.byref(d), C.byref(h))
+    assert st == 7, sx.status_string(st)  # SX_ERR_BAND
+    assert "nband" in sx.last_error()
+    # the declared band itself is accepted up to that point: a band exactly as
+    # wide as the widest element coupling passes the check
+    widest = max(int(g.max() - g.min()) + 1 for g in
+                 (m.btog[e][m.bmask[e] == 0] for e in range(m.nel)) if len(g))
+    assert widest == m.nband

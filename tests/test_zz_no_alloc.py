@@ -1,8 +1,9 @@
 """GPU tests of sx_field_solve_device_static, the direct solve whose scratch is
 a fixed device array (no device allocation in any call).
 
-* Two consecutive calls give bit for bit the result of sx_field_solve_device
-  (same kernels), with and without boundary values.
+* Consecutive calls give bit for bit the result of sx_field_solve_device
+  (same kernels): with and without boundary values, one plane, a block of
+  modes that does not start at mode 0, and on a stream the caller created.
 * The device's free memory is the same before and after those calls.
 * A solve needing more than SX_STATIC_SCRATCH_BYTES per mode is refused
   with SX_ERR_CAPACITY; a JACPCG system with SX_ERR_UNSUPPORTED.
@@ -31,36 +32,59 @@ def torch():
     return torch
 
 
-def _case(sx, with_bc):
+def _case(sx, with_bc, nz=12, base_mode=0):
     from semtex_b200.workloads import small_channel
-    w = small_channel(nx=8, ny=8, np_=9, nz=12, lam=1e6, seed=11)
-    S = sx.ModalMatrixSys(sx.Mesh(w.mesh), num_modes=w.num_modes, method=sx.DIRECT,
-                          lambda2_modes=w.lambda2, betak2_modes=w.betak2)
+    w = small_channel(nx=8, ny=8, np_=9, nz=max(nz, 2), lam=1e6, seed=11)
+    nm = 1 if nz == 1 else nz // 2
+    lam = w.lambda2[:nm]
+    bk2 = (np.arange(base_mode, base_mode + nm, dtype=np.float64)) ** 2
+    S = sx.ModalMatrixSys(sx.Mesh(w.mesh), base_mode=base_mode, num_modes=nm, method=sx.DIRECT,
+                          lambda2_modes=lam, betak2_modes=bk2)
+    forcing = w.forcing[:nz]
     bc = None
     if with_bc:
         nb = max(len(w.mesh.boundaries), 1)
-        bc = np.random.default_rng(5).standard_normal((w.nz, nb, w.mesh.np))
-    return w, S, bc
+        bc = np.random.default_rng(5).standard_normal((nz, nb, w.mesh.np))
+    return w, S, bc, forcing
 
 
-@pytest.mark.parametrize("with_bc", [False, True])
-def test_static_equals_device_on_consecutive_calls(sx, torch, with_bc):
-    w, S, bc = _case(sx, with_bc)
+# (boundary values, planes, first mode, stream): the legacy default stream with
+# and without boundary data; one plane (mode 0 alone); a rank's block of modes
+# (base_mode > 0: no Nyquist plane, plane 0 is not mode 0); a stream the caller
+# created, on which the job records and the solve are ordered
+CASES = {
+    "nz12": (False, 12, 0, False),
+    "nz12_bc": (True, 12, 0, False),
+    "nz1": (False, 1, 0, False),
+    "base_mode2": (True, 8, 2, False),
+    "user_stream": (True, 12, 0, True),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_static_equals_device_on_consecutive_calls(sx, torch, case):
+    with_bc, nz, base_mode, own_stream = CASES[case]
+    w, S, bc, forcing = _case(sx, with_bc, nz, base_mode)
     # device buffers made once: the copies below allocate nothing on the device
-    f_host = torch.tensor(w.forcing)
+    f_host = torch.tensor(forcing)
     f = torch.empty_like(f_host, device="cuda")
     u = torch.empty_like(f)
     b = None if bc is None else torch.tensor(bc, device="cuda")
     bptr = 0 if b is None else b.data_ptr()
-    args = (w.nz, w.mesh.nplane)
+    args = (nz, w.mesh.nplane)
+    stream = torch.cuda.Stream() if own_stream else None
+    sptr = stream.cuda_stream if stream is not None else 0
 
     def run(entry):
-        f.copy_(f_host)  # the forcing is overwritten by a solve
-        u.zero_()
-        st = entry(u.data_ptr(), f.data_ptr(), bptr, *args)
+        ctx = torch.cuda.stream(stream) if stream is not None else torch.cuda.stream(torch.cuda.default_stream())
+        with ctx:
+            f.copy_(f_host)  # the forcing is overwritten by a solve
+            u.zero_()
+            st = entry(u.data_ptr(), f.data_ptr(), bptr, *args, stream=sptr)
+            out = u.cpu().numpy()  # ordered after the solve on the same stream
         torch.cuda.synchronize()
         S.status()
-        return u.cpu().numpy(), st
+        return out, st
 
     ref, st_ref = run(S.solve_device)
     first, st1 = run(S.solve_device_static)  # first call on the device: set-up
@@ -71,7 +95,8 @@ def test_static_equals_device_on_consecutive_calls(sx, torch, with_bc):
     assert np.all(np.isfinite(ref)) and np.linalg.norm(ref) > 0.0
     for got in (first, second, third):
         assert np.array_equal(got, ref)
-    assert st1["planes_solved"] == st_ref["planes_solved"] == w.planes_solved
+    planes = 1 if nz == 1 else (nz - 1 if base_mode == 0 else nz)
+    assert st1["planes_solved"] == st_ref["planes_solved"] == planes
     assert st2["kernel_launches"] == st3["kernel_launches"] > 0
     assert free1 == free0
 
