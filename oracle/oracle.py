@@ -56,6 +56,7 @@ def lib():
         L.orc_sys_singular.argtypes = [C.c_void_p]
         L.orc_sys_singular.restype = C.c_int
         L.orc_sys_band.argtypes = [C.c_void_p, _dp]
+        L.orc_sys_set_band.argtypes = [C.c_void_p, _dp]
         L.orc_sys_hbi.argtypes = [C.c_void_p, _dp]
         L.orc_sys_hii.argtypes = [C.c_void_p, _dp]
         L.orc_sys_pc.argtypes = [C.c_void_p, _dp]
@@ -114,19 +115,35 @@ class OracleMesh:
 
 
 class OracleSystem:
-    """One MatrixSys (src/matrix.cpp:139-317) for (lambda2, betak2)."""
+    """One MatrixSys (src/matrix.cpp:139-317) for (lambda2, betak2).
 
-    def __init__(self, mesh: OracleMesh, lambda2: float, betak2: float, method: int = DIRECT):
+    factor="restated" factors the band with the oracle's own dpbtf2
+    restatement; factor="lapack" assembles the same band and factors it with
+    LAPACK's dpbtrf from scipy's bundled OpenBLAS -- the routine the reference
+    calls (src/matrix.cpp:259) -- which is blocked and far faster on large
+    bands (the factor is set-up; solves use the oracle's dpbtrs restatement
+    either way)."""
+
+    def __init__(self, mesh: OracleMesh, lambda2: float, betak2: float, method: int = DIRECT,
+                 factor: str = "restated"):
         self.mesh = mesh
         self.lambda2, self.betak2, self.method = lambda2, betak2, method
         info = C.c_int(0)
-        self.h = lib().orc_sys_create(mesh.h, lambda2, betak2, method, C.byref(info))
+        lapack = method == DIRECT and factor == "lapack"
+        self.h = lib().orc_sys_create(mesh.h, lambda2, betak2, 2 if lapack else method, C.byref(info))
         if info.value:
             lib().orc_sys_destroy(self.h)
             self.h = None
             raise RuntimeError(f"oracle system setup failed (info={info.value})")
         self.nsolve = lib().orc_sys_nsolve(self.h)
         self.singular = bool(lib().orc_sys_singular(self.h))
+        if lapack and self.nsolve:
+            from scipy.linalg.lapack import dpbtrf
+            H = self.band()                      # (nsolve, nband) row-major = LAPACK (ldab, n)
+            c, info2 = dpbtrf(H.T, lower=0, overwrite_ab=1)
+            if info2:
+                raise RuntimeError(f"oracle system setup failed (dpbtrf info={info2})")
+            lib().orc_sys_set_band(self.h, np.ascontiguousarray(c.T))
 
     def __del__(self):
         if getattr(self, "h", None):

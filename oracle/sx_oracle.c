@@ -599,11 +599,16 @@ typedef struct {
   double *PC;         /* npts */
 } orc_sys;
 
+/* method: 0 DIRECT, 1 JACPCG, 2 DIRECT with the band assembled but not
+ * factored (the caller factors it, e.g. with LAPACK dpbtrf as the reference
+ * does at src/matrix.cpp:259, and hands it back with orc_sys_set_band). */
 orc_sys *orc_sys_create(const orc_mesh *M, double lambda2, double betak2, int method, int *info)
 {
   orc_sys *S = (orc_sys *)calloc(1, sizeof(orc_sys));
   const int next = M->next, nint = M->nint, nel = M->nel, np = M->np;
   const double hCon = betak2 + lambda2;
+  const int factor = method == 0;
+  if (method == 2) method = 0;
   S->M = M; S->lambda2 = lambda2; S->betak2 = betak2; S->method = method;
   S->nglobal = M->nglobal; S->nband = M->nband;
   /* src/matrix.cpp:166-169 */
@@ -648,7 +653,7 @@ orc_sys *orc_sys_create(const orc_mesh *M, double lambda2, double betak2, int me
       int i = (side == 3) ? bmap[0] : start[nm];
       if (i < nsolve) S->H[(size_t)i * nband + nband - 1] += M->b_K[b] * area[nm];
     }
-    if (nsolve) {
+    if (nsolve && factor) {
       int r = orc_dpbtrf(nsolve, nband - 1, S->H, nband);
       if (r) *info = r;
     }
@@ -688,6 +693,7 @@ void orc_sys_destroy(orc_sys *S)
 int orc_sys_nsolve(const orc_sys *S) { return S->nsolve; }
 int orc_sys_singular(const orc_sys *S) { return S->singular; }
 void orc_sys_band(const orc_sys *S, double *H) { memcpy(H, S->H, sizeof(double) * (size_t)S->nsolve * S->nband); }
+void orc_sys_set_band(orc_sys *S, const double *H) { memcpy(S->H, H, sizeof(double) * (size_t)S->nsolve * S->nband); }
 void orc_sys_hbi(const orc_sys *S, double *hbi)
 {
   memcpy(hbi, S->hbi, sizeof(double) * (size_t)S->M->nel * S->M->next * S->M->nint);

@@ -31,6 +31,7 @@ class Workload:
     exact: np.ndarray | None = None
     seed: int = 0
     info: dict = field(default_factory=dict)
+    base_mode: int = 0           # first local mode (a rank's block of modes)
 
     @property
     def num_modes(self):
@@ -38,8 +39,18 @@ class Workload:
 
     @property
     def planes_solved(self):
-        """Planes the solve touches: plane 1 (Nyquist) is skipped."""
-        return 1 if self.nz == 1 else self.nz - 1
+        """Planes the solve touches: plane 1 (Nyquist) is skipped when the
+        block starts at mode 0."""
+        if self.nz == 1:
+            return 1
+        return self.nz - 1 if self.base_mode == 0 else self.nz
+
+    @property
+    def solved_planes(self):
+        """Indices of the solved planes."""
+        if self.nz == 1:
+            return [0]
+        return ([0] + list(range(2, self.nz))) if self.base_mode == 0 else list(range(self.nz))
 
     @property
     def dof_per_plane(self):
@@ -124,6 +135,36 @@ def config3(nx=64, ny=64, np_=11, nz=128, seed=3):
         f[plane] = -(np.pi ** 2 + 9.0 + lam[k]) * a[k] * shape
     return Workload(f"cfg3_channel_{nx}x{ny}_N{np_ - 1}_nz{nz}", m, nz, 1.0, lam, bk2, f, exact,
                     seed=seed, info={"jitter": 0.20})
+
+
+def config3_block(world=1, rank=0, nx=64, ny=64, np_=11, modes_per_rank=64, seed=3):
+    """Rank `rank`'s block of a config-3 problem with modes_per_rank * world
+    Fourier modes (nz = 2 modes_per_rank world planes), split as the
+    reference splits modes across processes (contiguous blocks,
+    src/geometry.cpp:72-101; partition.mode_block): the per-GPU work stays
+    that of config 3 as ranks are added (weak scaling).  The per-mode lambda2
+    and a_k of all modes come from one seeded stream, so world = 1 is
+    config3() exactly.  Only the block's planes are built: planes 2l, 2l+1 of
+    local mode l, with the Nyquist datum at plane 1 when the block starts at
+    mode 0."""
+    from .partition import mode_block
+    nm = modes_per_rank * world
+    base, count = mode_block(nm, world, rank)
+    m = _jittered_channel(nx, ny, np_, 0.20, seed)
+    rng = np.random.default_rng(seed)
+    lam = np.exp(rng.uniform(np.log(1e-2), np.log(1e4), size=nm))
+    a = rng.standard_normal(nm) * np.maximum(np.arange(nm), 1.0) ** -2.0
+    shape = m.eval_nodes(lambda x, y: np.sin(np.pi * y) * np.cos(3 * x))
+    nzl = 2 * count
+    f = np.zeros((nzl, m.nplane))
+    exact = np.zeros((nzl, m.nplane))
+    for l in range(count):
+        k = base + l
+        exact[2 * l] = a[k] * shape
+        f[2 * l] = -(np.pi ** 2 + 9.0 + lam[k]) * a[k] * shape
+    return Workload(f"cfg3_channel_{nx}x{ny}_N{np_ - 1}_nz{2 * nm}", m, nzl, 1.0, lam[base:base + count].copy(),
+                    np.zeros(count), f, exact, seed=seed,
+                    info={"jitter": 0.20, "modes_total": nm, "rank": rank, "world": world}, base_mode=base)
 
 
 def config5(nx=128, ny=64, np_=11, nz=256, seed=5, nu=5e-4, dt=5e-4):
