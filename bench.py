@@ -846,6 +846,8 @@ def run_profile(args):
     m = w.mesh
     S = sx.ModalMatrixSys(sx.Mesh(m), num_modes=w.num_modes, method=method,
                           lambda2_modes=w.lambda2, betak2_modes=w.betak2)
+    if args.band_cluster or args.band_stages or args.band_lead:
+        S.tune(band_cluster=args.band_cluster, band_stages=args.band_stages, band_lead=args.band_lead)
     f_src = torch.tensor(w.forcing, device="cuda")
     f = torch.empty_like(f_src)
     u = torch.zeros_like(f_src)
@@ -857,11 +859,17 @@ def run_profile(args):
         else:
             S.solve_batched(u.data_ptr(), f.data_ptr(), 0, w.nz, m.nplane, sx.MIXED_FP32,
                             tol_rel=args.tol, max_refine=20, stream=sptr)
+    ms = None
     if args.profile in ("band", "band3"):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         S.profile_band_sweeps(max(1, args.steps), sptr)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
     torch.cuda.synchronize()
     print(json.dumps({"profile": args.profile, "workload": w.name, "nband": m.nband,
-                      "nsolve": m.nsolve, "modes": w.num_modes}), flush=True)
+                      "nsolve": m.nsolve, "modes": w.num_modes, "sweep_launch_ms": ms}), flush=True)
 
 
 def main():
@@ -882,6 +890,9 @@ def main():
                     help="FP64 relative residual at which the mixed form stops")
     ap.add_argument("--profile", choices=["band", "band3", "mixed", "transform"], default=None,
                     help="bounded run of one kernel family for ncu (no bench line)")
+    ap.add_argument("--band-cluster", type=int, default=0, help="--profile band*: CTAs per cluster (0: default)")
+    ap.add_argument("--band-stages", type=int, default=0, help="--profile band*: ring depth (0: default)")
+    ap.add_argument("--band-lead", type=int, default=0, help="--profile band*: leader share K (1: none; 0: default)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -225,17 +225,33 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
  *                         factored mode
  *   SX_TUNE_BAND_STAGES   band-sweep tiles in flight per CTA, 1..4 (auto:
  *                         4, or 2 or 1 when that lets a larger cluster
- *                         stay resident -- two CTAs then share an SM)     */
-enum { SX_TUNE_INNER_ITERS = 1, SX_TUNE_BAND_CLUSTER = 2, SX_TUNE_MIXED_ROUTE = 3, SX_TUNE_BAND_STAGES = 4 };
+ *                         stay resident -- two CTAs then share an SM)
+ *   SX_TUNE_BAND_LEAD     the cluster leader's share of the band tiles off
+ *                         the critical path: K in 2..64 gives it the last of
+ *                         every K such tiles of a block column (worked on
+ *                         while it waits for the other CTAs' partial sums);
+ *                         1 = none (it keeps only the tile next to the
+ *                         diagonal and the diagonal block's inverse);
+ *                         <= 0 = the default                               */
+enum {
+  SX_TUNE_INNER_ITERS = 1,
+  SX_TUNE_BAND_CLUSTER = 2,
+  SX_TUNE_MIXED_ROUTE = 3,
+  SX_TUNE_BAND_STAGES = 4,
+  SX_TUNE_BAND_LEAD = 5
+};
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 
 /* Autotuner (no reference counterpart): times the batched form on the
  * caller's own data for each candidate schedule and keeps the fastest in the
- * modal system, as sx_modal_tune would set it --
+ * modal system for launches over that many systems (the band-sweep knobs
+ * set by hand give way to it; launches over other numbers of systems, e.g.
+ * the chunks of the host-buffer entry, keep their default) --
  *   the band-sweep cluster size (CTAs sharing one system's tiles; sizes the
  *   SM groups cannot hold are skipped) and ring depth (4, 2 or 1 tiles in
- *   flight per CTA), for SX_FP64 and for the modes that SX_MIXED_FP32
- *   routes to the band Cholesky;
+ *   flight per CTA), then the leader's share of the tiles on the best of
+ *   them, for SX_FP64 and for the modes that SX_MIXED_FP32 routes to the
+ *   band Cholesky;
  *   the floor on FP32 iterations per refinement round, for SX_MIXED_FP32.
  * d_f is only read (each trial solves a copy, allocated for the duration);
  * d_u holds the last trial's solution.  Candidates whose solve does not
@@ -246,6 +262,7 @@ typedef struct {
   double ms;        /* one solve with the chosen schedule                     */
   int trials;       /* schedules timed                                        */
   int band_stages;  /* chosen band-sweep ring depth (0: no band sweeps)       */
+  int band_lead;    /* chosen leader share K (0: none, as knob value 1)       */
 } sx_tune_result;
 SX_API int sx_modal_autotune(sx_modal modal, double *d_u, const double *d_f, const double *d_bc, int nz,
                              int plane_stride, int precision, double tol_rel, int max_refine, void *stream,

@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(_HERE, "libsemtex_b200.so")
 DIRECT, JACPCG, MIXED_SOLVER, AUTO = 0, 1, 2, 3
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
-TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE, TUNE_BAND_STAGES = 1, 2, 3, 4
+TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE, TUNE_BAND_STAGES, TUNE_BAND_LEAD = 1, 2, 3, 4, 5
 ROUTE_AUTO, ROUTE_CG, ROUTE_BAND = 0, 1, 2
 STATIC_SCRATCH_BYTES = 4 << 20  # SX_STATIC_SCRATCH_BYTES
 
@@ -66,7 +66,7 @@ class SolveStats(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("band_cluster", C.c_int), ("inner_iters", C.c_int), ("ms", C.c_double),
-                ("trials", C.c_int), ("band_stages", C.c_int)]
+                ("trials", C.c_int), ("band_stages", C.c_int), ("band_lead", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -328,11 +328,14 @@ class ModalMatrixSys:
         self.last_stats = st.as_dict()
         return u
 
-    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None, band_stages=None):
+    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None, band_stages=None, band_lead=None):
         """Schedule knobs of the batched forms (None leaves a knob alone, 0
         restores its default).  mixed_route: ROUTE_AUTO (by cost), ROUTE_CG
         (FP32 CG for every mode), ROUTE_BAND (band Cholesky for every
-        factored mode)."""
+        factored mode).  band_lead: K >= 2, the cluster leader taking the last
+        of every K band tiles off the critical path (1: none)."""
+        if band_lead is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_BAND_LEAD, int(band_lead)), "sx_modal_tune")
         if inner_iters is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_INNER_ITERS, int(inner_iters)), "sx_modal_tune")
         if band_cluster is not None:

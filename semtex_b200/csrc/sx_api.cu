@@ -14,23 +14,27 @@ using namespace sx;
 // sx_modal_s
 // ---------------------------------------------------------------------------
 
-int sx_modal_s::cluster(int nj, int *stages) {
-  int S = forced_stages > 0 ? forced_stages : BAND_STAGES_MAX, C = forced_cluster;
-  if (C <= 0) {
-    auto it = cluster_for.find(nj);
-    if (it != cluster_for.end()) {
-      C = it->second.first;
-      S = it->second.second;
+BandSched sx_modal_s::sched(int nj) {
+  int J = 1;
+  for (auto &s : uniq) J = std::max(J, s->J);
+  BandSched sc;
+  if (forced_cluster > 0) {
+    sc.C = forced_cluster;
+    sc.S = forced_stages > 0 ? forced_stages : BAND_STAGES_MAX;
+    sc.Q = default_lead(sc.C, J);
+  } else {
+    auto it = sched_for.find(nj);
+    if (it != sched_for.end()) {
+      sc = it->second;
     } else {
-      int J = 1;
-      for (auto &s : uniq) J = std::max(J, s->J);
       // ranks 1..C-1 share the J-1 tiles j >= 2, so C <= J
-      C = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2, &S, forced_stages);
-      cluster_for[nj] = std::make_pair(C, S);
+      sc.C = pick_cluster(nj, std::min(16, std::max(1, J)), 2, J + 2, &sc.S, forced_stages);
+      sc.Q = default_lead(sc.C, J);
+      sched_for[nj] = sc;
     }
   }
-  if (stages) *stages = S;
-  return C;
+  if (forced_lead >= 0) sc.Q = forced_lead;
+  return sc;
 }
 
 void sx_modal_s::rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vector<std::shared_ptr<System>> s) {
@@ -46,7 +50,7 @@ void sx_modal_s::rebind(sx_mesh_s *m, int base, int nmodes, int meth, std::vecto
   hyb.reset();
   mkey[0] = mkey[1] = mkey[2] = nullptr;
   mmodes.clear();
-  cluster_for.clear();
+  sched_for.clear();
 }
 
 sx_modal_s::~sx_modal_s() {
@@ -255,7 +259,13 @@ extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
     case SX_TUNE_BAND_STAGES:
       if (value < 0 || value > BAND_STAGES_MAX) return SX_ERR_ARG;
       s->forced_stages = value > 0 ? value : 0;
-      s->cluster_for.clear();
+      s->sched_for.clear();
+      s->fp64.reset();
+      s->hyb.reset();
+      return SX_OK;
+    case SX_TUNE_BAND_LEAD:
+      if (value > 64) return SX_ERR_ARG;
+      s->forced_lead = value <= 0 ? -1 : (value == 1 ? 0 : value);
       s->fp64.reset();
       s->hyb.reset();
       return SX_OK;
@@ -377,9 +387,7 @@ extern "C" int sx_field_solve_device(sx_modal s, double *d_u, double *d_f, const
     std::vector<Job> one(1, jobs[i]);
     if (S.method == SX_DIRECT) {
       int nl = 0;
-      int S = BAND_STAGES_MAX;
-      const int C = s->cluster(1, &S);
-      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st, C, &nl, S));
+      SX_TRY(direct_solve_jobs(M, s->djobs.p + i, one, st, s->sched(1), &nl));
       loc.kernel_launches += nl;
     } else {
       int iters = 0;
@@ -454,13 +462,13 @@ static int direct_batched(sx_modal_s *s, DirectBatch &B, const std::vector<Group
     SX_CUDA(cudaMemcpyAsync(B.djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
     SX_CUDA(cudaStreamSynchronize(st));
     SX_TRY(prepare_direct_kernels(M));
-    B.C = s->cluster((int)jobs.size(), &B.S);
+    B.sc = s->sched((int)jobs.size());
     B.jobs = jobs;
     B.modes = modes;
-    if (!s->use_graphs) return direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches, B.S);
+    if (!s->use_graphs) return direct_solve_jobs(M, B.djobs.p, jobs, st, B.sc, &B.launches);
     cudaGraph_t g = nullptr;
     SX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = direct_solve_jobs(M, B.djobs.p, jobs, st, B.C, &B.launches, B.S);
+    const int rc = direct_solve_jobs(M, B.djobs.p, jobs, st, B.sc, &B.launches);
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc != SX_OK) {
       if (g) cudaGraphDestroy(g);
@@ -638,84 +646,113 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
   cudaStream_t st = stream ? (cudaStream_t)stream : s->own;
   std::vector<Group> groups;
   SX_TRY(plane_groups(*s, nz, groups));
-  // does this form run band sweeps, and how many tiles do they stream?
-  bool band = precision == SX_FP64;
-  if (!band) {
+  // does this form run band sweeps, on how many systems, and how many tiles
+  // do they stream per block column?
+  int nj = precision == SX_FP64 ? (int)groups.size() : 0;
+  if (precision != SX_FP64) {
     for (auto &u : s->uniq)
       if (!u->pcf.p) SX_TRY(system_build_jacobi_diag(*u, st));
-    for (auto &g : groups) band = band || route_direct(*s, *s->sys[g.mode], tol_rel, max_refine);
+    for (auto &g : groups) nj += route_direct(*s, *s->sys[g.mode], tol_rel, max_refine) ? 1 : 0;
   }
+  const bool band = nj > 0;
   int J = 1;
   for (auto &u : s->uniq) J = std::max(J, u->J);
   // the occupancy queries below need the sweep kernels' shared-memory limit
   if (band) SX_TRY(prepare_direct_kernels(s->mesh->view()));
-  std::vector<std::pair<int, int>> clusters;  // (cluster size, ring depth)
-  std::vector<int> inners;
-  if (band)
-    for (int S : {BAND_STAGES_MAX, 2, 1})
-      for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
-        if (C <= J && band_active_clusters(C, 2, J + 2, S) > 0) clusters.push_back(std::make_pair(C, S));
-  if (clusters.empty()) clusters.push_back(std::make_pair(0, 0));
-  if (precision == SX_MIXED_FP32)
-    inners = {8, 12, 16, 24};
-  else
-    inners = {0};
   const size_t n = (size_t)nz * plane_stride;
   DBuf<double> fw;  // the trials' forcing: a solve overwrites its forcing
   SX_TRY(fw.alloc(n));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   SX_CUDA(cudaEventCreate(&e0));
   SX_CUDA(cudaEventCreate(&e1));
-  const int saved_cluster = s->forced_cluster, saved_stages = s->forced_stages, saved_inner = s->n_inner;
-  double best = INFINITY;
+  const int saved_cluster = s->forced_cluster, saved_stages = s->forced_stages, saved_lead = s->forced_lead;
+  const int saved_inner = s->n_inner;
+  struct Cand {
+    BandSched sc;
+    int inner;
+  };
+  Cand best{s->sched(std::max(nj, 1)), saved_inner};
+  double best_t = INFINITY;
   bool best_ok = false;
-  int bc = saved_cluster, bs = saved_stages, bi = saved_inner, trials = 0, rc = SX_OK;
-  for (auto CS : clusters)
-    for (int I : inners) {
-      s->forced_cluster = CS.first;
-      s->forced_stages = CS.second;
-      if (I > 0) s->n_inner = I;
-      s->fp64.reset();  // the captured graphs bake in the cluster size and ring depth
-      s->hyb.reset();
-      double t_min = INFINITY;
-      int r = SX_OK;
-      for (int rep = 0; rep < 3 && (r == SX_OK || r == SX_WARN_STEP_LIMIT); rep++) {
-        if ((rc = (cudaMemcpyAsync(fw.p, d_f, n * 8, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? SX_OK
-                                                                                                   : SX_ERR_CUDA)))
-          break;
-        cudaEventRecord(e0, st);
-        r = solve_batched_on(s, d_u, fw.p, d_bc, nz, plane_stride, precision, tol_rel, max_refine, st, nullptr);
-        cudaEventRecord(e1, st);
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-          rc = SX_ERR_CUDA;
-          break;
-        }
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (rep > 0) t_min = std::min(t_min, (double)ms);  // rep 0 captures the graphs
+  int trials = 0, rc = SX_OK;
+  // one candidate: three solves (the first captures the graphs), the faster
+  // of the last two; kept when it converges and beats the best so far
+  auto trial = [&](const Cand &c) {
+    s->forced_cluster = c.sc.C;
+    s->forced_stages = c.sc.S;
+    s->forced_lead = c.sc.Q;
+    s->n_inner = c.inner;
+    s->fp64.reset();  // the captured graphs bake in the schedule
+    s->hyb.reset();
+    double t_min = INFINITY;
+    int r = SX_OK;
+    for (int rep = 0; rep < 3 && (r == SX_OK || r == SX_WARN_STEP_LIMIT); rep++) {
+      if (cudaMemcpyAsync(fw.p, d_f, n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+        rc = SX_ERR_CUDA;
+        return;
       }
-      if (rc != SX_OK) break;
-      if (r != SX_OK && r != SX_WARN_STEP_LIMIT) continue;
-      trials++;
-      const bool ok = r == SX_OK;
-      if ((ok && !best_ok) || (ok == best_ok && t_min < best)) {
-        best = t_min;
-        best_ok = ok;
-        bc = CS.first;
-        bs = CS.second;
-        bi = I > 0 ? I : saved_inner;
+      cudaEventRecord(e0, st);
+      r = solve_batched_on(s, d_u, fw.p, d_bc, nz, plane_stride, precision, tol_rel, max_refine, st, nullptr);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = SX_ERR_CUDA;
+        return;
       }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) t_min = std::min(t_min, (double)ms);
     }
+    if (r != SX_OK && r != SX_WARN_STEP_LIMIT) return;
+    trials++;
+    const bool ok = r == SX_OK;
+    if ((ok && !best_ok) || (ok == best_ok && t_min < best_t)) {
+      best_t = t_min;
+      best_ok = ok;
+      best = c;
+    }
+  };
+  const int inner0 = precision == SX_MIXED_FP32 ? saved_inner : s->n_inner;
+  if (band) {
+    // (1) cluster size and ring depth, with the default leader share
+    for (int S : {BAND_STAGES_MAX, 3, 2, 1})
+      for (int C : {1, 2, 3, 4, 6, 8, 12, 16})
+        if (rc == SX_OK && C <= J && band_active_clusters(C, 2, J + 2, S) > 0)
+          trial({{C, S, default_lead(C, J)}, inner0});
+    // (2) the leader's share on the best of those: none, or the last of every
+    // K positions for K = C + 1, C + 2, 2C
+    const BandSched b1 = best.sc;
+    if (b1.C > 1)
+      for (int K : {0, b1.C, b1.C + 1, b1.C + 2, 2 * b1.C})
+        if (rc == SX_OK && K != b1.Q && (K == 0 || K <= J - 1) && (K != 2 * b1.C || 2 * b1.C > b1.C + 2))
+          trial({{b1.C, b1.S, K}, inner0});
+  }
+  // (3) the floor on FP32 iterations per round, on the best band schedule
+  if (precision == SX_MIXED_FP32) {
+    const BandSched b2 = best.sc;
+    for (int I : {8, 12, 16, 24})
+      if (rc == SX_OK && I != inner0) trial({b2, I});
+    if (rc == SX_OK && !band) trial({b2, inner0});
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // the graphs captured on the trial forcing must not outlive it
   s->fp64.reset();
   s->hyb.reset();
   s->mkey[0] = s->mkey[1] = s->mkey[2] = nullptr;
-  s->forced_cluster = trials ? bc : saved_cluster;
-  s->forced_stages = trials ? bs : saved_stages;
-  s->n_inner = trials ? bi : saved_inner;
-  s->cluster_for.clear();
+  s->sched_for.clear();
+  if (trials) {
+    // the choice is kept for this many systems per launch; hand-set band
+    // knobs give way to it
+    s->forced_cluster = s->forced_stages = 0;
+    s->forced_lead = -1;
+    if (band) s->sched_for[nj] = best.sc;
+    s->n_inner = best.inner;
+  } else {
+    s->forced_cluster = saved_cluster;
+    s->forced_stages = saved_stages;
+    s->forced_lead = saved_lead;
+    s->n_inner = saved_inner;
+  }
   SX_CUDA(cudaStreamSynchronize(st));
   if (rc != SX_OK) return rc;
   if (!trials) {
@@ -723,10 +760,11 @@ extern "C" int sx_modal_autotune(sx_modal s, double *d_u, const double *d_f, con
     return SX_ERR_UNSUPPORTED;
   }
   if (out) {
-    out->band_cluster = band ? s->forced_cluster : 0;
-    out->band_stages = band ? std::max(s->forced_stages, 0) : 0;
+    out->band_cluster = band ? best.sc.C : 0;
+    out->band_stages = band ? best.sc.S : 0;
+    out->band_lead = band ? best.sc.Q : 0;
     out->inner_iters = precision == SX_MIXED_FP32 ? s->n_inner : 0;
-    out->ms = best;
+    out->ms = best_t;
     out->trials = trials;
   }
   return SX_OK;
@@ -810,8 +848,11 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
     v.own_stream_external = true;
     v.n_inner = s->n_inner;
     v.mixed_route = s->mixed_route;
-    if (v.forced_cluster != s->forced_cluster) {
+    if (v.forced_cluster != s->forced_cluster || v.forced_stages != s->forced_stages ||
+        v.forced_lead != s->forced_lead) {
       v.forced_cluster = s->forced_cluster;
+      v.forced_stages = s->forced_stages;
+      v.forced_lead = s->forced_lead;
       v.fp64.reset();
       v.hyb.reset();
     }
@@ -872,7 +913,7 @@ extern "C" int sx_profile_band_sweeps(sx_modal s, int reps, void *stream) {
   if (!s || reps <= 0 || s->fp64.jobs.empty()) return SX_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   for (int r = 0; r < reps; r++)
-    SX_TRY(band_sweep_jobs(s->fp64.djobs.p, s->fp64.jobs, s->fp64.C, st, s->fp64.S));
+    SX_TRY(band_sweep_jobs(s->fp64.djobs.p, s->fp64.jobs, s->fp64.sc, st));
   return SX_OK;
 }
 
@@ -942,6 +983,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
     key.push_back(q.stride);
     key.push_back(q.s->forced_cluster);
     key.push_back(q.s->forced_stages);
+    key.push_back(q.s->forced_lead);
     for (auto &g : q.gd) key.push_back(g.mode);
     key.push_back(-1);
   }
@@ -955,7 +997,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
   b->dkey.clear();
   std::vector<Job> jobs;
   std::vector<size_t> j0;
-  int maxJ = 1, maxP = 1, forced = 0, fstages = 0;
+  int maxJ = 1, maxP = 1, forced = 0, fstages = 0, flead = -1;
   for (Part &q : parts) {
     j0.push_back(jobs.size());
     if (q.gd.empty()) continue;
@@ -969,6 +1011,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
     }
     forced = std::max(forced, q.s->forced_cluster);
     fstages = std::max(fstages, q.s->forced_stages);
+    flead = std::max(flead, q.s->forced_lead);
     SX_TRY(prepare_direct_kernels(q.s->mesh->view()));
   }
   j0.push_back(jobs.size());
@@ -976,11 +1019,12 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
   SX_CUDA(cudaMemcpyAsync(b->djobs.p, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st));
   SX_CUDA(cudaStreamSynchronize(st));
   b->jobs = jobs;
-  b->S = BAND_STAGES_MAX;
-  b->C = forced > 0 ? forced
-                    : pick_cluster((int)jobs.size(), std::min(16, std::max(1, maxJ)), maxP <= 2 ? 2 : 8, maxJ + 2,
-                                   &b->S, fstages);
-  if (forced > 0 && fstages > 0) b->S = fstages;
+  b->sc = BandSched();
+  b->sc.C = forced > 0 ? forced
+                       : pick_cluster((int)jobs.size(), std::min(16, std::max(1, maxJ)), maxP <= 2 ? 2 : 8,
+                                      maxJ + 2, &b->sc.S, fstages);
+  if (forced > 0 && fstages > 0) b->sc.S = fstages;
+  b->sc.Q = flead >= 0 ? flead : default_lead(b->sc.C, maxJ);
   auto body = [&]() -> int {
     int nl = 0;
     for (size_t i = 0; i < parts.size(); i++) {
@@ -988,7 +1032,7 @@ static int batch_direct(sx_batch b, std::vector<Part> &parts, bool graphs, cudaS
       const std::vector<Job> slice(jobs.begin() + j0[i], jobs.begin() + j0[i + 1]);
       SX_TRY(direct_rhs_jobs(parts[i].s->mesh->view(), b->djobs.p + j0[i], slice, st, &nl));
     }
-    SX_TRY(band_sweep_jobs(b->djobs.p, jobs, b->C, st, b->S));
+    SX_TRY(band_sweep_jobs(b->djobs.p, jobs, b->sc, st));
     nl++;
     for (size_t i = 0; i < parts.size(); i++) {
       if (parts[i].gd.empty()) continue;

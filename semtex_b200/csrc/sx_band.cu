@@ -32,6 +32,7 @@ namespace sx {
 
 constexpr long long WAIT_LIMIT = SWEEP_WAIT_DEFAULT;  // ~2 s at 1.9 GHz
 
+
 // Cycles a wait of the sweep loop may take before the kernel gives up
 // (SX_ERR_TIMEOUT); per device, set by sx_set_wait_limit.  The drain of a
 // CTA's own bulk copies on the way out always uses WAIT_LIMIT: those copies
@@ -44,29 +45,70 @@ int set_sweep_wait_limit(long long cycles) {
   return SX_OK;
 }
 
+// Division by a small runtime divisor d (1 <= d <= 2^16) of n < 2^24 by one
+// 64-bit multiply: floor(n / d) = (n ceil(2^40 / d)) >> 40 exactly in that
+// range (the rounding error of the reciprocal stays below 2^-16 <= 1 / d).
+struct FastDiv {
+  unsigned long long m = 1ull << 40;
+  unsigned d = 1;
+  __host__ __device__ FastDiv() {}
+  __host__ __device__ explicit FastDiv(unsigned dv) : m(((1ull << 40) + dv - 1) / dv), d(dv) {}
+  __device__ __forceinline__ int div(int n) const { return (int)(((unsigned long long)(unsigned)n * m) >> 40); }
+  __device__ __forceinline__ int mod(int n) const { return n - div(n) * (int)d; }
+};
+
 struct SweepGeom {
   int nblk, J, C, rank;
+  // Leader share: Q = 0, the leader (rank 0) owns only the j = 1 tile and
+  // D_k, and ranks 1..C-1 the tiles j >= 2 round-robin.  Q = K >= 2: the
+  // positions p = j - 2 of the tiles j >= 2 run in cycles of K whose last
+  // position is the leader's; the other positions go round-robin to ranks
+  // 1..C-1.  The leader works through its tiles of step t + 1 during step t,
+  // between its j = 1 tile and the wait for the ranks' partial sums, so they
+  // stay off the block-column chain; they are listed under step t, after
+  // the j = 1 tile and before D_k.
+  int Q;
+  FastDiv dC1, dQ, dQ1;  // divisions by C - 1, Q and Q - 1 (1 when unused)
   // tiles owned by `rank` at sequence step t (t < nblk: forward block t,
   // else backward block 2 nblk - 1 - t); D_k is always last, on rank 0.
   __device__ __forceinline__ int jmax(int t) const {
+    if (t >= 2 * nblk) return 0;
     return t < nblk ? min(J, t) : min(J, nblk - 1 - (2 * nblk - 1 - t));
+  }
+  // the leader's tiles of step t + 1, listed at step t
+  __device__ __forceinline__ int ahead_count(int t) const { return dQ.div(max(jmax(t + 1) - 1, 0)); }
+  // tiles j >= 2 of step t that are not the leader's
+  __device__ __forceinline__ int rank_positions(int t) const {
+    const int npos = max(jmax(t) - 1, 0);
+    return Q == 0 ? npos : npos - dQ.div(npos);
   }
   __device__ __forceinline__ int count(int t) const {
     const int jm = jmax(t);
     if (C == 1) return jm + 1;
-    if (rank == 0) return (jm >= 1 ? 1 : 0) + 1;
-    const int j0 = rank + 1;
-    return jm >= j0 ? (jm - j0) / (C - 1) + 1 : 0;
+    if (rank == 0) return (jm >= 1 ? 1 : 0) + (Q == 0 ? 0 : ahead_count(t)) + 1;
+    const int N = rank_positions(t);
+    return N > rank - 1 ? dC1.div(N - rank) + 1 : 0;
   }
-  // j of the idx-th owned tile (0 = D_k)
+  // j of the idx-th owned tile, in processing order: a rank's tiles j >= 2
+  // from the oldest block down; the leader's j = 1 tile, its tiles of step
+  // t + 1 from the oldest block down, then D_k (j = 0)
   __device__ __forceinline__ int jat(int t, int idx) const {
     const int jm = jmax(t);
     if (C == 1) return idx < jm ? jm - idx : 0;
-    if (rank == 0) return (jm >= 1 && idx == 0) ? 1 : 0;
-    const int j0 = rank + 1;
-    const int top = j0 + ((jm - j0) / (C - 1)) * (C - 1);
-    return top - idx * (C - 1);
+    if (rank == 0) {
+      const int a = jm >= 1 ? 1 : 0;
+      if (idx < a) return 1;
+      if (Q == 0) return 0;
+      const int F1 = ahead_count(t), e = idx - a;
+      return e < F1 ? (F1 - 1 - e) * Q + (Q - 1) + 2 : 0;
+    }
+    const int N = rank_positions(t);
+    const int n = N > rank - 1 ? dC1.div(N - rank) + 1 : 0;
+    const int i = (rank - 1) + (n - 1 - idx) * (C - 1);
+    return (Q == 0 ? i : i + dQ1.div(i)) + 2;
   }
+  // whether a tile j at step t is the leader's tile of step t + 1
+  __device__ __forceinline__ bool ahead(int j) const { return rank == 0 && C > 1 && Q > 0 && j >= 2; }
 };
 
 __device__ __forceinline__ const double *tile_src(const Job &Jb, int t, int j) {
@@ -83,7 +125,7 @@ __device__ __forceinline__ const double *tile_src(const Job &Jb, int t, int j) {
 // Two CTAs per SM for up to two planes (128 registers a thread), one for more.
 template <int PMAX>
 __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
-    k_band_sweep(const Job *__restrict__ jobs, int C, int S, int Wmax) {
+    k_band_sweep(const Job *__restrict__ jobs, int C, int S, int Wmax, int Q) {
   const int rank = (int)cluster_ctarank();
   const Job Jb = jobs[blockIdx.x / C];
   const int P = Jb.P, nblk = Jb.nblk, W = Jb.J + 2;
@@ -100,7 +142,9 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   __shared__ int abort_flag;
 
   const int tid = threadIdx.x, c = tid & (NB - 1), q = tid >> 6;
-  const SweepGeom G{nblk, Jb.J, C, rank};
+  const SweepGeom G{nblk, Jb.J, C, rank, Q, FastDiv((unsigned)max(C - 1, 1)), FastDiv((unsigned)max(Q, 1)),
+                    FastDiv((unsigned)max(Q - 1, 1))};
+  const FastDiv dW((unsigned)W);
   const long long lim = g_sweep_wait;
   if (tid == 0) {
     for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
@@ -115,8 +159,17 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
 
   const int T = 2 * nblk;
   // producer state (thread 0): next tile (tp, ip); counters are uniform.
-  int tp = 0, ip = 0;
+  int tp = 0, ip = 0, pslot = 0;
   long long nissued = 0, ncons = 0;
+  int cslot = 0;
+  uint32_t cphase = 0;  // slot and phase parity of tile ncons
+  auto consumed = [&]() {
+    ncons++;
+    if (++cslot == S) {
+      cslot = 0;
+      cphase ^= 1u;
+    }
+  };
   auto produce = [&](long long limit) {
     while (nissued < limit) {
       while (tp < T && ip >= G.count(tp)) {
@@ -125,10 +178,12 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       }
       if (tp >= T) return;
       const int j = G.jat(tp, ip);
-      double *dst = ring + (size_t)(nissued % S) * TSZ;
-      uint64_t *bar = &full[nissued % S];
+      double *dst = ring + (size_t)pslot * TSZ;
+      uint64_t *bar = &full[pslot];
+      if (++pslot == S) pslot = 0;
       mbar_arrive_expect_tx(bar, (uint32_t)(TSZ * sizeof(double)));
-      bulk_g2s(dst, tile_src(Jb, tp, j), (uint32_t)(TSZ * sizeof(double)), bar);
+      // the leader's share is listed a step early: the tile is step tp + 1's
+      bulk_g2s(dst, tile_src(Jb, G.ahead(j) ? tp + 1 : tp, j), (uint32_t)(TSZ * sizeof(double)), bar);
       nissued++;
       ip++;
     }
@@ -146,12 +201,18 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     }
     cp_async_commit();
   };
-  // The block a tile (t, j >= 2) multiplies, solved at step t - j: every
-  // thread of a rank waits (bounded) for the leader's release of it, then
-  // copies its chunk.  False if the wait ran out (nothing is copied then).
+  // The block a tile (t, j >= 2) multiplies, solved at step t - j (t + 1 - j
+  // for the leader's tiles of the next step): every thread of a rank waits
+  // (bounded) for the leader's release of it, then copies its chunk.  False
+  // if the wait ran out (nothing is copied then).
   auto fetch_y = [&](int t, int j, int b) -> bool {
-    const int src = t - j;
-    if (rank != 0 && !mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), lim)) return false;
+    const int src = (G.ahead(j) ? t + 1 : t) - j;
+    // only the copying threads need the release (the others read the block
+    // after a barrier that follows the copies)
+    if (rank != 0 && tid < P * (NB / 2)) {
+      const int qw = dW.div(src);
+      if (!mbar_wait(&ybar[src - qw * W], (uint32_t)(qw & 1), lim)) return false;
+    }
     copy_y(src, b);
     return true;
   };
@@ -173,13 +234,21 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       if (p < P) bnext[p] = Jb.rhs[(size_t)p * Jb.rhs_stride + c];
   }
 
+  // the leader's partial sums of its tiles of the next step (leader share)
+  double sn[PMAX];
+#pragma unroll
+  for (int p = 0; p < PMAX; p++) sn[p] = 0.0;
+
   for (int t = 0; t < T; t++) {
     const bool fwd = t < nblk;
     const int k = fwd ? t : 2 * nblk - 1 - t;
     const int n = G.count(t);
     double s[PMAX];
 #pragma unroll
-    for (int p = 0; p < PMAX; p++) s[p] = 0.0;
+    for (int p = 0; p < PMAX; p++) {
+      s[p] = sn[p];  // zero unless the leader worked on this step's tiles during the last one
+      sn[p] = 0.0;
+    }
     bool bad = false;
     // the step's first tile's block; each later one is fetched under the
     // work of the tile before it (j = 1 uses the leader's own yk, D_k none)
@@ -189,8 +258,8 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     for (int idx = 0; idx < n; idx++) {
       const int j = jn;
       if (j == 0) break;  // D_k: handled below by the leader
-      const int slot = (int)(ncons % S);
-      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), lim)) bad = true;
+      const int slot = cslot;
+      if (!mbar_wait(&full[slot], cphase, lim)) bad = true;
       cp_async_wait_all();  // this thread's chunks of the tile's block
       if (bad) abort_flag = 1;
       __syncthreads();
@@ -203,32 +272,43 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       if (jn >= 2) {
         if (!fetch_y(t, jn, (int)(ytile & 1))) abort_flag = 1;
       } else if (t + 1 < T) {
-        const int n1 = G.count(t + 1), j1 = n1 > 0 ? G.jat(t + 1, 0) : 0, src = t + 1 - j1;
-        if (j1 >= 2 && (rank == 0 || mbar_test_cluster(&ybar[src % W], (uint32_t)((src / W) & 1)))) {
+        const int n1 = G.count(t + 1), j1 = n1 > 0 ? G.jat(t + 1, 0) : 0;
+        const int src = (G.ahead(j1) ? t + 2 : t + 1) - j1;
+        // the leader copies without a release; block t itself is solved
+        // only at the end of this step
+        const int qw = dW.div(src);
+        if (j1 >= 2 && (rank == 0 ? src < t : mbar_test_cluster(&ybar[src - qw * W], (uint32_t)(qw & 1)))) {
           copy_y(src, (int)(ytile & 1));
           pre = true;
         }
       }
       const double *Tt = ring + (size_t)slot * TSZ;
-      if (fwd) {
+      // the leader's tiles of the next step go to sn, every other tile to s
+      auto tile_dot = [&](double(&acc)[PMAX]) {
+        if (fwd) {
 #pragma unroll 4
-        for (int rr = q * 16; rr < q * 16 + 16; rr++) {
-          const double tv = Tt[rr * LDT + c];
+          for (int rr = q * 16; rr < q * 16 + 16; rr++) {
+            const double tv = Tt[rr * LDT + c];
 #pragma unroll
-          for (int p = 0; p < PMAX; p++)
-            if (p < P) s[p] += tv * yv[p * NB + rr];
-        }
-      } else {
+            for (int p = 0; p < PMAX; p++)
+              if (p < P) acc[p] += tv * yv[p * NB + rr];
+          }
+        } else {
 #pragma unroll 4
-        for (int cc = q * 16; cc < q * 16 + 16; cc++) {
-          const double tv = Tt[c * LDT + cc];
+          for (int cc = q * 16; cc < q * 16 + 16; cc++) {
+            const double tv = Tt[c * LDT + cc];
 #pragma unroll
-          for (int p = 0; p < PMAX; p++)
-            if (p < P) s[p] += tv * yv[p * NB + cc];
+            for (int p = 0; p < PMAX; p++)
+              if (p < P) acc[p] += tv * yv[p * NB + cc];
+          }
         }
-      }
+      };
+      if (G.ahead(j))
+        tile_dot(sn);
+      else
+        tile_dot(s);
       __syncthreads();
-      ncons++;
+      consumed();
       if (tid == 0) produce(ncons + S);
     }
     if (abort_flag) break;
@@ -241,8 +321,8 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       // The leader reads pbuf[t & 1] of step t-2 before it publishes block
       // t-2; seeing that block means the slot is free again.
       if (t >= 2) {
-        const int src = t - 2;
-        if (!mbar_wait(&ybar[src % W], (uint32_t)((src / W) & 1), lim)) abort_flag = 1;
+        const int src = t - 2, qw = dW.div(src);
+        if (!mbar_wait(&ybar[src - qw * W], (uint32_t)(qw & 1), lim)) abort_flag = 1;
         __syncthreads();
         if (abort_flag) break;
       }
@@ -264,10 +344,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     if (C > 1) {
       if (!mbar_wait(&pbar[t & 1], (uint32_t)((t >> 1) & 1), lim)) abort_flag = 1;
     }
-    {
-      const int slot = (int)(ncons % S);
-      if (!mbar_wait(&full[slot], (uint32_t)((ncons / S) & 1), lim)) abort_flag = 1;
-    }
+    if (!mbar_wait(&full[cslot], cphase, lim)) abort_flag = 1;
     __syncthreads();
     if (abort_flag) break;
     if (q == 0) {
@@ -282,7 +359,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     }
     __syncthreads();
     {
-      const double *Dk = ring + (size_t)(ncons % S) * TSZ;
+      const double *Dk = ring + (size_t)cslot * TSZ;
 #pragma unroll
       for (int p = 0; p < PMAX; p++) s[p] = 0.0;
       for (int cc = q * 16; cc < q * 16 + 16; cc++) {
@@ -293,7 +370,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       }
     }
     __syncthreads();  // all reads of D_k done
-    ncons++;
+    consumed();
     if (tid == 0) produce(ncons + S);
 #pragma unroll
     for (int p = 0; p < PMAX; p++)
@@ -315,7 +392,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     // before the arrivals that follow the barrier
     if (q == 0) fence_acq_rel_cluster();
     __syncthreads();
-    if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[t % W], (uint32_t)tid));
+    if (tid > 0 && tid < C) mbar_arrive_cluster(map_rank(&ybar[dW.mod(t)], (uint32_t)tid));
     // the next step's right-hand side, issued after the fence (which would
     // wait for it) and used a step later
     if (q == 0 && t + 1 < T && t + 1 != nblk) {
@@ -331,7 +408,13 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     if (tid == 0) {
       atomicOr(Jb.status, 1 << SX_ERR_TIMEOUT);
       // drain this CTA's bulk copies still in flight (bounded)
-      for (long long i = ncons; i < nissued; i++) mbar_wait(&full[i % S], (uint32_t)((i / S) & 1), WAIT_LIMIT);
+      for (long long i = ncons; i < nissued; i++) {
+        mbar_wait(&full[cslot], cphase, WAIT_LIMIT);
+        if (++cslot == S) {
+          cslot = 0;
+          cphase ^= 1u;
+        }
+      }
     }
     __syncthreads();
   }
@@ -360,8 +443,9 @@ static int smem_optin() {
   return v;
 }
 
-// Launch both sweeps for every job: cluster size C per job.
-int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st, int smax) {
+// Launch both sweeps for every job: one cluster of sc.C CTAs per job.
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, const BandSched &sc, cudaStream_t st) {
+  const int C = sc.C, smax = sc.S;
   const int nj = (int)hjobs.size();
   if (nj == 0) return SX_OK;
   int maxP = 0, Wmax = 0;
@@ -392,9 +476,9 @@ int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cuda
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (pmax == 2)
-    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<2>, djobs, C, S, Wmax));
+    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<2>, djobs, C, S, Wmax, std::max(sc.Q, 0)));
   else
-    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<8>, djobs, C, S, Wmax));
+    SX_CUDA(cudaLaunchKernelEx(&cfg, k_band_sweep<8>, djobs, C, S, Wmax, std::max(sc.Q, 0)));
   return SX_OK;
 }
 
@@ -405,6 +489,13 @@ int prepare_band_kernels() {
   SX_CUDA(cudaFuncSetAttribute(k_band_sweep<2>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   SX_CUDA(cudaFuncSetAttribute(k_band_sweep<8>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   return SX_OK;
+}
+
+int default_lead(int C, int J) {
+  // an equal share (the last of every C positions) was the fastest share on
+  // every cluster size measured (config-3 band, 64 systems: C = 2, 3, 4);
+  // with fewer than C positions per block column the leader gets none
+  return (C >= 2 && J - 1 >= C) ? C : 0;
 }
 
 // Largest cluster size (<= cmax) for which `nj` clusters can be resident at
@@ -445,7 +536,7 @@ int band_active_clusters(int C, int pmax, int Wmax, int smax) {
 // stages_forced > 0 fixes the depth.
 int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out, int stages_forced) {
   int bestC = 1, bestS = BAND_STAGES_MAX;
-  for (int S0 : {BAND_STAGES_MAX, 2, 1}) {
+  for (int S0 : {BAND_STAGES_MAX, 3, 2, 1}) {
     if (stages_forced > 0 && S0 != stages_forced) continue;
     if (S0 == 1 && stages_forced != 1 && bestC > 2) continue;
     for (int C = 1; C <= cmax; C++) {

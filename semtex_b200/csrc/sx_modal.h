@@ -24,7 +24,8 @@ struct DirectBatch {
   std::vector<int> modes;  // local mode of each group, in job order
   DBuf<Job> djobs;
   std::vector<Job> jobs;   // host copy of the captured jobs
-  int C = 1, S = 4, launches = 0; // band-sweep cluster size and ring depth, kernels per solve
+  BandSched sc;                   // band-sweep schedule
+  int launches = 0;               // kernels per solve
   void reset() {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
@@ -67,11 +68,12 @@ struct sx_modal_s {
   int mixed_route = 0;               // 0 auto, 1 FP32 CG only, 2 band solve where factored
   bool use_graphs = true;
   cudaMemPool_t pool = nullptr;      // when set, workspaces are allocated from it
-  std::map<int, std::pair<int, int>> cluster_for;  // jobs per launch -> band-sweep cluster size, ring depth
-  int forced_cluster = 0, forced_stages = 0;
-  // Band-sweep cluster size (and, through stages, ring depth) for nj systems
-  // per launch: the knobs when set, else the largest resident cluster.
-  int cluster(int nj, int *stages = nullptr);
+  std::map<int, sx::BandSched> sched_for;  // systems per launch -> band-sweep schedule (default or tuned)
+  int forced_cluster = 0, forced_stages = 0, forced_lead = -1;
+  // Band-sweep schedule for nj systems per launch: the knobs where set, else
+  // the autotuner's choice for nj, else the largest cluster whose CTAs are
+  // all resident (and the default leader share).
+  sx::BandSched sched(int nj);
   // host-buffer entry, pipelined: per-chunk views of this system (16 modes
   // each, sharing its systems) and the copy streams and events
   struct HostPipe {
@@ -96,7 +98,8 @@ struct sx_batch_s {
   std::vector<sx::Job> jobs;
   std::vector<long long> dkey;  // members and buffers the direct graph was captured for
   cudaGraphExec_t dexec = nullptr;
-  int dlaunches = 0, C = 1, S = 4;
+  int dlaunches = 0;
+  sx::BandSched sc;
   bool use_graphs = true;       // capture and replay (the serving loop, whose member set
                                 // changes from batch to batch, enqueues directly)
   cudaStream_t own = nullptr, aux = nullptr;

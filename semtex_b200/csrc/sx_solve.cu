@@ -307,10 +307,10 @@ int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_
 }
 
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st, int C, int *launches, int stages) {
+                      cudaStream_t st, const BandSched &sc, int *launches) {
   int nl = 0;
   SX_TRY(direct_rhs_jobs(M, djobs, hjobs, st, &nl));
-  SX_TRY(band_sweep_jobs(djobs, hjobs, C, st, stages));
+  SX_TRY(band_sweep_jobs(djobs, hjobs, sc, st));
   SX_TRY(direct_backsub_jobs(M, djobs, (int)hjobs.size(), st, &nl));
   if (launches) *launches = nl + 1;
   return SX_OK;

@@ -73,8 +73,15 @@ __device__ __forceinline__ void helm_op(const T *D, const T *Q1, const T *Q2, co
 // Ring depth (tiles in flight per CTA) of the band sweeps: at most 4; 2
 // lets two CTAs share an SM, so that larger clusters stay resident.
 constexpr int BAND_STAGES_MAX = 4;
+// Schedule of one band-sweep launch: C CTAs per system's cluster, S tiles in
+// flight per CTA, and the leader's share of the tiles j >= 2: Q = 0 none,
+// Q = K >= 2 the last of every K of them (worked on a step ahead).
+struct BandSched {
+  int C = 1, S = BAND_STAGES_MAX, Q = 0;
+  bool operator==(const BandSched &o) const { return C == o.C && S == o.S && Q == o.Q; }
+};
 int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs,
-                      cudaStream_t st, int C, int *launches = nullptr, int stages = BAND_STAGES_MAX);
+                      cudaStream_t st, const BandSched &sc, int *launches = nullptr);
 // The phases of direct_solve_jobs, for batches whose band sweeps run in one
 // launch across meshes: essential values, condensed RHS (element kernels
 // and direct-stiffness sum); then, after the sweeps, the interior
@@ -82,8 +89,7 @@ int direct_solve_jobs(const MeshView &M, const Job *djobs, const std::vector<Job
 int direct_rhs_jobs(const MeshView &M, const Job *djobs, const std::vector<Job> &hjobs, cudaStream_t st,
                     int *launches);
 int direct_backsub_jobs(const MeshView &M, const Job *djobs, int nj, cudaStream_t st, int *launches);
-int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, int C, cudaStream_t st,
-                    int stages = BAND_STAGES_MAX);
+int band_sweep_jobs(const Job *djobs, const std::vector<Job> &hjobs, const BandSched &sc, cudaStream_t st);
 int prepare_band_kernels();
 // Bounded device-side waits on the current device (sx_set_wait_limit): the
 // band sweeps' and the FP32 iterations' limits in clock cycles (<= 0: one
@@ -92,6 +98,9 @@ constexpr long long SWEEP_WAIT_DEFAULT = 4000000000LL, CG_WAIT_DEFAULT = 2000000
 int set_sweep_wait_limit(long long cycles);
 int set_cg_wait_limit(long long cycles);
 int pick_cluster(int nj, int cmax, int pmax, int Wmax, int *stages_out = nullptr, int stages_forced = 0);
+// Default leader share Q (0 or a cycle length K >= 2) of a cluster of C CTAs
+// on a band of J off-diagonal tiles per block column.
+int default_lead(int C, int J);
 // Clusters of C band-sweep CTAs that can be resident at once (0: C does not
 // fit an SM group, so a launch with it would fail).
 int band_active_clusters(int C, int pmax, int Wmax, int stages = BAND_STAGES_MAX);

@@ -120,8 +120,7 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
   cudaStream_t st = (cudaStream_t)stream;
   const MeshView M = s->mesh->view();
   SX_TRY(prepare_direct_kernels(M));
-  int stages = BAND_STAGES_MAX;
-  const int C = s->cluster(1, &stages);
+  const BandSched sc = s->sched(1);
   const long long bcstride = (long long)std::max(Mh.nbound, 1) * Mh.np;
   // one host Job, reused: the 1-element vector is allocated once per thread
   // (direct_solve_jobs reads the host copy only while it enqueues)
@@ -164,7 +163,7 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
     k_put_job<<<1, 32, 0, st>>>(djob, j);
     SX_CUDA(cudaGetLastError());
     int nl = 0;
-    SX_TRY(direct_solve_jobs(M, djob, one, st, C, &nl, stages));
+    SX_TRY(direct_solve_jobs(M, djob, one, st, sc, &nl));
     loc.kernel_launches += nl + 1;
     loc.planes_solved += g.P;
   }

@@ -81,6 +81,27 @@ def test_batched_fp64_equals_plain(sx, torch, cluster, stages):
     assert st["planes_solved"] == w.nz - 1
 
 
+@pytest.mark.parametrize("cluster,stages,lead", [(2, 2, 2), (3, 2, 3), (3, 4, 4), (4, 2, 5), (4, 1, 8),
+                                                  (5, 2, 6), (2, 1, 3), (4, 2, 1)])
+def test_batched_fp64_leader_share_equals_plain(sx, torch, cluster, stages, lead):
+    """The cluster leader working a step ahead on its share of the band tiles
+    (the last of every `lead` tiles j >= 2; 1 = none) gives the plain form's
+    answer to rounding, for every cluster size and ring depth: a band of
+    9 tiles per block column, 54 block columns, so every CTA owns tiles."""
+    from semtex_b200.workloads import small_channel
+    w = small_channel(nx=24, ny=10, np_=9, nz=8, lam=1e4, seed=11)
+    _, S = _setup(sx, w)
+    S.tune(band_cluster=cluster, band_stages=stages, band_lead=lead)
+    up, _ = _run_device(torch, S, w, batched=False)
+    ub, st = _run_device(torch, S, w, batched=True)
+    sp = solved_planes(w.nz)
+    l2, mx = rel_errs(ub[sp], up[sp])
+    assert l2 <= 1e-13 and mx <= 1e-13, (cluster, lead, l2, mx)
+    uo, _ = solve_planes(OracleMesh(w.mesh), 0.0, 1.0, w.forcing, None, lambda2_per_mode=w.lambda2)
+    l2, mx = rel_errs(ub[sp], uo[sp])
+    assert l2 <= 1e-12 and mx <= 1e-12, (cluster, lead, l2, mx)
+
+
 @pytest.mark.parametrize("lam,inner", [(1e6, 12), (1e3, 30)])
 def test_mixed_matches_oracle(sx, torch, lam, inner):
     from semtex_b200.workloads import small_channel
