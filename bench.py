@@ -811,6 +811,8 @@ def run_profile(args):
            nz = 16 (8 systems, ~0.5 GB of factors, larger than L2)
     band3: band sweeps of two config-3 systems (the full 64 x 64, N = 10
            mesh, modes 0 and 1: 2.9 GB of factors, the config-3 band)
+    solve3: `steps` batched FP64 solves of config 3 at full size (every
+           mode factored, 121 GB), for a launch list (one-pass metrics only)
     mixed: the mixed-precision batched form on the full config-2 workload
            with Jacobi systems only (no band factors, ~0.3 GB resident)
     transform: the z-direction transform of the config-2 field (nz = 64,
@@ -837,6 +839,10 @@ def run_profile(args):
         from semtex_b200.workloads import config3_block
         w = config3_block(world=32, rank=0, modes_per_rank=2)
         method = sx.DIRECT
+    elif args.profile == "solve3":
+        from semtex_b200.workloads import config3_block
+        w = config3_block()
+        method = sx.DIRECT
     elif args.profile == "band":
         w = config2(ny=16, nz=16)
         method = sx.DIRECT
@@ -854,7 +860,7 @@ def run_profile(args):
     sptr = torch.cuda.current_stream().cuda_stream
     for _ in range(max(1, args.steps)):
         f.copy_(f_src)
-        if args.profile in ("band", "band3"):
+        if args.profile in ("band", "band3", "solve3"):
             S.solve_batched(u.data_ptr(), f.data_ptr(), 0, w.nz, m.nplane, sx.FP64, stream=sptr)
         else:
             S.solve_batched(u.data_ptr(), f.data_ptr(), 0, w.nz, m.nplane, sx.MIXED_FP32,
@@ -888,7 +894,7 @@ def main():
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
-    ap.add_argument("--profile", choices=["band", "band3", "mixed", "transform"], default=None,
+    ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform"], default=None,
                     help="bounded run of one kernel family for ncu (no bench line)")
     ap.add_argument("--band-cluster", type=int, default=0, help="--profile band*: CTAs per cluster (0: default)")
     ap.add_argument("--band-stages", type=int, default=0, help="--profile band*: ring depth (0: default)")

@@ -774,13 +774,24 @@ sx_modal_s::HostPipe::~HostPipe() {
   views.clear();
   for (cudaEvent_t e : in) cudaEventDestroy(e);
   for (cudaEvent_t e : done) cudaEventDestroy(e);
+  for (cudaStream_t x : cs) cudaStreamDestroy(x);
   if (h2d) cudaStreamDestroy(h2d);
   if (d2h) cudaStreamDestroy(d2h);
 }
 
-// Modes per chunk of the pipelined host entry: 32 planes, one full lane
-// chunk of the mixed form's kernels.
-constexpr int HOST_CHUNK_MODES = 16;
+// Modes per chunk of the pipelined host entry: half the modes, rounded up to
+// a multiple of 16 (32 planes, one full lane chunk of the mixed form's
+// kernels), at least 16.  Two chunks let the second chunk's copy in and the
+// first chunk's copy out overlap the solves; more, smaller chunks would
+// shorten the overlap's ends but run each chunk's band sweeps with fewer
+// systems per launch, where every system's block-column chain, not HBM,
+// sets the time (config 3: four 16-mode chunks 81.6 ms end to end against a
+// 41.9 ms solve).
+constexpr int HOST_CHUNK_MIN = 16;
+static int host_chunk_modes(int nmodes) {
+  const int half = (nmodes + 1) / 2;
+  return std::max(HOST_CHUNK_MIN, (half + HOST_CHUNK_MIN - 1) / HOST_CHUNK_MIN * HOST_CHUNK_MIN);
+}
 
 extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *f, const double *bc,
                                            int nz, int plane_stride, int precision, double tol_rel,
@@ -796,7 +807,8 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
   if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
   cudaStream_t st = s->own;
   const int nmodes = nz == 1 ? 1 : nz / 2;
-  const int nchunks = (nmodes + HOST_CHUNK_MODES - 1) / HOST_CHUNK_MODES;
+  const int chunk = host_chunk_modes(nmodes);
+  const int nchunks = (nmodes + chunk - 1) / chunk;
   if (nchunks < 2 || nz % 2 || nmodes > s->num_modes) {
     SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));
     if (bc) SX_CUDA(cudaMemcpyAsync(s->hbc.p, bc, nbc * 8, cudaMemcpyHostToDevice, st));
@@ -807,10 +819,12 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
     SX_TRY(take_status(s, true, st, false));
     return rc;
   }
-  // Pipelined: every chunk's forcing goes up on one stream at once; the
-  // chunks are solved in turn on `st`, each after its copy has landed; a
-  // chunk's solution goes down on a third stream while the next one is
-  // solved.  Chunk c covers modes [16c, 16c + 16), planes [32c, 32c + 32)
+  // Pipelined: every chunk's forcing goes up on one stream at once; each
+  // chunk is solved on its own stream as soon as its copy has landed, so the
+  // chunks' solves run side by side (with the band-sweep schedule of the
+  // whole field, whose CTAs they share out between them), and a chunk's
+  // solution goes down on a third stream as soon as it is solved.  Chunk c
+  // covers modes [chunk c, chunk (c + 1)), planes [2 chunk c, 2 chunk (c + 1))
   // (chunk 0 keeps the Nyquist plane 1 in place).
   if (!s->pipe) s->pipe.reset(new sx_modal_s::HostPipe());
   sx_modal_s::HostPipe &P = *s->pipe;
@@ -824,11 +838,18 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
     P.done.push_back(b);
   }
   while ((int)P.views.size() < nchunks) P.views.emplace_back(new sx_modal_s());
+  while ((int)P.cs.size() < nchunks) {
+    cudaStream_t x = nullptr;
+    SX_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    P.cs.push_back(x);
+  }
+  // the schedule a launch over every mode would take (tuned or default)
+  const BandSched psc = s->sched(nmodes);
   // the views share the system objects; their workspaces are their own
   SX_CUDA(cudaEventRecord(P.in[0], st));  // the device buffers are free once st's earlier work is done
   SX_CUDA(cudaStreamWaitEvent(P.h2d, P.in[0], 0));
   for (int c = 0; c < nchunks; c++) {
-    const int m0 = c * HOST_CHUNK_MODES, m1 = std::min(nmodes, m0 + HOST_CHUNK_MODES);
+    const int m0 = c * chunk, m1 = std::min(nmodes, m0 + chunk);
     const size_t off = (size_t)2 * m0 * plane_stride, len = (size_t)2 * (m1 - m0) * plane_stride;
     SX_CUDA(cudaMemcpyAsync(s->hf.p + off, f + off, len * 8, cudaMemcpyHostToDevice, P.h2d));
     if (bc)
@@ -839,35 +860,36 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
   int rc = SX_OK;
   sx_solve_stats tot{};
   for (int c = 0; c < nchunks; c++) {
-    const int m0 = c * HOST_CHUNK_MODES, m1 = std::min(nmodes, m0 + HOST_CHUNK_MODES);
+    const int m0 = c * chunk, m1 = std::min(nmodes, m0 + chunk);
     sx_modal_s &v = *P.views[c];
     const std::vector<std::shared_ptr<System>> sub(s->sys.begin() + m0, s->sys.begin() + m1);
     if (v.mesh != s->mesh || v.base_mode != s->base_mode + m0 || v.num_modes != m1 - m0 || v.sys != sub)
       v.rebind(s->mesh, s->base_mode + m0, m1 - m0, s->method, sub);
-    v.own = st;
+    cudaStream_t vs = P.cs[c];
+    v.own = vs;
     v.own_stream_external = true;
     v.n_inner = s->n_inner;
     v.mixed_route = s->mixed_route;
-    if (v.forced_cluster != s->forced_cluster || v.forced_stages != s->forced_stages ||
-        v.forced_lead != s->forced_lead) {
-      v.forced_cluster = s->forced_cluster;
-      v.forced_stages = s->forced_stages;
-      v.forced_lead = s->forced_lead;
+    if (v.forced_cluster != psc.C || v.forced_stages != psc.S || v.forced_lead != psc.Q) {
+      v.forced_cluster = psc.C;
+      v.forced_stages = psc.S;
+      v.forced_lead = psc.Q;
       v.fp64.reset();
       v.hyb.reset();
     }
     if (!v.dstatus.p) {
       SX_TRY(v.dstatus.alloc(1));
-      SX_TRY(v.dstatus.zero(st));
+      SX_TRY(v.dstatus.zero(vs));
     }
     const size_t off = (size_t)2 * m0 * plane_stride;
-    SX_CUDA(cudaStreamWaitEvent(st, P.in[c], 0));
+    SX_CUDA(cudaStreamWaitEvent(vs, P.in[c], 0));
     sx_solve_stats cs{};
     const int r = solve_batched_on(&v, s->hu.p + off, s->hf.p + off, bc ? s->hbc.p + 2 * m0 * bcp : nullptr,
-                                   2 * (m1 - m0), plane_stride, precision, tol_rel, max_refine, st, &cs);
+                                   2 * (m1 - m0), plane_stride, precision, tol_rel, max_refine, vs, &cs);
     if (r != SX_OK && r != SX_WARN_STEP_LIMIT) return r;
     if (r == SX_WARN_STEP_LIMIT) rc = r;
-    SX_CUDA(cudaEventRecord(P.done[c], st));
+    SX_CUDA(cudaEventRecord(P.done[c], vs));
+    SX_CUDA(cudaStreamWaitEvent(st, P.done[c], 0));  // later work on st follows every chunk
     SX_CUDA(cudaStreamWaitEvent(P.d2h, P.done[c], 0));
     SX_TRY(copy_solved_planes(u + off, s->hu.p + off, 2 * (m1 - m0), plane_stride, v.base_mode, P.d2h));
     tot.planes_solved += cs.planes_solved;
@@ -879,8 +901,8 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
     tot.kernel_launches += cs.kernel_launches;
   }
   SX_CUDA(cudaStreamSynchronize(P.d2h));
-  for (auto &v : P.views)
-    if (v->dstatus.p) SX_TRY(take_status(v.get(), true, st, false));
+  for (int c = 0; c < (int)P.views.size(); c++)
+    if (P.views[c]->dstatus.p) SX_TRY(take_status(P.views[c].get(), true, P.cs[c], false));
   if (stats) *stats = tot;
   return rc;
 }

@@ -79,6 +79,7 @@ struct sx_modal_s {
   struct HostPipe {
     std::vector<std::unique_ptr<sx_modal_s>> views;
     cudaStream_t h2d = nullptr, d2h = nullptr;
+    std::vector<cudaStream_t> cs;  // one per chunk: the chunks' solves run side by side
     std::vector<cudaEvent_t> in, done;
     ~HostPipe();
   };
