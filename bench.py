@@ -527,7 +527,8 @@ def run_ours(args, rank, world):
         line["multi_mesh"] = run_multi()
         line["transform_z"] = run_transform()
     if rank == 0 and world == 1 and args.serve_requests > 0:
-        line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu)
+        line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu,
+                                      precision=args.serve_precision, slots=args.serve_slots)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -749,54 +750,120 @@ def run_transform(reps=20):
     return out
 
 
-def run_serving(n_requests, check_oracle=True):
-    """The serving loop on a bounded sample of the mixed-size request stream
-    (config 4): requests are submitted at their Poisson arrival times
-    (2000/s) to a mixed-precision server with 4 slots, each solving up to 8
-    requests per multi-mesh batch; latency is submit to result on the host,
-    as the server measures it.  The smallest requests
-    are checked against the oracle's FP64 direct solve."""
+def _build_request(args):
+    """Build one planned serving request (a spawned worker process)."""
+    spec, seed = args
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    sys.path.insert(0, ROOT)
+    from semtex_b200.workloads import ServeSpec, serving_request
+    return serving_request(ServeSpec(*spec), seed)
+
+
+def run_serving(n_requests, check_oracle=True, precision="mixed", slots=4, window=48, builders=None):
+    """The serving loop on the first `n_requests` of the mixed-size request
+    stream (config 4: Poisson arrivals at 2000/s).  Requests are built by
+    worker processes a little ahead of need (mesh and seeded forcing) and
+    submitted in arrival order once their arrival time has passed and fewer
+    than `window` are in the server; a request's latency is counted from its
+    scheduled arrival, so the time it spends waiting outside the window is
+    queueing like any other (the server admits in arrival order, and with
+    `window` above slots x max_batch it always has the next requests at
+    hand).  This keeps the host memory of the stream bounded: a request holds
+    its forcing, the server's copy and its result only while in the window.
+    The three smallest requests are checked against the oracle's FP64 direct
+    solve."""
+    import dataclasses
+    import multiprocessing as mp
+    import queue as _queue
     import semtex_b200 as sx
-    from semtex_b200.workloads import serving_trace
-    t0 = time.perf_counter()
-    trace = serving_trace(n_requests)
-    prep_s = time.perf_counter() - t0
-    srv = sx.Server(slots=4, precision=sx.MIXED_FP32, tol_rel=1e-12, max_refine=30, inner_iters=12,
-                    max_batch=8)
+    from semtex_b200.workloads import serving_plan
+    plan = serving_plan(n_requests)
+    size = [(s.ex * s.order + 1) * (s.ey * s.order + 1) * (1 if s.modes == 1 else 2 * s.modes - 1) for s in plan]
+    check = set(sorted(range(n_requests), key=lambda k: size[k])[:3]) if check_oracle else set()
+    nb = builders or max(1, min(8, (os.cpu_count() or 2) - 2))
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(nb)
+    prefetch = 2 * nb
+    builds = []
+    nbuilt = 0
+
+    def top_up(upto):
+        nonlocal nbuilt
+        while nbuilt < min(n_requests, upto):
+            builds.append(pool.apply_async(_build_request, ((dataclasses.astuple(plan[nbuilt]), 4),)))
+            nbuilt += 1
+
+    top_up(prefetch)
+    builds[0].get(timeout=600)  # the workers are up before the clock starts
+    prec = sx.MIXED_FP32 if precision == "mixed" else sx.FP64
+    srv = sx.Server(slots=slots, precision=prec, tol_rel=1e-12, max_refine=30, inner_iters=12, max_batch=8)
+    results = [None] * n_requests
+    kept = {}
+    ids = _queue.Queue()
+    completed = [0]
+
+    def waiter():
+        while True:
+            item = ids.get()
+            if item is None:
+                return
+            k, rid, t_sub = item
+            st, lat, u = srv.wait(rid, timeout_s=3600.0)
+            results[k] = (st, t_sub + lat * 1e-3)
+            if k in check:
+                kept[k] = kept[k] + (u,)
+            completed[0] += 1
+
+    th = threading.Thread(target=waiter, daemon=True)
+    th.start()
+    dofs = 0
     try:
-        ids = []
         start = time.perf_counter()
-        for r in trace:
+        for k in range(n_requests):
+            top_up(k + 1 + prefetch)
+            r = builds[k].get(timeout=600)
+            builds[k] = None
+            dofs += r.dof_solves
+            while k - completed[0] >= window:
+                time.sleep(0.0005)
             while time.perf_counter() - start < r.t_arrival:
                 pass
-            ids.append(srv.submit(r.mesh, r.lambda2, r.betak2, r.forcing))
-        res = [srv.wait(i, timeout_s=600.0) for i in ids]
-        makespan = time.perf_counter() - start
+            rid = srv.submit(r.mesh, r.lambda2, r.betak2, r.forcing)
+            if k in check:
+                kept[k] = (r,)
+            ids.put((k, rid, time.perf_counter() - start))
+        ids.put(None)
+        th.join()
+        makespan = max(t for _, t in results)
         st = srv.stats()
     finally:
         srv.close()
-    lat = np.array([lt for _, lt, _ in res])
-    ok = sum(1 for s, _, _ in res if s == sx.OK)
-    dofs = sum(r.dof_solves for r in trace)
-    out = {"requests": n_requests, "trace": "cfg4: E_x,E_y~U[2,64], N~U{4..10}, modes~U[1,64], "
-                                            "lambda2~logU[1e-2,1e4], Poisson 2000/s, seed 4",
-           "slots": 4, "precision": "mixed (FP32 CG / FP64 band per mode, FP64 refinement)",
+        pool.terminate()
+    lat = np.array([(results[k][1] - plan[k].t_arrival) * 1e3 for k in range(n_requests)])
+    ok = sum(1 for s, _ in results if s == sx.OK)
+    out = {"requests": n_requests,
+           "trace": "cfg4: E_x,E_y~U[2,64], N~U{4..10}, modes~U[1,64], lambda2~logU[1e-2,1e4], Poisson 2000/s "
+                    "(plan seed 4; request k's forcing from seed (4, k))",
+           "slots": slots,
+           "precision": ("mixed (FP32 CG / FP64 band per mode, FP64 refinement)" if precision == "mixed"
+                         else "FP64 band Cholesky for every mode"),
+           "latency": "scheduled arrival to result on the host",
            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
            "mean_ms": float(lat.mean()), "makespan_s": makespan,
            "throughput_dof_solves_per_s": dofs / makespan, "requests_per_s": n_requests / makespan,
+           "arrival_window_s": plan[-1].t_arrival, "in_server_window": window,
            "converged_to_1e-12": ok, "mesh_hits": st["mesh_hits"], "system_misses": st["system_misses"],
-           "evictions": st["evictions"], "host_prep_s_untimed": prep_s,
-           "max_batch": 8, "batches": st["batches"],
+           "evictions": st["evictions"], "max_batch": 8, "batches": st["batches"],
            "mean_batch": st["completed"] / max(st["batches"], 1),
-           # per request, averaged: waiting for admission, mesh/system builds
-           # and factorisation, the batch solve with its copies
+           # per request, averaged, as the server sees them: waiting for
+           # admission, mesh/system builds and factorisation, the batch solve
            "queue_ms_mean": st["queue_ms"] / n_requests, "build_ms_mean": st["build_ms"] / n_requests,
            "solve_ms_mean": st["solve_ms"] / n_requests}
     if check_oracle:
         from oracle.oracle import OracleMesh, solve_planes
         worst = 0.0
-        for k in sorted(range(n_requests), key=lambda k: trace[k].dof_solves)[:3]:
-            r, u = trace[k], res[k][2]
+        for k in sorted(kept):
+            r, u = kept[k]
             uo, _ = solve_planes(OracleMesh(r.mesh), 0.0, 1.0, r.forcing, None, lambda2_per_mode=r.lambda2)
             sp = [0] + list(range(2, r.nz)) if r.nz > 1 else [0]
             worst = max(worst, rel_err(u[sp], uo[sp])[0])
@@ -890,6 +957,9 @@ def main():
     ap.add_argument("--serve-only", type=int, default=0, metavar="N",
                     help="run only the serving loop on the first N requests of the config-4 stream "
                          "and print its JSON (not a bench line)")
+    ap.add_argument("--serve-precision", choices=["mixed", "fp64"], default="mixed",
+                    help="serving loop: mixed (per mode FP32 CG or FP64 band) or fp64 (band for every mode)")
+    ap.add_argument("--serve-slots", type=int, default=4, help="serving loop: requests on the device at once")
     ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
@@ -903,7 +973,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.serve_only > 0:
-        print(json.dumps({"serving_only": run_serving(args.serve_only, check_oracle=False)}), flush=True)
+        print(json.dumps({"serving_only": run_serving(args.serve_only, check_oracle=False,
+                                                      precision=args.serve_precision, slots=args.serve_slots)}),
+              flush=True)
         return
     if args.profile:
         run_profile(args)

@@ -498,14 +498,16 @@ int sx::cg_round_iters(double kratio, double hcon) {
 }
 
 bool sx::band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon,
-                      int n_inner, double tol_rel, int max_refine, double reuse) {
+                      int n_inner, double tol_rel, int max_refine, double reuse, double iter_floor_s,
+                      double iter_factor) {
   const int per_round = std::max(std::max(n_inner, 1), cg_round_iters(kratio, hcon));
   if (per_round > CG_ROUND_CAP) return true;
   const int nn = np * np, next = 4 * (np - 1), nint = nn - next;
   const double rounds = std::max(1.0, std::ceil(-std::log10(std::max(tol_rel, 1e-15)) / 6.0));
   if (rounds > max_refine) return true;
   const double npts = nglobal + (double)nel * nint;
-  const double cg_s = rounds * per_round * 2.0 * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn) / 2.1e12;
+  const double iter_s = std::max(iter_floor_s, 2.0 * 4.0 * (8.0 * npts + 2.0 * (double)nel * nn) / 2.1e12);
+  const double cg_s = rounds * per_round * iter_factor * iter_s;
   const double band_s =
       (2.0 * nsolve * (double)nband * 8.0 + (double)nel * ((double)next * nint + (double)nint * nint) * 8.0) /
       1.9e12;

@@ -282,9 +282,12 @@ int cg_round_iters(double kratio, double hcon);
 // above -- the serving stream ran slower (makespan 7.2-7.7 s against
 // 5.3-7.8 s in an A/B on one box), so the calibrated pair stays.
 // A mode whose rounds would exceed CG_ROUND_CAP iterations, or whose CG would
-// need more than max_refine rounds, goes to the band.
+// need more than max_refine rounds, goes to the band.  iter_floor_s is the
+// least time an FP32 iteration takes whatever its bytes (a launch and, when
+// the iterations are not replayed from a captured graph, the host's issue
+// of it), iter_factor a margin on the iteration model.
 bool band_cheaper(int np, int nel, int nglobal, int nsolve, int nband, double kratio, double hcon, int n_inner,
-                  double tol_rel, int max_refine, double reuse);
+                  double tol_rel, int max_refine, double reuse, double iter_floor_s = 0.0, double iter_factor = 1.0);
 
 // Solve workspace for up to `planes` planes of one system.
 struct Work {

@@ -105,6 +105,9 @@ struct SysEntry {
   bool ready = false, failed = false;
 };
 
+// Least time of one FP32 iteration of a serving batch (a launch from the host).
+constexpr double SERVE_ITER_S = 12e-6;
+
 size_t mesh_estimate(const MeshCopy &m) {
   const size_t nn = (size_t)m.np * m.np, next = 4 * (m.np - 1);
   return (size_t)m.nel * nn * (5 * 8 + 4 * 4 + 16 + 1) + (size_t)m.nel * next * (4 * 3 + 16) +
@@ -199,8 +202,15 @@ struct sx_server_s {
     std::memcpy(&a, &lam, 8);
     std::memcpy(&b, &bk2, 8);
     if (systems.count(std::make_tuple(m.key, a, b, (int)SX_DIRECT))) return SX_DIRECT;
+    // The serving loop's FP32 iterations are launched one by one from the
+    // host (a batch's member set changes from batch to batch, so nothing is
+    // captured) with the host checking every round: at least SERVE_ITER_S
+    // an iteration, and the iteration model is charged twice over (measured
+    // on serving-sized meshes, lambda2 = 10 + k^2: 32 x 32, N = 7, 32 modes:
+    // Jacobi-CG 124 ms against a band build of 93 ms and a 3 ms solve;
+    // 64 x 64, N = 10, 64 modes: 6.5 s against 3.3 s and 45 ms).
     return band_cheaper(m.np, m.nel, m.nglobal, m.nsolve, m.nband, m.kratio, lam + bk2, cfg.inner_iters,
-                        cfg.tol_rel, cfg.max_refine, 1.0)
+                        cfg.tol_rel, cfg.max_refine, 1.0, SERVE_ITER_S, 2.0)
                ? SX_DIRECT
                : SX_JACPCG;
   }

@@ -240,37 +240,41 @@ def number_mesh(np_, elem_vids, canon, essential_sides, renumber="rcm"):
                      "none" (naive element-traverse order)
 
     Returns btog, bmask (nel, next), nglobal, nsolve, nband.
+
+    Each element boundary slot gets a code: a vertex its canonical id, the
+    t-th interior node of an edge (t counted from the edge's lower vertex)
+    nv + edge id (nm - 1) + t - 1.  Global ids are given in order of first
+    appearance over elements and their slots (Side::connect's traverse
+    order), essential nodes are moved last (sortGid), then the solve nodes
+    are renumbered by RCM over the element coupling graph.
     """
     nel = elem_vids.shape[0]
     nm = np_ - 1
     next_ = 4 * nm
-    keys = np.empty((nel, next_), dtype=object)
-    for e in range(nel):
-        k = 0
-        for s in range(4):
-            p = canon[elem_vids[e, s]]
-            q = canon[elem_vids[e, (s + 1) % 4]]
-            keys[e, k] = ("v", p)
-            k += 1
-            lo, hi = (p, q) if p < q else (q, p)
-            for t in range(1, nm):
-                tt = t if p < q else nm - t
-                keys[e, k] = ("e", lo, hi, tt)
-                k += 1
+    canon = np.asarray(canon, dtype=np.int64)
+    nv = int(canon.max()) + 1 if canon.size else 0
+    P = canon[np.asarray(elem_vids, dtype=np.int64)]   # side start vertex, (nel, 4)
+    Q = np.roll(P, -1, axis=1)                          # side end vertex
+    lo, hi = np.minimum(P, Q), np.maximum(P, Q)
+    _, eid = np.unique(lo * max(nv, 1) + hi, return_inverse=True)
+    eid = eid.reshape(nel, 4)
+    codes = np.empty((nel, 4, nm), dtype=np.int64)
+    codes[:, :, 0] = P
+    if nm > 1:
+        t = np.arange(1, nm, dtype=np.int64)[None, None, :]
+        tt = np.where((P < Q)[:, :, None], t, nm - t)
+        codes[:, :, 1:] = nv + eid[:, :, None] * (nm - 1) + (tt - 1)
     # naive numbering in element/side traverse order (Side::connect)
-    gid = {}
-    btog = np.empty((nel, next_), dtype=np.int64)
-    for e in range(nel):
-        for k in range(next_):
-            key = keys[e, k]
-            if key not in gid:
-                gid[key] = len(gid)
-            btog[e, k] = gid[key]
-    nglobal = len(gid)
+    uc, first, inv = np.unique(codes.reshape(-1), return_index=True, return_inverse=True)
+    rank = np.empty(len(uc), dtype=np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(uc))
+    btog = rank[inv].reshape(nel, next_)
+    nglobal = len(uc)
     ess = np.zeros(nglobal, dtype=bool)
-    for (e, s) in essential_sides:
-        for k in range(s * nm, s * nm + np_):
-            ess[btog[e, k % next_]] = True
+    if essential_sides:
+        es = np.array(sorted(essential_sides), dtype=np.int64).reshape(-1, 2)
+        ks = (es[:, 1:2] * nm + np.arange(np_)[None, :]) % next_
+        ess[btog[es[:, 0:1], ks]] = True
     # sortGid: unknowns first, each partition in ascending naive order
     unknown = np.flatnonzero(~ess)
     known = np.flatnonzero(ess)
@@ -280,27 +284,58 @@ def number_mesh(np_, elem_vids, canon, essential_sides, renumber="rcm"):
     new[known] = nsolve + np.arange(len(known))
     btog = new[btog]
     if renumber == "rcm" and nsolve > 0:
-        rows, cols = [], []
-        for e in range(nel):
-            g = np.unique(btog[e][btog[e] < nsolve])
-            rr, cc = np.meshgrid(g, g, indexing="ij")
-            rows.append(rr.ravel())
-            cols.append(cc.ravel())
-        rows = np.concatenate(rows)
-        cols = np.concatenate(cols)
+        solve = btog < nsolve
+        pair = solve[:, :, None] & solve[:, None, :]
+        rows = np.broadcast_to(btog[:, :, None], pair.shape)[pair]
+        cols = np.broadcast_to(btog[:, None, :], pair.shape)[pair]
         perm = _rcm_order(rows, cols, nsolve)
-        inv = np.empty(nglobal, dtype=np.int64)
-        inv[perm] = np.arange(nsolve)
-        inv[nsolve:] = np.arange(nsolve, nglobal)
-        btog = inv[btog]
+        inv2 = np.empty(nglobal, dtype=np.int64)
+        inv2[perm] = np.arange(nsolve)
+        inv2[nsolve:] = np.arange(nsolve, nglobal)
+        btog = inv2[btog]
     bmask = (btog >= nsolve).astype(np.int32)
+    solve = bmask == 0
     nband = 0
-    for e in range(nel):
-        g = btog[e][bmask[e] == 0]
-        if len(g):
-            nband = max(nband, int(g.max() - g.min()))
+    if solve.any():
+        gmax = np.where(solve, btog, -1).max(axis=1)
+        gmin = np.where(solve, btog, np.iinfo(np.int64).max).min(axis=1)
+        has = solve.any(axis=1)
+        nband = int((gmax[has] - gmin[has]).max())
     nband += 1
     return btog.astype(np.int32), bmask, nglobal, nsolve, nband
+
+
+def elements_nodes(np_: int, z: np.ndarray, vx: np.ndarray, vy: np.ndarray):
+    """element_nodes for every element at once: vx, vy (nel, 4) -> X, Y
+    (nel, np, np), the same arithmetic element by element."""
+    nel = vx.shape[0]
+    nm = np_ - 1
+    X = np.zeros((nel, np_, np_))
+    Y = np.zeros((nel, np_, np_))
+    for s in range(4):
+        sp = z if s < 2 else -z[::-1]
+        for A, V in ((X, vx), (Y, vy)):
+            v1 = V[:, s][:, None]
+            v2 = V[:, (s + 1) % 4][:, None]
+            pv = v1 + (v2 - v1) * 0.5 * (sp + 1.0)[None, :]
+            if s == 0:
+                A[:, 0, 0:nm] = pv[:, :nm]
+            elif s == 1:
+                A[:, 0:nm, nm] = pv[:, :nm]
+            elif s == 2:
+                A[:, nm, nm:0:-1] = pv[:, :nm]
+            else:
+                A[:, nm:0:-1, 0] = pv[:, :nm]
+    zr = z[None, None, 1:nm]
+    zs = z[None, 1:nm, None]
+    for a in (X, Y):
+        a[:, 1:nm, 1:nm] = (0.50 * ((1.0 - zr) * a[:, 1:nm, 0:1] + (1.0 + zr) * a[:, 1:nm, nm:nm + 1]
+                                    + (1.0 - zs) * a[:, 0:1, 1:nm] + (1.0 + zs) * a[:, nm:nm + 1, 1:nm])
+                            - 0.25 * ((1.0 - zr) * (1.0 - zs) * a[:, 0:1, 0:1]
+                                      + (1.0 - zr) * (1.0 + zs) * a[:, nm:nm + 1, 0:1]
+                                      + (1.0 - zs) * (1.0 + zr) * a[:, 0:1, nm:nm + 1]
+                                      + (1.0 + zs) * (1.0 + zr) * a[:, nm:nm + 1, nm:nm + 1]))
+    return X, Y
 
 
 def rect_mesh(nx, ny, np_, x0=0.0, x1=1.0, y0=0.0, y1=1.0, jitter=0.0, seed=None,
@@ -343,16 +378,13 @@ def rect_mesh(nx, ny, np_, x0=0.0, x1=1.0, y0=0.0, y1=1.0, jitter=0.0, seed=None
         for j in range(ny + 1):
             canon[vid(nx, j)] = vid(0, j)
     nel = nx * ny
-    evids = np.zeros((nel, 4), dtype=np.int64)
-    vx = np.zeros((nel, 4))
-    vy = np.zeros((nel, 4))
-    for j in range(ny):
-        for i in range(nx):
-            e = j * nx + i
-            corners = [(i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)]
-            evids[e] = [vid(a, b) for a, b in corners]
-            vx[e] = [VX[b, a] for a, b in corners]
-            vy[e] = [VY[b, a] for a, b in corners]
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    ii, jj = ii.ravel(), jj.ravel()                      # element e = j nx + i
+    ci = np.stack([ii, ii + 1, ii + 1, ii], axis=1)      # CCW corners
+    cj = np.stack([jj, jj, jj + 1, jj + 1], axis=1)
+    evids = (cj * (nx + 1) + ci).astype(np.int64)
+    vx = np.asarray(VX)[cj, ci].astype(np.float64)
+    vy = np.asarray(VY)[cj, ci].astype(np.float64)
     bnds = []
 
     def add(side_name, e, s):
@@ -377,8 +409,5 @@ def rect_mesh(nx, ny, np_, x0=0.0, x1=1.0, y0=0.0, y1=1.0, jitter=0.0, seed=None
     ess = {(b.elmt, b.side) for b in bnds if b.kind == ESSENTIAL}
     btog, bmask, nglobal, nsolve, nband = number_mesh(np_, evids, canon, ess, renumber)
     z = gll_points(np_)
-    X = np.zeros((nel, np_, np_))
-    Y = np.zeros((nel, np_, np_))
-    for e in range(nel):
-        X[e], Y[e] = element_nodes(np_, z, vx[e], vy[e])
+    X, Y = elements_nodes(np_, z, vx, vy)
     return QuadMesh(np_, nel, X, Y, btog, bmask, nglobal, nsolve, nband, bnds, vx, vy)

@@ -64,14 +64,16 @@ class Workload:
 def scatter_global(m: QuadMesh, gvals: np.ndarray) -> np.ndarray:
     """Continuous field from values per unique node: gvals has
     nglobal + nel*nint entries (element-boundary globals first, then each
-    element's interior nodes in edge-map order); returns the element plane."""
+    element's interior nodes in edge-map order); returns the element plane.
+    A leading axis of gvals (planes) is kept: (..., n) -> (..., nplane)."""
     emap, _ = edge_maps(m.np)
-    out = np.zeros((m.nel, m.npnp))
-    bvals = gvals[: m.nglobal][m.btog]                        # (nel, next)
-    ivals = gvals[m.nglobal:].reshape(m.nel, m.nint)          # (nel, nint)
-    out[:, emap[: m.next]] = bvals
-    out[:, emap[m.next:]] = ivals
-    return out.reshape(-1)
+    # source of every element-plane value: a boundary slot's global node, or
+    # the element's own interior node
+    src = np.empty((m.nel, m.npnp), dtype=np.int64)
+    src[:, emap[: m.next]] = m.btog
+    src[:, emap[m.next:]] = m.nglobal + np.arange(m.nel * m.nint, dtype=np.int64).reshape(m.nel, m.nint)
+    g = np.asarray(gvals)
+    return np.take(g, src.reshape(-1), axis=-1)
 
 
 def _jittered_channel(nx, ny, np_, jitter, seed, lx=2 * np.pi):
@@ -93,11 +95,11 @@ def fourier_forcing(m: QuadMesh, nz: int, rng, decay=8.0):
     node, Re and Im planes independent, scattered continuously."""
     n = m.n_unique
     f = np.zeros((nz, m.nplane))
-    for plane in range(nz):
-        if plane == 1 and nz > 1:
-            continue
-        k = plane >> 1
-        f[plane] = scatter_global(m, rng.standard_normal(n) * np.exp(-k / decay))
+    planes = [p for p in range(nz) if not (p == 1 and nz > 1)]   # the Nyquist plane stays zero
+    # one draw for every plane is the same stream as one draw per plane in turn
+    g = rng.standard_normal((len(planes), n))
+    g *= np.exp(-(np.array(planes) >> 1) / decay)[:, None]
+    f[planes] = scatter_global(m, g)
     return f
 
 
@@ -220,27 +222,53 @@ class ServeRequest:
         return self.mesh.n_unique * (1 if self.nz == 1 else self.nz - 1)
 
 
-def serving_trace(n_requests, seed=4, rate=2000.0):
-    """Mixed-size request stream (config 4): Poisson arrivals at `rate`/s;
-    each request a straight-sided E_x x E_y quad mesh of [0,1]^2 with E_x,
-    E_y uniform in [2, 64], order N uniform in {4..10}, a mode count uniform
-    in [1, 64], lambda2 log-uniform in [1e-2, 1e4] (plus k^2 per mode, beta =
-    1), seeded Gaussian Fourier forcing, Dirichlet on every side.  The first
-    `n_requests` requests of the seeded stream."""
+@dataclass
+class ServeSpec:
+    """One request of the serving stream before its mesh and forcing are built."""
+    index: int
+    t_arrival: float
+    ex: int
+    ey: int
+    order: int
+    modes: int
+    lam: float
+
+
+def serving_plan(n_requests, seed=4, rate=2000.0):
+    """The mixed-size request stream (config 4): Poisson arrivals at
+    `rate`/s; each request a straight-sided E_x x E_y quad mesh of [0,1]^2
+    with E_x, E_y uniform in [2, 64], order N uniform in {4..10}, a mode count
+    uniform in [1, 64], lambda2 log-uniform in [1e-2, 1e4] (plus k^2 per
+    mode, beta = 1), Dirichlet on every side.  The sizes, constants and
+    arrival times of the first `n_requests` come from one seeded stream."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
-    for _ in range(n_requests):
+    for i in range(n_requests):
         ex, ey = (int(v) for v in rng.integers(2, 65, size=2))
         order = int(rng.integers(4, 11))
         modes = int(rng.integers(1, 65))
         lam = float(np.exp(rng.uniform(np.log(1e-2), np.log(1e4))))
-        m = rect_mesh(ex, ey, order + 1, 0.0, 1.0, 0.0, 1.0)
-        nz = 1 if modes == 1 else 2 * modes
-        f = fourier_forcing(m, nz, rng)
-        out.append(ServeRequest(t, m, np.full(modes, lam), np.arange(modes, dtype=np.float64) ** 2, f))
+        out.append(ServeSpec(i, t, ex, ey, order, modes, lam))
         t += float(rng.exponential(1.0 / rate))
     return out
+
+
+def serving_request(spec: ServeSpec, seed=4) -> ServeRequest:
+    """Build one planned request: its mesh and seeded Gaussian Fourier
+    forcing (fourier_forcing, from the request's own stream (seed, index), so
+    that requests can be built in any order or in parallel)."""
+    m = rect_mesh(spec.ex, spec.ey, spec.order + 1, 0.0, 1.0, 0.0, 1.0)
+    nz = 1 if spec.modes == 1 else 2 * spec.modes
+    f = fourier_forcing(m, nz, np.random.default_rng([seed, spec.index]))
+    return ServeRequest(spec.t_arrival, m, np.full(spec.modes, spec.lam),
+                        np.arange(spec.modes, dtype=np.float64) ** 2, f)
+
+
+def serving_trace(n_requests, seed=4, rate=2000.0):
+    """The first `n_requests` of the serving stream, built (serving_plan,
+    serving_request)."""
+    return [serving_request(s, seed) for s in serving_plan(n_requests, seed, rate)]
 
 
 def small_mesh_mix(n_meshes=24, seed=9):

@@ -24,3 +24,14 @@ def test_serving_trace_shapes_and_ranges():
     # seeded: the same stream twice
     again = serving_trace(6, seed=4)
     assert all(np.array_equal(a.forcing, b.forcing) for a, b in zip(tr, again))
+
+
+def test_serving_requests_build_in_any_order():
+    from semtex_b200.workloads import serving_plan, serving_request
+    plan = serving_plan(5, seed=4)
+    fwd = [serving_request(s) for s in plan]
+    rev = [serving_request(s) for s in reversed(plan)][::-1]
+    assert all(np.array_equal(a.forcing, b.forcing) and a.t_arrival == b.t_arrival for a, b in zip(fwd, rev))
+    # a plan is a prefix of a longer plan
+    assert [(s.ex, s.ey, s.order, s.modes, s.lam) for s in serving_plan(3)] == \
+        [(s.ex, s.ey, s.order, s.modes, s.lam) for s in plan[:3]]
