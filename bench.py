@@ -841,6 +841,9 @@ def run_serving(n_requests, check_oracle=True, precision="mixed", slots=4, windo
         pool.terminate()
     lat = np.array([(results[k][1] - plan[k].t_arrival) * 1e3 for k in range(n_requests)])
     ok = sum(1 for s, _ in results if s == sx.OK)
+    statuses = {}
+    for s_, _ in results:
+        statuses[sx.status_string(s_)] = statuses.get(sx.status_string(s_), 0) + 1
     out = {"requests": n_requests,
            "trace": "cfg4: E_x,E_y~U[2,64], N~U{4..10}, modes~U[1,64], lambda2~logU[1e-2,1e4], Poisson 2000/s "
                     "(plan seed 4; request k's forcing from seed (4, k))",
@@ -852,7 +855,8 @@ def run_serving(n_requests, check_oracle=True, precision="mixed", slots=4, windo
            "mean_ms": float(lat.mean()), "makespan_s": makespan,
            "throughput_dof_solves_per_s": dofs / makespan, "requests_per_s": n_requests / makespan,
            "arrival_window_s": plan[-1].t_arrival, "in_server_window": window,
-           "converged_to_1e-12": ok, "mesh_hits": st["mesh_hits"], "system_misses": st["system_misses"],
+           "converged_to_1e-12": ok, "statuses": statuses, "failed": st["failed"],
+           "mesh_hits": st["mesh_hits"], "system_misses": st["system_misses"],
            "evictions": st["evictions"], "max_batch": 8, "batches": st["batches"],
            "mean_batch": st["completed"] / max(st["batches"], 1),
            # per request, averaged, as the server sees them: waiting for

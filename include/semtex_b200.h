@@ -290,6 +290,57 @@ SX_API int sx_profile_mixed_iterations(sx_modal modal, int reps, void *stream);
  * once, other lengths (which share a workspace) are waited for. */
 SX_API int sx_transform_z(double *d_data, int nz, int plane_stride, int npts, int sign, void *stream);
 
+/* ---- field files: replace the Header writer and AuxField stream I/O -------
+ * The reference's field-file format: a 10-line ASCII header (Header <<,
+ * src/data2df.cpp:503-535; read by strm>>Domain, src/domain.cpp:284-400, and
+ * by compare, utility/compare.cpp:112-175) and the fields' planes in binary,
+ * field after field, plane after plane, nel*np*np doubles each
+ * (ostream<<AuxField / istream>>AuxField, src/auxfield.cpp:997-1095).  Host
+ * memory, planes plane_stride doubles apart (the padding of a plane read is
+ * zeroed).  A file written on a machine of the other byte order is swapped
+ * on reading (Domain's reader does the same). */
+typedef struct {
+  char session[256];  /* session name                                            */
+  int np, nz, nel;    /* knots per element side, planes, elements                */
+  int step;           /* time step number                                        */
+  double time, dt, kinvis, beta;
+  char fields[64];    /* one character per field, in file order, e.g. "uvwp"     */
+  int swapped;        /* set by the readers: the file's byte order is not ours   */
+} sx_field_header;
+/* Write len(h->fields) fields, fields[f] = nz planes. */
+SX_API int sx_field_write(const char *path, const sx_field_header *h, const double *const *fields,
+                          int plane_stride);
+SX_API int sx_field_read_header(const char *path, sx_field_header *h);
+/* Read every field of the file into fields[f] (NULL skips field f). */
+SX_API int sx_field_read(const char *path, sx_field_header *h, double *const *fields, int plane_stride);
+/* compare-style norms of exact - computed on the GPU (device pointers, nz
+ * planes of `mesh`): norms[2z] = max |exact - computed| over plane z (compare's
+ * norm_inf, utility/compare.cpp:206-218), norms[2z+1] = AuxField::errors' L2
+ * figure (src/auxfield.cpp:813-860: the elements' sqrt(sum e^2 Q4) summed,
+ * over the summed element areas) at the fields' own GLL points.  norms is
+ * host memory; the call waits for the result. */
+SX_API int sx_field_norms(sx_mesh mesh, const double *d_computed, const double *d_exact, int nz,
+                          int plane_stride, double *norms, void *stream);
+
+/* ---- numbering files: replace BCmgr::buildnum's reader and enumerate's writer
+ * The text file session.num (written by enumerate, printup in
+ * utility/enumerate.cpp:426-537; read by BCmgr::buildnum, src/bcmgr.cpp:586-
+ * 790): per number set NEL, NP_MAX, NEXT_MAX, NINT_MAX, NTOTAL, NBOUNDARY,
+ * NGLOBAL, NSOLVE, OPTIMIZATION, BANDWIDTH (diagonal included), then per
+ * element boundary slot (element, side, offset) the bmap (btog) and mask of
+ * each set -- the same layout as sx_mesh_desc's btog and bmask.
+ * sx_numbering_read takes the set whose name holds `field` (e.g. 'u' from set
+ * "uv"), checks NEL, NP_MAX and NBOUNDARY against nel and np as the reader
+ * does (SX_ERR_ARG on a mismatch), fills btog and bmask (nel*4*(np-1) each)
+ * and returns NGLOBAL, NSOLVE, BANDWIDTH and the set's name (set_fields may be
+ * NULL). */
+SX_API int sx_numbering_read(const char *path, char field, int nel, int np, int *btog, int *bmask, int *nglobal,
+                             int *nsolve, int *nband, char *set_fields, int set_fields_cap);
+/* Write nset number sets in enumerate's layout (btog[j], bmask[j] of set j). */
+SX_API int sx_numbering_write(const char *path, const char *fields, int nset, const char *const *set_fields,
+                              int nel, int np, const int *const *btog, const int *const *bmask,
+                              const int *nglobal, const int *nsolve, const int *nband, int optimization);
+
 /* ---- multi-mesh batch (no reference counterpart) --------------------------
  * Solves the planes of several modal systems -- different meshes, element
  * counts, orders and mode sets -- together, on device buffers.  Each is the
@@ -327,7 +378,7 @@ SX_API int sx_batch_destroy(sx_batch batch);
 typedef struct sx_server_s *sx_server;
 
 typedef struct {
-  unsigned long long hbm_budget; /* device bytes for caches + in-flight work; 0 = 80% of free */
+  unsigned long long hbm_budget; /* device bytes for caches + in-flight work; 0 = 70% of free */
   int slots;                     /* requests on the device at once; 0 = 4                      */
   int precision;                 /* SX_MIXED_FP32 (PCG) or SX_FP64 (DIRECT, cached factors)     */
   double tol_rel;                /* mixed: FP64 relative residual target; 0 = 1e-12            */

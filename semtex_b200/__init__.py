@@ -103,6 +103,18 @@ if not os.path.exists(LIB_PATH):
                       "(no CPU fallback exists)")
 
 
+class FieldHeader(C.Structure):
+    _fields_ = [("session", C.c_char * 256), ("np", C.c_int), ("nz", C.c_int), ("nel", C.c_int),
+                ("step", C.c_int), ("time", C.c_double), ("dt", C.c_double), ("kinvis", C.c_double),
+                ("beta", C.c_double), ("fields", C.c_char * 64), ("swapped", C.c_int)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["session"] = self.session.decode()
+        d["fields"] = self.fields.decode()
+        return d
+
+
 def _load():
     L = C.CDLL(LIB_PATH)
     vp, ip, dp = C.c_void_p, C.c_int, C.c_double
@@ -134,6 +146,10 @@ def _load():
     L.sx_modal_tune.argtypes = [vp, ip, ip]
     L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
     L.sx_transform_z.argtypes = [vp, ip, ip, ip, ip, vp]
+    L.sx_field_write.argtypes = [C.c_char_p, P(FieldHeader), P(P(dp)), ip]
+    L.sx_field_read_header.argtypes = [C.c_char_p, P(FieldHeader)]
+    L.sx_field_read.argtypes = [C.c_char_p, P(FieldHeader), P(P(dp)), ip]
+    L.sx_field_norms.argtypes = [vp, vp, vp, ip, ip, P(dp), vp]
     L.sx_batch_create.argtypes = [P(vp)]
     L.sx_batch_destroy.argtypes = [vp]
     L.sx_batch_solve.argtypes = [vp, ip, P(vp), P(vp), P(vp), P(vp), P(ip), P(ip), ip, dp, ip, vp,
@@ -377,6 +393,37 @@ def transform_z(d_data, nz, plane_stride, npts=None, sign=1, stream=0):
     plane order), sign=-1 back."""
     _check(lib.sx_transform_z(d_data, nz, plane_stride, plane_stride if npts is None else npts, sign, stream),
            "sx_transform_z")
+
+
+def write_field(path, fields, np_, nel, session="semtex_b200", step=0, time=0.0, dt=0.0, kinvis=0.0,
+                beta=0.0):
+    """Write a field file in the reference's format (sx_field_write).
+    fields: {name (one character): (nz, nel*np*np) array}, in file order."""
+    names = "".join(fields)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1, nel * np_ * np_) for a in fields.values()]
+    nz = arrs[0].shape[0]
+    h = FieldHeader(session.encode()[:255], np_, nz, nel, step, time, dt, kinvis, beta, names.encode(), 0)
+    ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_dptr(a) for a in arrs])
+    _check(lib.sx_field_write(str(path).encode(), C.byref(h), ptrs, nel * np_ * np_), "sx_field_write")
+
+
+def read_field(path):
+    """Read a field file (sx_field_read): (header dict, {name: (nz, nel*np*np) array})."""
+    h = FieldHeader()
+    _check(lib.sx_field_read_header(str(path).encode(), C.byref(h)), "sx_field_read_header")
+    n = h.nel * h.np * h.np
+    arrs = [np.zeros((h.nz, n)) for _ in h.fields.decode()]
+    ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_dptr(a) for a in arrs])
+    _check(lib.sx_field_read(str(path).encode(), C.byref(h), ptrs, n), "sx_field_read")
+    return h.as_dict(), dict(zip(h.fields.decode(), arrs))
+
+
+def field_norms(mesh, d_computed, d_exact, nz, stride, stream=0):
+    """compare-style norms of exact - computed per plane on the GPU
+    (sx_field_norms): array (nz, 2) of (inf, L2)."""
+    out = np.zeros(2 * nz)
+    _check(lib.sx_field_norms(mesh.h, d_computed, d_exact, nz, stride, _dptr(out), stream), "sx_field_norms")
+    return out.reshape(nz, 2)
 
 
 class Batch:

@@ -182,6 +182,22 @@ struct sx_server_s {
     if (step > 0 && cudaMallocFromPoolAsync(&p, step, mem_pool, stream) == cudaSuccess) cudaFreeAsync(p, stream);
     cudaGetLastError();  // best effort: the pool still grows on demand
   }
+  // After a batch: requests of many sizes leave the pool fragmented, and
+  // it grows by new mappings where a free run is too short; once its
+  // reserved memory passes the budget, hand the unused part back (the
+  // allocations in use stay), so that the device never fills up with free
+  // pool memory that a plain cudaMalloc (mesh tables) cannot use.
+  void trim_pool(cudaStream_t stream) {
+    uint64_t reserved = 0;
+    if (cudaMemPoolGetAttribute(mem_pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    if (reserved <= cfg.hbm_budget) return;
+    cudaStreamSynchronize(stream);  // this slot's frees are complete
+    cudaMemPoolTrimTo(mem_pool, (size_t)(0.75 * (double)cfg.hbm_budget));
+    cudaGetLastError();
+  }
   ~sx_server_s() {
     systems.clear();
     meshes.clear();
@@ -216,6 +232,15 @@ struct sx_server_s {
   }
   bool admissible(Req *r, size_t &need);
   void evict_for(size_t need, uint64_t keep_mesh);
+  // After a batch (caller holds mu): the cache keeps at most a quarter of the
+  // budget of entries no request is using.  A stream whose requests rarely
+  // share a system (each carries its own lambda2) gains nothing from a full
+  // cache, and a pool that holds the whole budget in systems of every size
+  // fragments until its reserved memory fills the device.
+  void trim_cache() {
+    const size_t budget = (size_t)cfg.hbm_budget, cap = budget / 4;
+    if (bytes_cached > cap) evict_for(budget - cap - std::min(bytes_reserved, budget - cap), 0);
+  }
   void worker(int slot);
   using SysKey = std::tuple<uint64_t, uint64_t, uint64_t, int>;
   // One request's mesh and systems.
@@ -249,13 +274,37 @@ bool sx_server_s::admissible(Req *r, size_t &need) {
   need = work_estimate(r->mesh, r->nz, cfg.precision);
   if (!meshes.count(r->mesh.key)) need += mesh_estimate(r->mesh);
   r->kinds.resize(r->num_modes);
-  for (int l = 0; l < r->num_modes; l++) {
-    const int kind = r->kinds[l] = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
+  for (int l = 0; l < r->num_modes; l++) r->kinds[l] = mode_kind(r->mesh, r->lam[l], r->bk2[l]);
+  // One request's new band factors may take at most a quarter of the budget
+  // (the largest request of the serving stream, 64 x 64 elements at N = 10
+  // with 64 modes, would need ~113 GB): past that, the modes with the
+  // largest Helmholtz constant, whose FP32 iterations converge fastest, go to
+  // the iterations instead (mixed precision only; the FP64 server refuses
+  // what cannot fit).
+  auto key_of = [&](int l, int kind) {
     uint64_t a, b;
     std::memcpy(&a, &r->lam[l], 8);
     std::memcpy(&b, &r->bk2[l], 8);
-    if (!systems.count(std::make_tuple(r->mesh.key, a, b, kind))) need += system_estimate(r->mesh, kind);
+    return std::make_tuple(r->mesh.key, a, b, kind);
+  };
+  if (cfg.precision == SX_MIXED_FP32) {
+    const size_t cap = cfg.hbm_budget / 4, per = system_estimate(r->mesh, SX_DIRECT);
+    size_t band = 0;
+    std::vector<int> order;
+    for (int l = 0; l < r->num_modes; l++)
+      if (r->kinds[l] == SX_DIRECT && !systems.count(key_of(l, SX_DIRECT))) {
+        band += per;
+        order.push_back(l);
+      }
+    std::sort(order.begin(), order.end(),
+              [&](int a, int b) { return r->lam[a] + r->bk2[a] > r->lam[b] + r->bk2[b]; });
+    for (size_t i = 0; i < order.size() && band > cap; i++) {
+      r->kinds[order[i]] = SX_JACPCG;
+      band -= per;
+    }
   }
+  for (int l = 0; l < r->num_modes; l++)
+    if (!systems.count(key_of(l, r->kinds[l]))) need += system_estimate(r->mesh, r->kinds[l]);
   return bytes_cached + bytes_reserved + need <= cfg.hbm_budget;
 }
 
@@ -574,10 +623,18 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
     release(batch[i], prep[i]);
     batch[i]->status = rc[i];
   }
-  // keep small workspaces for the next batch, free the large ones
-  for (int i = 0; i < n; i++)
-    if (pool[i]->bytes > KEEP_WS_BYTES) pool[i].reset(new Member());
+  // keep small workspaces for the next batch, free the large ones; a kept
+  // workspace lets go of the request's systems (it would otherwise keep
+  // them alive after the cache has evicted them and stopped counting them)
+  for (int i = 0; i < n; i++) {
+    if (pool[i]->bytes > KEEP_WS_BYTES)
+      pool[i].reset(new Member());
+    else if (pool[i]->ws)
+      pool[i]->ws->rebind(nullptr, 0, 0, pool[i]->ws->method, {});
+  }
+  trim_pool(stream);
   std::lock_guard<std::mutex> lk(mu);
+  trim_cache();
   st.batches++;
   auto ms = [](Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
@@ -591,11 +648,19 @@ void sx_server_s::serve_batch(std::vector<Req *> &batch, std::vector<std::unique
       dm += p.direct_ms;
       jm += p.jacobi_ms;
     }
+    size_t fr = 0, tot = 0;
+    uint64_t pres = 0, pused = 0;
+    cudaMemGetInfo(&fr, &tot);
+    cudaMemPoolGetAttribute(mem_pool, cudaMemPoolAttrReservedMemCurrent, &pres);
+    cudaMemPoolGetAttribute(mem_pool, cudaMemPoolAttrUsedMemCurrent, &pused);
+    cudaGetLastError();
     std::fprintf(stderr,
                  "sx_server batch %llu: %d requests, t=%.1f ms, build %.1f (meshes %.1f, band systems %.1f, "
-                 "Jacobi %.1f), factor and waits %.1f (%zu systems factored), solve %.1f\n",
+                 "Jacobi %.1f), factor and waits %.1f (%zu systems factored), solve %.1f | device free %.1f GB, "
+                 "pool %.1f / %.1f GB, cached %.1f GB (%zu meshes, %zu systems), reserved %.1f GB\n",
                  (unsigned long long)st.batches, n, ms(t_start, t0), ms(tl, tf), mm, dm, jm, ms(tf, t1), nfactor,
-                 ms(t1, t2));
+                 ms(t1, t2), fr / 1e9, pused / 1e9, pres / 1e9, bytes_cached / 1e9, meshes.size(), systems.size(),
+                 bytes_reserved / 1e9);
     for (int i = 0; i < n; i++)
       if (rc[i] != SX_OK && rc[i] != SX_WARN_STEP_LIMIT)
         std::fprintf(stderr, "sx_server   request %llu failed: status %d (%s)\n", (unsigned long long)batch[i]->id,
@@ -689,7 +754,7 @@ extern "C" int sx_server_create(const sx_server_config *cfg, sx_server *out) {
   if (c.hbm_budget == 0) {
     size_t fr = 0, tot = 0;
     SX_CUDA(cudaMemGetInfo(&fr, &tot));
-    c.hbm_budget = (unsigned long long)(0.8 * fr);
+    c.hbm_budget = (unsigned long long)(0.7 * fr);
   }
   S->st.bytes_budget = c.hbm_budget;
   {
@@ -699,7 +764,11 @@ extern "C" int sx_server_create(const sx_server_config *cfg, sx_server *out) {
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = S->device;
     SX_CUDA(cudaMemPoolCreate(&S->mem_pool, &props));
-    uint64_t keep = ~0ull;  // never hand memory back between requests
+    // hold on to freed memory up to a quarter of the budget (a
+    // sub-allocation from the pool costs microseconds, a fresh mapping up to
+    // a millisecond); above it the pool hands unused memory back at
+    // synchronisation points, for the allocations made outside it
+    uint64_t keep = c.hbm_budget / 4;
     SX_CUDA(cudaMemPoolSetAttribute(S->mem_pool, cudaMemPoolAttrReleaseThreshold, &keep));
   }
   S->trace = std::getenv("SX_SERVER_TRACE") != nullptr;
