@@ -150,6 +150,10 @@ def _load():
     L.sx_field_read_header.argtypes = [C.c_char_p, P(FieldHeader)]
     L.sx_field_read.argtypes = [C.c_char_p, P(FieldHeader), P(P(dp)), ip]
     L.sx_field_norms.argtypes = [vp, vp, vp, ip, ip, P(dp), vp]
+    L.sx_numbering_read.argtypes = [C.c_char_p, C.c_char, ip, ip, P(ip), P(ip), P(ip), P(ip), P(ip),
+                                    C.c_char_p, ip]
+    L.sx_numbering_write.argtypes = [C.c_char_p, C.c_char_p, ip, P(C.c_char_p), ip, ip, P(P(ip)), P(P(ip)),
+                                     P(ip), P(ip), P(ip), ip]
     L.sx_batch_create.argtypes = [P(vp)]
     L.sx_batch_destroy.argtypes = [vp]
     L.sx_batch_solve.argtypes = [vp, ip, P(vp), P(vp), P(vp), P(vp), P(ip), P(ip), ip, dp, ip, vp,
@@ -424,6 +428,48 @@ def field_norms(mesh, d_computed, d_exact, nz, stride, stream=0):
     out = np.zeros(2 * nz)
     _check(lib.sx_field_norms(mesh.h, d_computed, d_exact, nz, stride, _dptr(out), stream), "sx_field_norms")
     return out.reshape(nz, 2)
+
+
+def write_numbering(path, sets, fields=None, optimization=3):
+    """Write a numbering file (session.num) in enumerate's layout
+    (sx_numbering_write).  sets: {set name (e.g. "uv"): QuadMesh}, meshes of
+    one geometry whose btog/bmask/nglobal/nsolve/nband are written."""
+    names = list(sets)
+    ms = [sets[k] for k in names]
+    m0 = ms[0]
+    bt = [np.ascontiguousarray(m.btog, dtype=np.int32).reshape(-1) for m in ms]
+    bm = [np.ascontiguousarray(m.bmask, dtype=np.int32).reshape(-1) for m in ms]
+    n = len(ms)
+    cn = (C.c_char_p * n)(*[k.encode() for k in names])
+    pb = (C.POINTER(C.c_int) * n)(*[_iptr(a) for a in bt])
+    pm = (C.POINTER(C.c_int) * n)(*[_iptr(a) for a in bm])
+    ng = (C.c_int * n)(*[m.nglobal for m in ms])
+    ns = (C.c_int * n)(*[m.nsolve for m in ms])
+    nb = (C.c_int * n)(*[m.nband for m in ms])
+    _check(lib.sx_numbering_write(str(path).encode(), (fields or "".join(names)).encode(), n, cn, m0.nel, m0.np,
+                                  pb, pm, ng, ns, nb, optimization), "sx_numbering_write")
+
+
+def read_numbering(path, field, nel, np_):
+    """Read the number set of `field` from a numbering file
+    (sx_numbering_read): dict of btog, bmask (nel, 4(np-1)), nglobal, nsolve,
+    nband and the set's name."""
+    nx = 4 * (np_ - 1)
+    bt = np.zeros(nel * nx, dtype=np.int32)
+    bm = np.zeros(nel * nx, dtype=np.int32)
+    ng, ns, nb = C.c_int(), C.c_int(), C.c_int()
+    name = C.create_string_buffer(64)
+    _check(lib.sx_numbering_read(str(path).encode(), field.encode(), nel, np_, _iptr(bt), _iptr(bm), C.byref(ng),
+                                 C.byref(ns), C.byref(nb), name, 64), "sx_numbering_read")
+    return {"btog": bt.reshape(nel, nx), "bmask": bm.reshape(nel, nx), "nglobal": ng.value,
+            "nsolve": ns.value, "nband": nb.value, "set": name.value.decode()}
+
+
+def with_numbering(qm: QuadMesh, num):
+    """A copy of mesh qm numbered by `num` (read_numbering's result)."""
+    import dataclasses
+    return dataclasses.replace(qm, btog=num["btog"].astype(np.int32), bmask=num["bmask"].astype(np.int32),
+                               nglobal=num["nglobal"], nsolve=num["nsolve"], nband=num["nband"])
 
 
 class Batch:

@@ -269,6 +269,7 @@ struct Words {
       w.push_back((char)c);
       c = std::fgetc(fp);
     }
+    if (c != EOF) std::ungetc(c, fp);  // the word's end stays, as after `stream >> word`
     return w;
   }
   void rest_of_line() {

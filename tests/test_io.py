@@ -64,3 +64,59 @@ def test_not_a_field_file_is_refused(sx, tmp_path):
     short.write_bytes(short.read_bytes()[:-8])
     with pytest.raises(sx.SolverError):
         sx.read_field(short)
+
+
+def _channel_pair(renumber="rcm"):
+    from semtex_b200.mesh import rect_mesh
+    kw = dict(x0=0.0, x1=2 * np.pi, y0=0.0, y1=1.0, jitter=0.15, seed=2, periodic_x=True, renumber=renumber)
+    mu = rect_mesh(6, 4, 5, bc={"bottom": "D", "top": "D"}, **kw)   # velocity: Dirichlet walls
+    mp = rect_mesh(6, 4, 5, bc={"bottom": "N", "top": "N"}, **kw)   # pressure: natural walls
+    return mu, mp
+
+
+def test_numbering_round_trip_two_sets(sx, tmp_path):
+    """Two number sets, as enumerate writes them for "uvp" (utility/
+    enumerate.cpp:426-537): "uv" with essential walls, "p" without."""
+    mu, mp = _channel_pair()
+    path = tmp_path / "chan.num"
+    sx.write_numbering(path, {"uv": mu, "p": mp}, fields="uvp")
+    text = path.read_text().splitlines()
+    assert text[0].split() == ["#", "FIELDS", ":", "uvp"]
+    assert text[2].split()[:6] == ["#", "2", "NUMBER", "SETS", ":", "uv"]
+    assert text[12].split()[-2:] == [str(mu.nband), str(mp.nband)]   # BANDWIDTH line
+    assert len(text) == 15 + mu.nel * mu.next
+    for field, m in (("v", mu), ("p", mp)):
+        n = sx.read_numbering(path, field, m.nel, m.np)
+        assert np.array_equal(n["btog"], m.btog) and np.array_equal(n["bmask"], m.bmask)
+        assert (n["nglobal"], n["nsolve"], n["nband"]) == (m.nglobal, m.nsolve, m.nband)
+    assert sx.read_numbering(path, "u", mu.nel, mu.np)["set"] == "uv"
+
+
+def test_numbering_checks_like_buildnum(sx, tmp_path):
+    """Mismatches of NEL / NP_MAX and a missing field are refused, as
+    BCmgr::buildnum refuses them (src/bcmgr.cpp:660-750)."""
+    mu, _ = _channel_pair()
+    path = tmp_path / "one.num"
+    sx.write_numbering(path, {"u": mu})
+    with pytest.raises(sx.SolverError, match="number of elements"):
+        sx.read_numbering(path, "u", mu.nel + 1, mu.np)
+    with pytest.raises(sx.SolverError, match="element order"):
+        sx.read_numbering(path, "u", mu.nel, mu.np + 1)
+    with pytest.raises(sx.SolverError, match="no number set"):
+        sx.read_numbering(path, "c", mu.nel, mu.np)
+
+
+def test_numbering_with_free_spacing(sx, tmp_path):
+    """The reader reads words, as the reference's stream extraction does:
+    a file laid out with other column widths reads the same."""
+    mu, _ = _channel_pair(renumber="none")
+    path = tmp_path / "loose.num"
+    rows = [f"{e + 1} {a // (mu.np - 1) + 1} {a % (mu.np - 1)} {mu.btog[e, a]} {mu.bmask[e, a]}"
+            for e in range(mu.nel) for a in range(mu.next)]
+    head = ["# FIELDS : u", "# --", "# 1 NUMBER SETS : u", f"# NEL : {mu.nel}", f"# NP_MAX : {mu.np}",
+            f"# NEXT_MAX : {mu.next}", f"# NINT_MAX : {mu.nint}", f"# NTOTAL : {mu.nel * mu.npnp}",
+            f"# NBOUNDARY : {mu.nel * mu.next}", f"# NGLOBAL : {mu.nglobal}", f"# NSOLVE : {mu.nsolve}",
+            "# OPTIMIZATION : 0", f"# BANDWIDTH : {mu.nband}", "# --", "# elmt side offst bmap mask"]
+    path.write_text("\n".join(head + rows) + "\n")
+    n = sx.read_numbering(path, "u", mu.nel, mu.np)
+    assert np.array_equal(n["btog"], mu.btog) and n["nband"] == mu.nband
