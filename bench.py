@@ -18,7 +18,8 @@ host-pointer C-ABI call with the host<->device copies inside the timed region;
 the plain FP64 mode-by-mode form and the batched FP64 form are reported
 beside it, and the lowest-, median- and highest-lambda2 modes are checked
 against the oracle.  Config 2 (32 x 32, N = 8, nz = 64, lambda2 = 1e6 + k^2),
-the multi-mesh batch, the z-transform and the serving loop are extra keys.
+the multi-mesh batch, the z-transform, the DNS elliptic-phase field
+operations (config 5's field shape) and the serving loop are extra keys.
 
 Multi-GPU (torchrun): Fourier modes are independent, so the modes of a
 64 N-mode problem are split in contiguous blocks of 64 (the reference's mode
@@ -526,6 +527,7 @@ def run_ours(args, rank, world):
         line["config2"] = run_config2(args)
         line["multi_mesh"] = run_multi()
         line["transform_z"] = run_transform()
+        line["dns_elliptic_phase"] = run_dns()
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu,
                                       precision=args.serve_precision, slots=args.serve_slots)
@@ -750,6 +752,111 @@ def run_transform(reps=20):
     return out
 
 
+def _dns_fields(nz, n, count, seed):
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    return [torch.randn((nz, n), dtype=torch.float64, device="cuda", generator=g) for _ in range(count)]
+
+
+def run_dns(reps=5, nz=256, check=True):
+    """The DNS elliptic-phase field operations (waveProp, setPForce, project,
+    Field::smooth, AuxField::gradient) on config 5's field shape: 128 x 64
+    quads jittered +-15 %, N = 10 (8192 elements, 991,232 points a plane),
+    nz = 256 planes -- 2.03 GB a field, every operand larger than L2.
+    Seeded random device fields (synthetic: these operations are linear and
+    their cost does not depend on the values).  CUDA events on the launching
+    stream, median of `reps`; the roofline is each operand read once and each
+    result written once (the partials and numbering, 40 MB, are counted
+    once).  Planes of modes 0, 1 and 127 are checked against the oracle, which
+    is also timed on them (one core)."""
+    import torch
+    import semtex_b200 as sx
+    from semtex_b200.workloads import _jittered_channel
+    torch.cuda.set_device(0)
+    m = _jittered_channel(128, 64, 11, 0.15, 5)
+    mesh = sx.Mesh(m)
+    n, nel, npnp = m.nplane, m.nel, m.npnp
+    f8 = nz * n * 8
+    peak, kind = _peaks()
+    sptr = torch.cuda.current_stream().cuda_stream
+    order, dt, nu, beta = 2, 5e-4, 5e-4, 1.0
+    us = [_dns_fields(nz, n, 3, 50 + q) for q in range(order)]
+    uf = [_dns_fields(nz, n, 3, 60 + q) for q in range(order)]
+    h = _dns_fields(nz, n, 3, 70)
+    p, fp, gx = _dns_fields(nz, n, 3, 80)
+    out3 = [torch.empty_like(p) for _ in range(3)]
+    ptr = lambda ts: [t.data_ptr() for t in ts]  # noqa: E731
+    geo_bytes = 4 * nel * npnp * 8
+    num_bytes = m.nglobal * 8 + m.nglobal * 4 + nel * m.next * 4 + nel * npnp * 8
+    ops = {
+        "wave_prop": (lambda: sx.wave_prop([ptr(x) for x in us], [ptr(x) for x in uf], ptr(h), nz * n, dt,
+                                           stream=sptr),
+                      (2 * order + 1) * 3 * f8, "k_wave_prop"),
+        "pressure_forcing": (lambda: sx.pressure_forcing(mesh, ptr(h), fp.data_ptr(), nz, n, dt, beta, stream=sptr),
+                             4 * f8 + geo_bytes, "k_elem<11, PFORCE>"),
+        "project": (lambda: sx.project(mesh, ptr(h), p.data_ptr(), ptr(out3), nz, n, dt, nu, ndim=3, beta=beta,
+                                       stream=sptr),
+                    7 * f8 + geo_bytes, "k_elem<11, PROJECT>"),
+        "gradient_x": (lambda: sx.field_gradient(mesh, gx.data_ptr(), nz, n, 0, stream=sptr),
+                       2 * f8 + geo_bytes // 2, "k_elem<11, GRAD>"),
+        # the element-boundary values of every plane read and written once
+        "smooth": (lambda: sx.field_smooth(mesh, out3[0].data_ptr(), nz, n, stream=sptr),
+                   2 * nz * nel * m.next * 8 + num_bytes, "k_smooth"),
+    }
+    res = {}
+    for name, (fn, nbytes, kern) in ops.items():
+        fn()  # warm-up
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "algorithmic_bytes": int(nbytes), "achieved_gbs": gbs, "frac": gbs / peak,
+                     "kernel": kern}
+    out = {"workload": f"cfg5 field shape: {m.nel} elements N=10, {n} points a plane, nz={nz}",
+           "field_bytes": f8, "peak_gbs": peak, "peak_kind": kind, "ops": res,
+           "l2": "every operand 2.03 GB, larger than L2; no flush"}
+    if check:
+        from oracle import dns
+        geo = dns.Geometry(m)
+        # fresh inputs: run each operation once more and compare the sample
+        sx.pressure_forcing(mesh, ptr(h), fp.data_ptr(), nz, n, dt, beta, stream=sptr)
+        sx.project(mesh, ptr(h), p.data_ptr(), ptr(out3), nz, n, dt, nu, ndim=3, beta=beta, stream=sptr)
+        torch.cuda.synchronize()
+        errs, cpu = {}, {}
+        for k in (0, 1, nz // 2 - 1):
+            sl = slice(2 * k, 2 * k + 2)
+            hh = [x[sl].cpu().numpy() for x in h]
+            pp = p[sl].cpu().numpy()
+            t0 = time.perf_counter()
+            want_f = dns.pressure_forcing(geo, hh, dt, beta, base_mode=k)
+            t1 = time.perf_counter()
+            want_u = dns.project(geo, hh, pp, dt, nu, ndim=3, beta=beta, base_mode=k)
+            t2 = time.perf_counter()
+            cpu.setdefault("pressure_forcing", []).append((t1 - t0) / 2 * 1e3)
+            cpu.setdefault("project", []).append((t2 - t1) / 2 * 1e3)
+            got_f = fp[sl].cpu().numpy()
+            e = np.abs(got_f - want_f).max() / np.abs(want_f).max()
+            for c in range(3):
+                got = out3[c][sl].cpu().numpy()
+                e = max(e, np.abs(got - want_u[c]).max() / np.abs(want_u[c]).max())
+            errs[str(k)] = float(e)
+        out["max_rel_err_vs_oracle"] = {"modes": errs, "worst": max(errs.values()),
+                                        "scale": "max |GPU - oracle| over max |oracle|, per mode"}
+        out["cpu_oracle_ms_per_plane"] = {k: float(np.median(v)) for k, v in cpu.items()}
+        out["gpu_ms_per_plane"] = {k: res[k]["ms"] / nz for k in ("pressure_forcing", "project")}
+        out["cpu_oracle"] = "numpy restatement (oracle/dns.py), one core, modes 0, 1 and 127"
+    del us, uf, h, p, fp, gx, out3
+    torch.cuda.empty_cache()
+    return out
+
+
 def _build_request(args):
     """Build one planned serving request (a spawned worker process)."""
     spec, seed = args
@@ -889,6 +996,8 @@ def run_profile(args):
     transform: the z-direction transform of the config-2 field (nz = 64,
            82,944 points, 42 MB), forward and inverse, `steps` times each,
            a 256 MB write between calls
+    dns:   the DNS elliptic-phase operations on config 5's plane shape with
+           nz = 32 (254 MB a field), `steps` + 1 launches of each
     """
     import torch
     import semtex_b200 as sx
@@ -905,6 +1014,10 @@ def run_profile(args):
                 sx.transform_z(d.data_ptr(), w.nz, w.mesh.nplane, w.mesh.nplane, sign, sptr)
         torch.cuda.synchronize()
         print(json.dumps({"profile": "transform", "nz": w.nz, "points": w.mesh.nplane}), flush=True)
+        return
+    if args.profile == "dns":
+        print(json.dumps({"profile": "dns", "run": run_dns(reps=max(1, args.steps), nz=32, check=False)}),
+              flush=True)
         return
     if args.profile == "band3":
         from semtex_b200.workloads import config3_block
@@ -957,7 +1070,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the extra keys (config 2, multi-mesh batch, z-transform)")
+                    help="skip the extra keys (config 2, multi-mesh batch, z-transform, DNS operations)")
     ap.add_argument("--serve-only", type=int, default=0, metavar="N",
                     help="run only the serving loop on the first N requests of the config-4 stream "
                          "and print its JSON (not a bench line)")
@@ -968,7 +1081,7 @@ def main():
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
-    ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform"], default=None,
+    ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform", "dns"], default=None,
                     help="bounded run of one kernel family for ncu (no bench line)")
     ap.add_argument("--band-cluster", type=int, default=0, help="--profile band*: CTAs per cluster (0: default)")
     ap.add_argument("--band-stages", type=int, default=0, help="--profile band*: ring depth (0: default)")

@@ -127,6 +127,12 @@ SX_API int sx_mesh_destroy(sx_mesh mesh);
 /* Read back element e's geometric factors Q1,Q2,Q3,Q4,Q8 (np*np each). */
 SX_API int sx_mesh_geometry(sx_mesh mesh, int e, double *q1, double *q2, double *q3, double *q4,
                      double *q8);
+/* Read back element e's inverse mapping partials dr/dx, dr/dy, ds/dx, ds/dy
+ * (np*np each; zero where the null-mapping rule of src/element.cpp:1431-1434
+ * drops them) and, when imass is not NULL, the inverse assembled boundary
+ * mass (nglobal doubles, src/bcmgr.cpp:805-821).  Any pointer may be NULL. */
+SX_API int sx_mesh_partials(sx_mesh mesh, int e, double *drdx, double *drdy, double *dsdx, double *dsdy,
+                            double *imass);
 
 /* ---- modal system: replaces ModalMatrixSys::ModalMatrixSys ---------------
  * src/matrix.cpp:33-110, MatrixSys::MatrixSys src/matrix.cpp:139-317.
@@ -289,6 +295,53 @@ SX_API int sx_profile_mixed_iterations(sx_modal modal, int reps, void *stream);
  * Enqueued on `stream`; nz = 2, 4, ..., 64 run as one kernel and return at
  * once, other lengths (which share a workspace) are waited for. */
 SX_API int sx_transform_z(double *d_data, int nz, int plane_stride, int npts, int sign, void *stream);
+
+/* ---- DNS elliptic phase: the field operations around the Helmholtz solves --
+ * Device data in the solve entry points' layout: nz planes plane_stride
+ * doubles apart (the buffers hold nz * plane_stride doubles), each plane
+ * nel*np*np points, element-major, np x np row-major.  Fourier planes are
+ * ordered as the solves take them: with base_mode 0, plane 0 is mode 0 and
+ * plane 1 Nyquist; planes 2k, 2k+1 hold Re, Im of mode k + base_mode.  Each
+ * call is enqueued on `stream` and returns at once.  Padding beyond a
+ * plane's points is neither read nor written (d/dz and the wave step aside,
+ * which the reference also applies to it).  Cylindrical geometry (the
+ * reference's mulY steps) is not supported by this library's meshes.
+ *
+ * AuxField::gradient (src/auxfield.cpp:514-616) in place: dir 0 d/dx, 1
+ * d/dy (Element::grad, src/element.cpp:552-596, every plane); dir 2 d/dz of
+ * Fourier planes (nz even): Re' = -beta k Im, Im' = beta k Re, the planes
+ * of mode 0 and Nyquist zeroed when base_mode is 0. */
+SX_API int sx_field_gradient(sx_mesh mesh, double *d_data, int nz, int plane_stride, int dir, double beta,
+                             int base_mode, void *stream);
+/* setPForce (dns/integrate.cpp:262-277): d_out = (sum_i d/dx_i us[i]) / dt
+ * over ndim (2 or 3) components, summed x + y, then + z, then times 1/dt.
+ * ndim 3 needs nz even; d_out may be us[0] or us[1], not us[2].  dt = 0 is
+ * SX_ERR_ARG (the reference's "divide by zero"). */
+SX_API int sx_dns_pressure_forcing(sx_mesh mesh, const double *const *d_us, int ndim, double *d_out, int nz,
+                                   int plane_stride, double dt, double beta, int base_mode, void *stream);
+/* project (dns/integrate.cpp:280-310): for the nadv advected fields,
+ *   uf[i] = alpha us[i] (times prandtl for the scalar, index ncom, when
+ *           nadv = ncom + 1) + (1/kinvis) d/dx_i p   for i < ndim,
+ * alpha = -1/(dt kinvis); ncom velocity components, ndim <= ncom <= 3.
+ * uf[i] may be us[i] (in place); no uf[i] may be p. */
+SX_API int sx_dns_project(sx_mesh mesh, const double *const *d_us, const double *d_p, double *const *d_uf,
+                          int ndim, int ncom, int nadv, int nz, int plane_stride, double dt, double kinvis,
+                          double prandtl, double beta, int base_mode, void *stream);
+/* Field::smooth (src/field.cpp:190-276) in place on every plane: the Q4-
+ * weighted sum of each global node's element-boundary values, taken element
+ * after element as bndryDsSum does (src/element.cpp:464-487), times the
+ * inverse assembled mass, written back to every slot of the node
+ * (bndryInsert).  Interior points are unchanged. */
+SX_API int sx_field_smooth(sx_mesh mesh, double *d_data, int nz, int plane_stride, void *stream);
+/* waveProp (dns/integrate.cpp:227-259): for each of nadv fields,
+ *   h[i] = sum_{q < order} (-alpha_{q+1} us[q][i] + dt beta_q uf[q][i]),
+ * alpha the stiffly-stable and beta the extrapolation weights of the given
+ * order (1-3, src/integration.cpp:98-163), accumulated level by level as the
+ * reference's axpy sequence does.  us, uf: order*nadv device pointers,
+ * level-major (us[q*nadv + i] = level q of field i), npts doubles each; h[i]
+ * may be any of its field's inputs. */
+SX_API int sx_dns_wave_prop(const double *const *d_us, const double *const *d_uf, double *const *d_h, int nadv,
+                            int order, long long npts, double dt, void *stream);
 
 /* ---- field files: replace the Header writer and AuxField stream I/O -------
  * The reference's field-file format: a 10-line ASCII header (Header <<,

@@ -146,6 +146,12 @@ def _load():
     L.sx_modal_tune.argtypes = [vp, ip, ip]
     L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
     L.sx_transform_z.argtypes = [vp, ip, ip, ip, ip, vp]
+    L.sx_mesh_partials.argtypes = [vp, ip] + [P(dp)] * 5
+    L.sx_field_gradient.argtypes = [vp, vp, ip, ip, ip, dp, ip, vp]
+    L.sx_dns_pressure_forcing.argtypes = [vp, P(vp), ip, vp, ip, ip, dp, dp, ip, vp]
+    L.sx_dns_project.argtypes = [vp, P(vp), vp, P(vp), ip, ip, ip, ip, ip, dp, dp, dp, dp, ip, vp]
+    L.sx_field_smooth.argtypes = [vp, vp, ip, ip, vp]
+    L.sx_dns_wave_prop.argtypes = [P(vp), P(vp), P(vp), ip, ip, C.c_longlong, dp, vp]
     L.sx_field_write.argtypes = [C.c_char_p, P(FieldHeader), P(P(dp)), ip]
     L.sx_field_read_header.argtypes = [C.c_char_p, P(FieldHeader)]
     L.sx_field_read.argtypes = [C.c_char_p, P(FieldHeader), P(P(dp)), ip]
@@ -235,6 +241,13 @@ class Mesh:
         h = C.c_void_p()
         _check(lib.sx_mesh_create(C.byref(d), C.byref(h)), "sx_mesh_create")
         self.h = h
+
+    def partials(self, e):
+        """Element e's (drdx, drdy, dsdx, dsdy) and the inverse boundary
+        mass (nglobal)."""
+        out = [np.zeros(self.qm.npnp) for _ in range(4)] + [np.zeros(self.qm.nglobal)]
+        _check(lib.sx_mesh_partials(self.h, e, *[_dptr(a) for a in out]), "sx_mesh_partials")
+        return out
 
     def geometry(self, e):
         out = [np.zeros(self.qm.npnp) for _ in range(5)]
@@ -397,6 +410,50 @@ def transform_z(d_data, nz, plane_stride, npts=None, sign=1, stream=0):
     plane order), sign=-1 back."""
     _check(lib.sx_transform_z(d_data, nz, plane_stride, plane_stride if npts is None else npts, sign, stream),
            "sx_transform_z")
+
+
+def _ptrs(ptrs):
+    return (C.c_void_p * len(ptrs))(*[int(x) for x in ptrs])
+
+
+def field_gradient(mesh, d_data, nz, stride, dir, beta=1.0, base_mode=0, stream=0):
+    """AuxField::gradient (src/auxfield.cpp:514-616) in place on nz device
+    planes: dir 0 d/dx, 1 d/dy, 2 d/dz of Fourier planes."""
+    _check(lib.sx_field_gradient(mesh.h, d_data, nz, stride, dir, beta, base_mode, stream), "sx_field_gradient")
+
+
+def pressure_forcing(mesh, d_us, d_out, nz, stride, dt, beta=1.0, base_mode=0, stream=0):
+    """setPForce (dns/integrate.cpp:262-277): d_out = div(us) / dt, us the
+    len(d_us) (2 or 3) velocity components."""
+    _check(lib.sx_dns_pressure_forcing(mesh.h, _ptrs(d_us), len(d_us), d_out, nz, stride, dt, beta, base_mode,
+                                       stream), "sx_dns_pressure_forcing")
+
+
+def project(mesh, d_us, d_p, d_uf, nz, stride, dt, kinvis, ndim, ncom=None, prandtl=1.0, beta=1.0,
+            base_mode=0, stream=0):
+    """project (dns/integrate.cpp:280-310): uf[i] = -us[i]/(dt kinvis)
+    (times prandtl for a scalar after the ncom velocities) + grad_i(p)/kinvis
+    for i < ndim."""
+    ncom = len(d_us) if ncom is None else ncom
+    _check(lib.sx_dns_project(mesh.h, _ptrs(d_us), d_p, _ptrs(d_uf), ndim, ncom, len(d_us), nz, stride, dt,
+                              kinvis, prandtl, beta, base_mode, stream), "sx_dns_project")
+
+
+def field_smooth(mesh, d_data, nz, stride, stream=0):
+    """Field::smooth (src/field.cpp:190-276) in place on nz device planes."""
+    _check(lib.sx_field_smooth(mesh.h, d_data, nz, stride, stream), "sx_field_smooth")
+
+
+def wave_prop(d_us, d_uf, d_h, npts, dt, stream=0):
+    """waveProp (dns/integrate.cpp:227-259): d_us[q][i], d_uf[q][i] = level
+    q of field i (order = len(d_us) levels), d_h[i] the results."""
+    order, nadv = len(d_us), len(d_h)
+    us = [x for lev in d_us for x in lev]
+    uf = [x for lev in d_uf for x in lev]
+    if len(us) != order * nadv or len(uf) != order * nadv:
+        raise ValueError("every level needs one pointer per field")
+    _check(lib.sx_dns_wave_prop(_ptrs(us), _ptrs(uf), _ptrs(d_h), nadv, order, npts, dt, stream),
+           "sx_dns_wave_prop")
 
 
 def write_field(path, fields, np_, nel, session="semtex_b200", step=0, time=0.0, dt=0.0, kinvis=0.0,

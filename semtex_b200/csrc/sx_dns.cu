@@ -1,0 +1,551 @@
+// sx_dns.cu -- the field operations of the DNS elliptic phase that build the
+// Helmholtz solves' forcing and consume their solutions, on device planes in
+// the solve entry points' layout (nz planes plane_stride doubles apart; each
+// plane element-major, each element np x np row-major).
+//
+// Reference:
+//   AuxField::gradient      src/auxfield.cpp:514-616 (the scalar branch, :583-612)
+//   Element::grad           src/element.cpp:552-596
+//   inverse partials        src/element.cpp:1403-1411, null mapping :1431-1434
+//   waveProp                dns/integrate.cpp:227-259
+//   setPForce               dns/integrate.cpp:262-277
+//   project                 dns/integrate.cpp:280-310
+//   Field::smooth           src/field.cpp:190-276
+//   Element::bndryDsSum     src/element.cpp:464-487, bndryInsert :540-548
+//   Integration::StifflyStable / Extrapolation  src/integration.cpp:98-163
+//
+// Every operation is bound by HBM traffic: each field plane is read once and
+// each result written once; the per-element partials are read once per CTA
+// and reused over a group of planes.
+#include <algorithm>
+
+#include "sx_internal.h"
+#include "sx_modal.h"
+#include "sx_ptx.cuh"
+
+namespace sx {
+namespace {
+
+// ---------------------------------------------------------------------------
+// element kernels: x / y derivatives (Element::grad) with their epilogues
+// ---------------------------------------------------------------------------
+//
+// A CTA holds a tile of TE consecutive elements of one plane in shared
+// memory and walks a group of planes, copying the next plane's tile in
+// (cp.async) while it works on this one.  Each derivative the operation
+// forms (a "job": d/dx of u, d/dy of v, ...) has two groups of 64 threads.
+// A "row" thread (t, r) forms row r of element t's r-derivative,
+//     dr[r][j] = sum_k u[r][k] D[j][k]        (u D^T, src/element.cpp:569)
+// times that row of dr/dx (or dr/dy) into A; a "column" thread (t, c) forms
+// column c of the s-derivative,
+//     ds[i][c] = sum_k D[i][k] u[k][c]        (D u, src/element.cpp:570)
+// times ds/dx (or ds/dy) into C.  The epilogue adds C + A -- the rounding
+// sequence of vmul + vvtvp (src/element.cpp:571-572) -- and applies the
+// operation's own arithmetic on the way out.  D is a kernel parameter: every
+// thread of a warp reads the same entry at the same time, so it is a
+// constant-bank operand of the FMA; each thread keeps its row (column) of
+// its job's partial in registers for the whole plane group.
+
+constexpr int EL_GROUP = 64;
+
+enum ElemOp { OP_GRAD = 0, OP_PFORCE = 1, OP_PROJECT = 2 };
+
+template <int NP>
+struct DMat {
+  double d[NP * NP];
+};
+
+template <int NP>
+constexpr int tile_elems() {
+  return EL_GROUP / NP;
+}
+// odd row pitch: the row walks (stride LP) and the column walks (stride 1)
+// of a warp are free of bank conflicts
+template <int NP>
+constexpr int row_pitch() {
+  return NP | 1;
+}
+template <int NP>
+constexpr int tile_words() {
+  return tile_elems<NP>() * NP * row_pitch<NP>();
+}
+template <int OP>
+constexpr int n_fields() {
+  return OP == OP_PFORCE ? 2 : 1;  // fields copied per plane
+}
+template <int OP>
+constexpr int n_jobs() {
+  return OP == OP_GRAD ? 1 : 2;  // derivatives formed per plane
+}
+// tiles [2 buffers][fields], then A [jobs], C [jobs]
+template <int NP, int OP>
+constexpr size_t elem_smem() {
+  return sizeof(double) * (size_t)(2 * n_fields<OP>() + 2 * n_jobs<OP>()) * tile_words<NP>();
+}
+template <int OP>
+constexpr int elem_threads() {
+  return 2 * EL_GROUP * n_jobs<OP>();
+}
+template <int OP>
+constexpr int elem_min_blocks() {
+  return OP == OP_GRAD ? 6 : 3;
+}
+
+struct ElemArgs {
+  const double *f0, *f1;  // fields in the tile: GRAD u; PFORCE u, v; PROJECT P
+  const double *fz;       // differentiated in z: PFORCE w; PROJECT P
+  double *out;            // GRAD: f0 (in place); PFORCE: the forcing
+  const double *us[4];    // PROJECT: u^ components
+  double *uf[4];          //          results
+  // partials of job 0 (r, s) and job 1 (r, s)
+  const double *r0, *s0, *r1, *s1;
+  long long stride;
+  int nel, nz, zgroup, base, ndim, ncom, nadv;
+  double beta, dtinv, alpha, bvisc, prandtl;
+};
+
+// Plane z of d/dz of a Fourier-space field w (src/auxfield.cpp:597-610):
+// mode k = z/2 + base; Re' = -beta k Im, Im' = beta k Re; with base 0 the
+// planes of mode 0 and Nyquist are zero.
+__device__ __forceinline__ double dz_value(const double *__restrict__ w, int z, size_t off, long long stride,
+                                           int base, double beta) {
+  const int k = z >> 1;
+  if (base == 0 && k == 0) return 0.0;
+  const double bk = beta * (double)(k + base);
+  if (z & 1) return __dmul_rn(bk, w[(size_t)(z - 1) * stride + off]);
+  return __dmul_rn(-bk, w[(size_t)(z + 1) * stride + off]);
+}
+
+// Row r of a tile times D^T (row threads) or D times column r (column
+// threads), scaled by the thread's partials p: into dst at the same places.
+template <int NP, int LP>
+__device__ __forceinline__ void deriv_line(const double *__restrict__ T, double *__restrict__ dst, bool rowt, int t,
+                                           int r, const DMat<NP> &D, const double (&p)[NP]) {
+  const int b = rowt ? (t * NP + r) * LP : t * NP * LP + r;
+  const int step = rowt ? 1 : LP;
+  double u[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) u[k] = T[b + k * step];
+#pragma unroll
+  for (int j = 0; j < NP; j++) {
+    double d = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) d = fma(u[k], D.d[j * NP + k], d);
+    dst[b + j * step] = __dmul_rn(d, p[j]);
+  }
+}
+
+template <int NP, int OP>
+__global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
+    k_elem(const ElemArgs a, const DMat<NP> D) {
+  constexpr int TE = tile_elems<NP>(), LP = row_pitch<NP>(), TW = tile_words<NP>();
+  constexpr int NF = n_fields<OP>(), NJ = n_jobs<OP>(), NT = elem_threads<OP>();
+  extern __shared__ double sm[];
+  double *tiles = sm;                // [2 buffers][NF][TW]
+  double *A = sm + 2 * NF * TW;      // [NJ][TW] row products
+  double *Cs = A + NJ * TW;          // [NJ][TW] column products
+  const int tid = threadIdx.x;
+  const int e0 = blockIdx.x * TE;
+  const int ne = min(TE, a.nel - e0);
+  const int nwords = ne * NP * NP;  // the tile's contiguous doubles in a plane
+  const int z0 = blockIdx.y * a.zgroup, z1 = min(a.nz, z0 + a.zgroup);
+  const int grp = tid / EL_GROUP, lt = tid - grp * EL_GROUP;
+  const bool rowt = (grp & 1) == 0;
+  const int job = grp >> 1;
+  const int t = lt / NP, r = lt - (lt / NP) * NP;
+  const bool active = t < ne;
+
+  // this thread's row (row threads) or column (column threads) of its job's
+  // partial
+  double p[NP];
+  {
+    const double *q = job == 0 ? (rowt ? a.r0 : a.s0) : (rowt ? a.r1 : a.s1);
+    const size_t eb = (size_t)(e0 + (active ? t : 0)) * NP * NP;
+#pragma unroll
+    for (int k = 0; k < NP; k++) p[k] = active ? q[eb + (rowt ? r * NP + k : k * NP + r)] : 0.0;
+  }
+  double *prod = (rowt ? A : Cs) + job * TW;
+  // the job's field: PFORCE's second job differentiates v, every other job
+  // the first field
+  const int fsel = (OP == OP_PFORCE && job == 1) ? 1 : 0;
+
+  auto issue = [&](int z, int buf) {
+    const size_t pb = (size_t)z * a.stride + (size_t)e0 * NP * NP;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const double *src = (f == 0 ? a.f0 : a.f1) + pb;
+      double *dst = tiles + (buf * NF + f) * TW;
+      for (int i = tid; i < nwords; i += NT) {
+        const int row = i / NP;
+        cp_async8_ca(dst + row * LP + (i - row * NP), src + i);
+      }
+    }
+    cp_async_commit();
+  };
+
+  if (z0 < z1) issue(z0, 0);
+  for (int z = z0; z < z1; z++) {
+    const int buf = (z - z0) & 1;
+    if (z + 1 < z1) {
+      issue(z + 1, buf ^ 1);
+      cp_async_wait_one();
+    } else {
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    if (active) deriv_line<NP, LP>(tiles + (buf * NF + fsel) * TW, prod, rowt, t, r, D, p);
+    __syncthreads();
+    // epilogue, coalesced over the tile's doubles of plane z
+    const size_t pb = (size_t)z * a.stride + (size_t)e0 * NP * NP;
+    for (int i = tid; i < nwords; i += NT) {
+      const int row = i / NP;
+      const int si = row * LP + (i - row * NP);
+      const size_t gi = pb + i;
+      const double g0 = __dadd_rn(Cs[si], A[si]);
+      if (OP == OP_GRAD) {
+        a.out[gi] = g0;
+      } else if (OP == OP_PFORCE) {
+        // ((d/dx u + d/dy v) + d/dz w) / dt  (dns/integrate.cpp:272-276)
+        double s = __dadd_rn(g0, __dadd_rn(Cs[TW + si], A[TW + si]));
+        if (a.ndim == 3) s = __dadd_rn(s, dz_value(a.fz, z, (size_t)e0 * NP * NP + i, a.stride, a.base, a.beta));
+        a.out[gi] = __dmul_rn(s, a.dtinv);
+      } else {
+        // u^^ = alpha u^ (times Pr for the scalar) + bvisc grad P
+        // (dns/integrate.cpp:296-309)
+        const double g1 = __dadd_rn(Cs[TW + si], A[TW + si]);
+        double us[4];  // every component's load issued before the first store
+#pragma unroll
+        for (int c = 0; c < 4; c++) us[c] = c < a.nadv ? a.us[c][gi] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          if (c >= a.nadv) break;
+          double v = __dmul_rn(a.alpha, us[c]);
+          if (c == a.ncom) v = __dmul_rn(v, a.prandtl);
+          if (c < a.ndim) {
+            const double g = c == 0   ? g0
+                             : c == 1 ? g1
+                                      : dz_value(a.fz, z, (size_t)e0 * NP * NP + i, a.stride, a.base, a.beta);
+            v = __dadd_rn(v, __dmul_rn(a.bvisc, g));
+          }
+          a.uf[c][gi] = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// d/dz in place on Fourier planes (src/auxfield.cpp:597-610): thread per
+// (mode, point), both planes of the mode read before either is written.
+__global__ void k_dz_inplace(double *__restrict__ w, int nmodes, int npts, long long stride, int base, double beta) {
+  const int m = blockIdx.y;
+  double *re = w + (size_t)(2 * m) * stride, *im = re + stride;
+  const int k = m + base;
+  const double bk = beta * (double)k;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
+    if (base == 0 && m == 0) {
+      re[i] = 0.0;
+      im[i] = 0.0;
+    } else {
+      const double a = re[i], b = im[i];
+      re[i] = __dmul_rn(-bk, b);
+      im[i] = __dmul_rn(bk, a);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field::smooth: mass-weighted direct stiffness average of element boundaries
+// ---------------------------------------------------------------------------
+//
+// Thread per global node g.  The reference sums Q4 u of every element slot
+// holding g into dssum[g] element after element, scales by imass[g] and
+// writes the value back into those slots.  The CSR g2e lists each node's
+// slots in element order, so the sum here is the reference's sum, rounding
+// for rounding, and each slot is read and written by one thread only.
+constexpr int SMOOTH_CACHE = 8;
+
+__global__ void __launch_bounds__(256)
+    k_smooth(double *__restrict__ u, const int *__restrict__ ptr, const int *__restrict__ idx,
+             const int *__restrict__ emap, const double *__restrict__ Q4, const double *__restrict__ imass,
+             int nglobal, int next, int npnp, int nz, int zgroup, long long stride) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nglobal) return;
+  const int z0 = blockIdx.y * zgroup, z1 = min(nz, z0 + zgroup);
+  const int b = ptr[g], n = ptr[g + 1] - b;
+  int off[SMOOTH_CACHE];
+  double wq[SMOOTH_CACHE];
+#pragma unroll
+  for (int c = 0; c < SMOOTH_CACHE; c++) {
+    off[c] = 0;
+    wq[c] = 0.0;
+    if (c < n) {
+      const int slot = idx[b + c], e = slot / next;
+      off[c] = e * npnp + emap[slot - e * next];
+      wq[c] = Q4[off[c]];
+    }
+  }
+  const double im = imass[g];
+  for (int z = z0; z < z1; z++) {
+    double *p = u + (size_t)z * stride;
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < SMOOTH_CACHE; c++)
+      if (c < n) s = __dadd_rn(s, __dmul_rn(wq[c], p[off[c]]));
+    for (int c = SMOOTH_CACHE; c < n; c++) {  // vertices shared by more than 8 elements
+      const int slot = idx[b + c], e = slot / next;
+      const int o = e * npnp + emap[slot - e * next];
+      s = __dadd_rn(s, __dmul_rn(Q4[o], p[o]));
+    }
+    s = __dmul_rn(s, im);
+#pragma unroll
+    for (int c = 0; c < SMOOTH_CACHE; c++)
+      if (c < n) p[off[c]] = s;
+    for (int c = SMOOTH_CACHE; c < n; c++) {
+      const int slot = idx[b + c], e = slot / next;
+      p[e * npnp + emap[slot - e * next]] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// waveProp: u^ = sum_q (-alpha_{q+1} u_q + dt beta_q N_q)
+// ---------------------------------------------------------------------------
+
+struct WaveArgs {
+  const double *us[3][4], *uf[3][4];
+  double *h[4];
+  double a[3], b[3];  // -alpha_{q+1}, dt beta_q
+  int order, nadv;
+  long long n;
+};
+
+__global__ void __launch_bounds__(256) k_wave_prop(const WaveArgs w) {
+  const long long step = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += step)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (c >= w.nadv) break;
+      // H = 0, then axpy(-alpha[q+1], Us[q]), axpy(beta[q], Uf[q]) level by
+      // level (dns/integrate.cpp:241-258)
+      double h = 0.0;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        if (q >= w.order) break;
+        h = __dadd_rn(h, __dmul_rn(w.a[q], w.us[q][c][i]));
+        h = __dadd_rn(h, __dmul_rn(w.b[q], w.uf[q][c][i]));
+      }
+      w.h[c][i] = h;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+#define SX_DNS_NP_SWITCH(np, CALL)                    \
+  switch (np) {                                       \
+    case 3: { constexpr int N_ = 3; CALL; } break;   \
+    case 4: { constexpr int N_ = 4; CALL; } break;   \
+    case 5: { constexpr int N_ = 5; CALL; } break;   \
+    case 6: { constexpr int N_ = 6; CALL; } break;   \
+    case 7: { constexpr int N_ = 7; CALL; } break;   \
+    case 8: { constexpr int N_ = 8; CALL; } break;   \
+    case 9: { constexpr int N_ = 9; CALL; } break;   \
+    case 10: { constexpr int N_ = 10; CALL; } break; \
+    case 11: { constexpr int N_ = 11; CALL; } break; \
+    case 12: { constexpr int N_ = 12; CALL; } break; \
+    default: return SX_ERR_UNSUPPORTED;               \
+  }
+
+// Planes per CTA: as many as keep at least ~4 waves of two CTAs per SM.
+int plane_group(long long tiles, int nz) {
+  for (int zg : {16, 8, 4, 2})
+    if (tiles * ((nz + zg - 1) / zg) >= 4LL * 2 * 148) return std::min(zg, nz);
+  return 1;
+}
+
+template <int NP, int OP>
+int launch_elem(const sx_mesh_s &M, ElemArgs a, cudaStream_t st) {
+  constexpr int TE = tile_elems<NP>();
+  constexpr size_t smem = elem_smem<NP, OP>();
+  static_assert(smem <= 227 * 1024, "element tile does not fit in shared memory");
+  if (smem > 48 * 1024)
+    SX_CUDA(cudaFuncSetAttribute(k_elem<NP, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  DMat<NP> D;
+  for (int i = 0; i < NP * NP; i++) D.d[i] = M.D[i];
+  const long long tiles = (M.nel + TE - 1) / TE;
+  a.nel = M.nel;
+  a.zgroup = plane_group(tiles, a.nz);
+  const dim3 grid((unsigned)tiles, (unsigned)((a.nz + a.zgroup - 1) / a.zgroup));
+  k_elem<NP, OP><<<grid, elem_threads<OP>(), smem, st>>>(a, D);
+  SX_CUDA(cudaGetLastError());
+  return SX_OK;
+}
+
+template <int OP>
+int run_elem(const sx_mesh_s &M, const ElemArgs &a, cudaStream_t st) {
+  SX_DNS_NP_SWITCH(M.np, return (launch_elem<N_, OP>(M, a, st)));
+  return SX_ERR_UNSUPPORTED;
+}
+
+int check_planes(const sx_mesh_s &M, int nz, int plane_stride, const char *who) {
+  if (nz < 1 || plane_stride < M.nel * M.npnp) {
+    set_error("%s: nz = %d, plane_stride = %d (a plane holds %d points)", who, nz, plane_stride, M.nel * M.npnp);
+    return SX_ERR_ARG;
+  }
+  return check_mesh_device(M, who);
+}
+
+}  // namespace
+}  // namespace sx
+
+using namespace sx;
+
+extern "C" int sx_field_gradient(sx_mesh mesh, double *d_data, int nz, int plane_stride, int dir, double beta,
+                                 int base_mode, void *stream) {
+  if (!mesh || !d_data || dir < 0 || dir > 2 || base_mode < 0) return SX_ERR_ARG;
+  SX_TRY(check_planes(*mesh, nz, plane_stride, "sx_field_gradient"));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dir == 2) {
+    if (nz % 2) {
+      set_error("sx_field_gradient: d/dz needs Fourier planes in pairs (nz = %d)", nz);
+      return SX_ERR_ARG;
+    }
+    const int npts = mesh->nel * mesh->npnp;
+    const dim3 grid((unsigned)std::min((npts + 255) / 256, 148 * 4), (unsigned)(nz / 2));
+    k_dz_inplace<<<grid, 256, 0, st>>>(d_data, nz / 2, npts, plane_stride, base_mode, beta);
+    SX_CUDA(cudaGetLastError());
+    return SX_OK;
+  }
+  ElemArgs a{};
+  a.f0 = d_data;
+  a.f1 = d_data;
+  a.out = d_data;
+  a.r0 = dir == 0 ? mesh->ddrdx.p : mesh->ddrdy.p;
+  a.s0 = dir == 0 ? mesh->ddsdx.p : mesh->ddsdy.p;
+  a.r1 = a.r0;
+  a.s1 = a.s0;
+  a.stride = plane_stride;
+  a.nz = nz;
+  return run_elem<OP_GRAD>(*mesh, a, st);
+}
+
+extern "C" int sx_dns_pressure_forcing(sx_mesh mesh, const double *const *d_us, int ndim, double *d_out, int nz,
+                                       int plane_stride, double dt, double beta, int base_mode, void *stream) {
+  if (!mesh || !d_us || !d_out || ndim < 2 || ndim > 3 || base_mode < 0) return SX_ERR_ARG;
+  for (int i = 0; i < ndim; i++)
+    if (!d_us[i]) return SX_ERR_ARG;
+  if (dt == 0.0) {
+    set_error("sx_dns_pressure_forcing: divide by zero (dt = 0)");
+    return SX_ERR_ARG;
+  }
+  SX_TRY(check_planes(*mesh, nz, plane_stride, "sx_dns_pressure_forcing"));
+  if (ndim == 3 && (nz % 2 || d_out == d_us[2])) {
+    set_error("sx_dns_pressure_forcing: 3 dimensions need Fourier planes in pairs and an output apart from w");
+    return SX_ERR_ARG;
+  }
+  ElemArgs a{};
+  a.f0 = d_us[0];
+  a.f1 = d_us[1];
+  a.fz = ndim == 3 ? d_us[2] : nullptr;
+  a.out = d_out;
+  a.r0 = mesh->ddrdx.p;
+  a.s0 = mesh->ddsdx.p;
+  a.r1 = mesh->ddrdy.p;
+  a.s1 = mesh->ddsdy.p;
+  a.stride = plane_stride;
+  a.nz = nz;
+  a.ndim = ndim;
+  a.base = base_mode;
+  a.beta = beta;
+  a.dtinv = 1.0 / dt;
+  return run_elem<OP_PFORCE>(*mesh, a, (cudaStream_t)stream);
+}
+
+extern "C" int sx_dns_project(sx_mesh mesh, const double *const *d_us, const double *d_p, double *const *d_uf,
+                              int ndim, int ncom, int nadv, int nz, int plane_stride, double dt, double kinvis,
+                              double prandtl, double beta, int base_mode, void *stream) {
+  if (!mesh || !d_us || !d_p || !d_uf || ndim < 2 || ndim > 3 || ncom < ndim || ncom > 3 || nadv < ncom ||
+      nadv > ncom + 1 || base_mode < 0)
+    return SX_ERR_ARG;
+  for (int i = 0; i < nadv; i++)
+    if (!d_us[i] || !d_uf[i] || d_uf[i] == d_p) return SX_ERR_ARG;
+  if (dt * kinvis == 0.0 || kinvis == 0.0) {
+    set_error("sx_dns_project: D_T * KINVIS and KINVIS must be nonzero");
+    return SX_ERR_ARG;
+  }
+  SX_TRY(check_planes(*mesh, nz, plane_stride, "sx_dns_project"));
+  if (ndim == 3 && nz % 2) {
+    set_error("sx_dns_project: 3 dimensions need Fourier planes in pairs (nz = %d)", nz);
+    return SX_ERR_ARG;
+  }
+  ElemArgs a{};
+  a.f0 = d_p;
+  a.f1 = d_p;
+  a.fz = d_p;
+  for (int i = 0; i < nadv; i++) {
+    a.us[i] = d_us[i];
+    a.uf[i] = d_uf[i];
+  }
+  a.r0 = mesh->ddrdx.p;
+  a.s0 = mesh->ddsdx.p;
+  a.r1 = mesh->ddrdy.p;
+  a.s1 = mesh->ddsdy.p;
+  a.stride = plane_stride;
+  a.nz = nz;
+  a.ndim = ndim;
+  a.ncom = nadv > ncom ? ncom : -1;  // the scalar's index, when there is one
+  a.nadv = nadv;
+  a.base = base_mode;
+  a.beta = beta;
+  a.alpha = -1.0 / (dt * kinvis);
+  a.bvisc = 1.0 / kinvis;
+  a.prandtl = prandtl;
+  return run_elem<OP_PROJECT>(*mesh, a, (cudaStream_t)stream);
+}
+
+extern "C" int sx_field_smooth(sx_mesh mesh, double *d_data, int nz, int plane_stride, void *stream) {
+  if (!mesh || !d_data) return SX_ERR_ARG;
+  SX_TRY(check_planes(*mesh, nz, plane_stride, "sx_field_smooth"));
+  const int threads = 256;
+  const long long blocks = (mesh->nglobal + threads - 1) / threads;
+  const int zg = plane_group(blocks, nz);
+  const dim3 grid((unsigned)blocks, (unsigned)((nz + zg - 1) / zg));
+  k_smooth<<<grid, threads, 0, (cudaStream_t)stream>>>(d_data, mesh->dg2e_ptr.p, mesh->dg2e_idx.p, mesh->demap.p,
+                                                       mesh->dQ4.p, mesh->dimass.p, mesh->nglobal, mesh->next,
+                                                       mesh->npnp, nz, zg, plane_stride);
+  SX_CUDA(cudaGetLastError());
+  return SX_OK;
+}
+
+extern "C" int sx_dns_wave_prop(const double *const *d_us, const double *const *d_uf, double *const *d_h, int nadv,
+                                int order, long long npts, double dt, void *stream) {
+  if (!d_us || !d_uf || !d_h || nadv < 1 || nadv > 4 || order < 1 || order > 3 || npts < 0) return SX_ERR_ARG;
+  // Stiffly-stable (backward differentiation) and extrapolation weights of
+  // order 1-3 (Gear 1971, Table 11.1; src/integration.cpp:98-163)
+  static const double alpha[3][4] = {{1.0, -1.0, 0.0, 0.0}, {1.5, -2.0, 0.5, 0.0}, {11.0 / 6.0, -3.0, 1.5, -1.0 / 3.0}};
+  static const double extrap[3][3] = {{1.0, 0.0, 0.0}, {2.0, -1.0, 0.0}, {3.0, -3.0, 1.0}};
+  WaveArgs w{};
+  for (int q = 0; q < order; q++) {
+    w.a[q] = -alpha[order - 1][q + 1];
+    w.b[q] = extrap[order - 1][q] * dt;
+    for (int c = 0; c < nadv; c++) {
+      w.us[q][c] = d_us[q * nadv + c];
+      w.uf[q][c] = d_uf[q * nadv + c];
+      if (!w.us[q][c] || !w.uf[q][c]) return SX_ERR_ARG;
+    }
+  }
+  for (int c = 0; c < nadv; c++) {
+    if (!d_h[c]) return SX_ERR_ARG;
+    w.h[c] = d_h[c];
+  }
+  w.order = order;
+  w.nadv = nadv;
+  w.n = npts;
+  if (npts == 0) return SX_OK;
+  const long long blocks = std::min<long long>((npts + 255) / 256, 148LL * 8);
+  k_wave_prop<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(w);
+  SX_CUDA(cudaGetLastError());
+  return SX_OK;
+}

@@ -182,6 +182,10 @@ struct sx_mesh_s {
   std::vector<double> z, w, D;
   std::vector<int> emap, pmap;
   std::vector<double> Q1, Q2, Q3, Q4, Q8;  // host copies
+  // inverse mapping partials dr/dx, dr/dy, ds/dx, ds/dy (zero where the
+  // reference's null-mapping drops them) and the inverse of the assembled
+  // boundary mass (BoundarySys imass)
+  std::vector<double> drdx, drdy, dsdx, dsdy, imass;
   std::vector<unsigned char> hasQ3;
   std::vector<int> btog, bmask, emask;
   std::vector<int> b_elmt, b_side, b_kind;
@@ -189,6 +193,7 @@ struct sx_mesh_s {
   std::vector<int> colour_ptr, colour_elmt;  // element colouring (no shared nodes)
   // device
   sx::DBuf<double> dD, dQ1, dQ2, dQ3, dQ4, dQ8, dK, dC, darea;
+  sx::DBuf<double> ddrdx, ddrdy, ddsdx, ddsdy, dimass;
   sx::DBuf<float> dQ1f, dQ2f, dQ3f, dQ4f, dDf;
   sx::DBuf<unsigned char> dhasQ3;
   sx::DBuf<int> dpmap;

@@ -159,6 +159,20 @@ static int element_geometry(sx_mesh_s &M, int e, const double *x, const double *
   // Null-mapping: drop Q3 for undistorted elements (src/element.cpp:1431-1435).
   M.hasQ3[e] = nrm2(nn, Q3) >= EPS;
   if (!M.hasQ3[e]) std::memset(Q3, 0, sizeof(double) * nn);
+  // Inverse mapping partials (src/element.cpp:1403-1411), each dropped by
+  // the same null-mapping test (:1431-1434); a dropped partial reads as 0.
+  if (M.drdx.empty()) return SX_OK;  // geometry-only callers
+  double *rx = &M.drdx[(size_t)e * nn], *ry = &M.drdy[(size_t)e * nn];
+  double *sx_ = &M.dsdx[(size_t)e * nn], *sy = &M.dsdy[(size_t)e * nn];
+  for (int k = 0; k < nn; k++) {
+    const double jac = dxdr[k] * dyds[k] - dxds[k] * dydr[k];
+    rx[k] = dyds[k] / jac;
+    ry[k] = -dxds[k] / jac;
+    sx_[k] = -dydr[k] / jac;
+    sy[k] = dxdr[k] / jac;
+  }
+  for (double *a : {rx, ry, sx_, sy})
+    if (nrm2(nn, a) < EPS) std::memset(a, 0, sizeof(double) * nn);
   return SX_OK;
 }
 
@@ -295,6 +309,7 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   const size_t tot = (size_t)nel * nn, tb = (size_t)nel * next;
   M->Q1.assign(tot, 0.0); M->Q2.assign(tot, 0.0); M->Q3.assign(tot, 0.0);
   M->Q4.assign(tot, 0.0); M->Q8.assign(tot, 0.0);
+  M->drdx.assign(tot, 0.0); M->drdy.assign(tot, 0.0); M->dsdx.assign(tot, 0.0); M->dsdy.assign(tot, 0.0);
   M->hasQ3.assign(nel, 0);
   for (int e = 0; e < nel; e++)
     SX_TRY(element_geometry(*M, e, d->x + (size_t)e * nn, d->y + (size_t)e * nn));
@@ -412,6 +427,14 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
     std::vector<int> fill(M->colour_ptr.begin(), M->colour_ptr.end() - 1);
     for (int e = 0; e < nel; e++) M->colour_elmt[fill[colour[e]]++] = e;
   }
+  // Inverse of the assembled boundary mass: unity summed into the global
+  // numbering with the Q4 weights, element after element (bndryDsSum,
+  // src/element.cpp:464-487, as BCmgr::buildnum uses it, src/bcmgr.cpp:805-821).
+  M->imass.assign(d->nglobal, 0.0);
+  for (int e = 0; e < nel; e++)
+    for (int i = 0; i < next; i++)
+      M->imass[M->btog[(size_t)e * next + i]] += M->Q4[(size_t)e * nn + M->emap[i]];
+  for (int g = 0; g < d->nglobal; g++) M->imass[g] = 1.0 / M->imass[g];
   // FP32 copies of the geometry for the mixed-precision operator.
   std::vector<float> f1(tot), f2(tot), f3(tot), f4(tot);
   for (size_t i = 0; i < tot; i++) {
@@ -425,6 +448,11 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   SX_TRY(M->dQ3.upload(M->Q3.data(), tot));
   SX_TRY(M->dQ4.upload(M->Q4.data(), tot));
   SX_TRY(M->dQ8.upload(M->Q8.data(), tot));
+  SX_TRY(M->ddrdx.upload(M->drdx.data(), tot));
+  SX_TRY(M->ddrdy.upload(M->drdy.data(), tot));
+  SX_TRY(M->ddsdx.upload(M->dsdx.data(), tot));
+  SX_TRY(M->ddsdy.upload(M->dsdy.data(), tot));
+  SX_TRY(M->dimass.upload(M->imass.data(), M->imass.size()));
   SX_TRY(M->dQ1f.upload(f1.data(), tot));
   SX_TRY(M->dQ2f.upload(f2.data(), tot));
   SX_TRY(M->dQ3f.upload(f3.data(), tot));
@@ -503,5 +531,17 @@ extern "C" int sx_mesh_geometry(sx_mesh m, int e, double *q1, double *q2, double
   if (q3) std::memcpy(q3, &m->Q3[o], n * 8);
   if (q4) std::memcpy(q4, &m->Q4[o], n * 8);
   if (q8) std::memcpy(q8, &m->Q8[o], n * 8);
+  return SX_OK;
+}
+
+extern "C" int sx_mesh_partials(sx_mesh m, int e, double *drdx, double *drdy, double *dsdx, double *dsdy,
+                                double *imass) {
+  if (!m || e < 0 || e >= m->nel) return SX_ERR_ARG;
+  const size_t o = (size_t)e * m->npnp, n = m->npnp;
+  if (drdx) std::memcpy(drdx, &m->drdx[o], n * 8);
+  if (drdy) std::memcpy(drdy, &m->drdy[o], n * 8);
+  if (dsdx) std::memcpy(dsdx, &m->dsdx[o], n * 8);
+  if (dsdy) std::memcpy(dsdy, &m->dsdy[o], n * 8);
+  if (imass) std::memcpy(imass, m->imass.data(), m->imass.size() * 8);
   return SX_OK;
 }

@@ -89,9 +89,17 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 __device__ __forceinline__ void cp_async16_cg(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+// 8-byte asynchronous copy global -> this CTA's shared memory (L1 allowed:
+// callers only read data that no other CTA writes during the launch).
+// Both addresses 8-B aligned.
+__device__ __forceinline__ void cp_async8_ca(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Wait until every cp.async group of the calling thread has landed.
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Wait until at most one (the most recent) cp.async group is still in flight.
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // 1-D TMA bulk copy this CTA's shared memory -> global, in the calling
 // thread's bulk group.  dst/src 16-B aligned, bytes a multiple of 16.  The
