@@ -69,22 +69,39 @@ template <int NP>
 constexpr int tile_words() {
   return tile_elems<NP>() * NP * row_pitch<NP>();
 }
+// a staged field's slot: the tile rounded up to 16 bytes
+template <int NP>
+constexpr int stage_words() {
+  return (tile_words<NP>() + 1) & ~1;
+}
+// fields staged per plane, at most: GRAD u; PFORCE u, v and w's partner
+// plane; PROJECT P, P's partner plane and up to four u^ components
 template <int OP>
-constexpr int n_fields() {
-  return OP == OP_PFORCE ? 2 : 1;  // fields copied per plane
+constexpr int max_stage() {
+  return OP == OP_GRAD ? 1 : OP == OP_PFORCE ? 3 : 6;
 }
 template <int OP>
 constexpr int n_jobs() {
   return OP == OP_GRAD ? 1 : 2;  // derivatives formed per plane
 }
-// tiles [2 buffers][fields], then A [jobs], C [jobs]
-template <int NP, int OP>
-constexpr size_t elem_smem() {
-  return sizeof(double) * (size_t)(2 * n_fields<OP>() + 2 * n_jobs<OP>()) * tile_words<NP>();
+// planes in the copy ring: two in flight while a third is worked on; one
+// for project, whose five or six staged fields would otherwise leave room
+// for two CTAs an SM
+template <int OP>
+constexpr int el_ring() {
+  return OP == OP_PROJECT ? 2 : 3;
 }
+// tiles [ring slots][staged fields], then A [jobs], C [jobs]
+template <int NP, int OP>
+constexpr size_t elem_smem(int nstage) {
+  return sizeof(double) *
+         ((size_t)el_ring<OP>() * nstage * stage_words<NP>() + 2 * n_jobs<OP>() * tile_words<NP>());
+}
+// a row group and a column group; with two jobs a thread forms both, each
+// D entry it reads serving two multiply-adds
 template <int OP>
 constexpr int elem_threads() {
-  return 2 * EL_GROUP * n_jobs<OP>();
+  return 2 * EL_GROUP;
 }
 template <int OP>
 constexpr int elem_min_blocks() {
@@ -92,29 +109,19 @@ constexpr int elem_min_blocks() {
 }
 
 struct ElemArgs {
-  const double *f0, *f1;  // fields in the tile: GRAD u; PFORCE u, v; PROJECT P
-  const double *fz;       // differentiated in z: PFORCE w; PROJECT P
-  double *out;            // GRAD: f0 (in place); PFORCE: the forcing
-  const double *us[4];    // PROJECT: u^ components
-  double *uf[4];          //          results
+  // fields staged into shared memory plane by plane; a "partner" field is
+  // read at plane z ^ 1 (the other half of plane z's Fourier mode)
+  const double *stage[6];
+  int partner[6];
+  int nstage, ubase;      // PROJECT: the first u^ component's stage
+  double *out;            // GRAD: the field itself (in place); PFORCE: the forcing
+  double *uf[4];          // PROJECT: results
   // partials of job 0 (r, s) and job 1 (r, s)
   const double *r0, *s0, *r1, *s1;
   long long stride;
   int nel, nz, zgroup, base, ndim, ncom, nadv;
   double beta, dtinv, alpha, bvisc, prandtl;
 };
-
-// Plane z of d/dz of a Fourier-space field w (src/auxfield.cpp:597-610):
-// mode k = z/2 + base; Re' = -beta k Im, Im' = beta k Re; with base 0 the
-// planes of mode 0 and Nyquist are zero.
-__device__ __forceinline__ double dz_value(const double *__restrict__ w, int z, size_t off, long long stride,
-                                           int base, double beta) {
-  const int k = z >> 1;
-  if (base == 0 && k == 0) return 0.0;
-  const double bk = beta * (double)(k + base);
-  if (z & 1) return __dmul_rn(bk, w[(size_t)(z - 1) * stride + off]);
-  return __dmul_rn(-bk, w[(size_t)(z + 1) * stride + off]);
-}
 
 // Row r of a tile times D^T (row threads) or D times column r (column
 // threads), scaled by the thread's partials p: into dst at the same places.
@@ -135,71 +142,120 @@ __device__ __forceinline__ void deriv_line(const double *__restrict__ T, double 
   }
 }
 
+// Both jobs of a line: two fields with a partial each (TWO_FIELDS) or one
+// field with two partials (the x and y derivatives of the same P).
+template <int NP, int LP, bool TWO_FIELDS>
+__device__ __forceinline__ void deriv_pair(const double *__restrict__ T0, const double *__restrict__ T1,
+                                           double *__restrict__ d0, double *__restrict__ d1, bool rowt, int t,
+                                           int r, const DMat<NP> &D, const double (&p0)[NP],
+                                           const double (&p1)[NP]) {
+  const int b = rowt ? (t * NP + r) * LP : t * NP * LP + r;
+  const int step = rowt ? 1 : LP;
+  double u[NP], v[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    u[k] = T0[b + k * step];
+    v[k] = TWO_FIELDS ? T1[b + k * step] : 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < NP; j++) {
+    double x = 0.0, y = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      const double dk = D.d[j * NP + k];
+      x = fma(u[k], dk, x);
+      if (TWO_FIELDS) y = fma(v[k], dk, y);
+    }
+    d0[b + j * step] = __dmul_rn(x, p0[j]);
+    d1[b + j * step] = __dmul_rn(TWO_FIELDS ? y : x, p1[j]);
+  }
+}
+
 template <int NP, int OP>
 __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
     k_elem(const ElemArgs a, const DMat<NP> D) {
-  constexpr int TE = tile_elems<NP>(), LP = row_pitch<NP>(), TW = tile_words<NP>();
-  constexpr int NF = n_fields<OP>(), NJ = n_jobs<OP>(), NT = elem_threads<OP>();
-  extern __shared__ double sm[];
-  double *tiles = sm;                // [2 buffers][NF][TW]
-  double *A = sm + 2 * NF * TW;      // [NJ][TW] row products
+  constexpr int TE = tile_elems<NP>(), LP = row_pitch<NP>(), TW = tile_words<NP>(), SW = stage_words<NP>();
+  constexpr int NS = max_stage<OP>(), NJ = n_jobs<OP>(), NT = elem_threads<OP>();
+  constexpr bool FLAT = LP == NP;  // tile rows unpadded: the tile is the plane's contiguous run
+  constexpr int EL_RING = el_ring<OP>();
+  extern __shared__ __align__(16) double sm[];
+  const int ns = a.nstage;
+  double *tiles = sm;                  // [EL_RING buffers][ns][SW]
+  double *A = sm + EL_RING * ns * SW;  // [NJ][TW] row products
   double *Cs = A + NJ * TW;          // [NJ][TW] column products
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * TE;
   const int ne = min(TE, a.nel - e0);
   const int nwords = ne * NP * NP;  // the tile's contiguous doubles in a plane
   const int z0 = blockIdx.y * a.zgroup, z1 = min(a.nz, z0 + a.zgroup);
-  const int grp = tid / EL_GROUP, lt = tid - grp * EL_GROUP;
-  const bool rowt = (grp & 1) == 0;
-  const int job = grp >> 1;
+  const bool rowt = tid < EL_GROUP;
+  const int lt = rowt ? tid : tid - EL_GROUP;
   const int t = lt / NP, r = lt - (lt / NP) * NP;
   const bool active = t < ne;
 
-  // this thread's row (row threads) or column (column threads) of its job's
-  // partial
-  double p[NP];
+  // this thread's row (row threads) or column (column threads) of each
+  // job's partial
+  double p0[NP], p1[NP];
   {
-    const double *q = job == 0 ? (rowt ? a.r0 : a.s0) : (rowt ? a.r1 : a.s1);
+    const double *q0 = rowt ? a.r0 : a.s0, *q1 = rowt ? a.r1 : a.s1;
     const size_t eb = (size_t)(e0 + (active ? t : 0)) * NP * NP;
 #pragma unroll
-    for (int k = 0; k < NP; k++) p[k] = active ? q[eb + (rowt ? r * NP + k : k * NP + r)] : 0.0;
+    for (int k = 0; k < NP; k++) {
+      const size_t node = eb + (rowt ? r * NP + k : k * NP + r);
+      p0[k] = active ? q0[node] : 0.0;
+      p1[k] = (NJ == 2 && active) ? q1[node] : 0.0;
+    }
   }
-  double *prod = (rowt ? A : Cs) + job * TW;
-  // the job's field: PFORCE's second job differentiates v, every other job
-  // the first field
-  const int fsel = (OP == OP_PFORCE && job == 1) ? 1 : 0;
+  double *prod = rowt ? A : Cs;
 
+  // every call commits one cp.async group (empty past the plane group's
+  // end), so that "all but the newest EL_RING - 1 groups" is always plane z
   auto issue = [&](int z, int buf) {
-    const size_t pb = (size_t)z * a.stride + (size_t)e0 * NP * NP;
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
-      const double *src = (f == 0 ? a.f0 : a.f1) + pb;
-      double *dst = tiles + (buf * NF + f) * TW;
-      for (int i = tid; i < nwords; i += NT) {
-        const int row = i / NP;
-        cp_async8_ca(dst + row * LP + (i - row * NP), src + i);
+    for (int f = 0; f < NS; f++) {
+      if (f >= ns || z >= z1) break;
+      const double *src = a.stage[f] + (size_t)(a.partner[f] ? z ^ 1 : z) * a.stride + (size_t)e0 * NP * NP;
+      double *dst = tiles + (buf * ns + f) * SW;
+      if (FLAT) {
+        for (int i = tid; i < nwords; i += NT) cp_async8_ca(dst + i, src + i);
+      } else {
+        for (int i = tid; i < nwords; i += NT) {
+          const int row = i / NP;
+          cp_async8_ca(dst + row * LP + (i - row * NP), src + i);
+        }
       }
     }
     cp_async_commit();
   };
 
-  if (z0 < z1) issue(z0, 0);
+  for (int q = 0; q < EL_RING - 1; q++) issue(z0 + q, q);
   for (int z = z0; z < z1; z++) {
-    const int buf = (z - z0) & 1;
-    if (z + 1 < z1) {
-      issue(z + 1, buf ^ 1);
-      cp_async_wait_one();
-    } else {
-      cp_async_wait_all();
+    const int buf = (z - z0) % EL_RING;
+    // the ring slot of plane z + EL_RING - 1 was last read in iteration z - 1,
+    // which every thread has left (the barrier that ends it)
+    issue(z + EL_RING - 1, (buf + EL_RING - 1) % EL_RING);
+    cp_async_wait_ring<EL_RING - 1>();
+    __syncthreads();
+    auto S = [&](int f) { return tiles + (buf * ns + f) * SW; };
+    if (active) {
+      if (OP == OP_GRAD)
+        deriv_line<NP, LP>(S(0), prod, rowt, t, r, D, p0);
+      else
+        deriv_pair<NP, LP, OP == OP_PFORCE>(S(0), S(1), prod, prod + TW, rowt, t, r, D, p0, p1);
     }
     __syncthreads();
-    if (active) deriv_line<NP, LP>(tiles + (buf * NF + fsel) * TW, prod, rowt, t, r, D, p);
-    __syncthreads();
+    // d/dz factor of plane z (src/auxfield.cpp:597-610): mode k = z/2 + base;
+    // Re' = -beta k Im, Im' = beta k Re; zero for mode 0 and Nyquist when base is 0
+    const int kz = (z >> 1) + a.base;
+    const double bz = (a.base == 0 && z < 2) ? 0.0 : ((z & 1) ? a.beta * (double)kz : -(a.beta * (double)kz));
     // epilogue, coalesced over the tile's doubles of plane z
     const size_t pb = (size_t)z * a.stride + (size_t)e0 * NP * NP;
+    const double *sz = OP == OP_PFORCE ? S(ns == 3 ? 2 : 0) : S(a.ndim == 3 ? 1 : 0);  // the z partner
+    const double *su[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) su[c] = (OP == OP_PROJECT && c < a.nadv) ? S(a.ubase + c) : sz;
     for (int i = tid; i < nwords; i += NT) {
-      const int row = i / NP;
-      const int si = row * LP + (i - row * NP);
+      const int si = FLAT ? i : (i / NP) * LP + (i - (i / NP) * NP);
       const size_t gi = pb + i;
       const double g0 = __dadd_rn(Cs[si], A[si]);
       if (OP == OP_GRAD) {
@@ -207,24 +263,19 @@ __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
       } else if (OP == OP_PFORCE) {
         // ((d/dx u + d/dy v) + d/dz w) / dt  (dns/integrate.cpp:272-276)
         double s = __dadd_rn(g0, __dadd_rn(Cs[TW + si], A[TW + si]));
-        if (a.ndim == 3) s = __dadd_rn(s, dz_value(a.fz, z, (size_t)e0 * NP * NP + i, a.stride, a.base, a.beta));
+        if (ns == 3) s = __dadd_rn(s, __dmul_rn(bz, sz[si]));
         a.out[gi] = __dmul_rn(s, a.dtinv);
       } else {
         // u^^ = alpha u^ (times Pr for the scalar) + bvisc grad P
-        // (dns/integrate.cpp:296-309)
+        // (dns/integrate.cpp:296-309); staged: P, P's partner, u^ ...
         const double g1 = __dadd_rn(Cs[TW + si], A[TW + si]);
-        double us[4];  // every component's load issued before the first store
-#pragma unroll
-        for (int c = 0; c < 4; c++) us[c] = c < a.nadv ? a.us[c][gi] : 0.0;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           if (c >= a.nadv) break;
-          double v = __dmul_rn(a.alpha, us[c]);
+          double v = __dmul_rn(a.alpha, su[c][si]);
           if (c == a.ncom) v = __dmul_rn(v, a.prandtl);
           if (c < a.ndim) {
-            const double g = c == 0   ? g0
-                             : c == 1 ? g1
-                                      : dz_value(a.fz, z, (size_t)e0 * NP * NP + i, a.stride, a.base, a.beta);
+            const double g = c == 0 ? g0 : c == 1 ? g1 : __dmul_rn(bz, sz[si]);
             v = __dadd_rn(v, __dmul_rn(a.bvisc, g));
           }
           a.uf[c][gi] = v;
@@ -368,8 +419,8 @@ int plane_group(long long tiles, int nz) {
 template <int NP, int OP>
 int launch_elem(const sx_mesh_s &M, ElemArgs a, cudaStream_t st) {
   constexpr int TE = tile_elems<NP>();
-  constexpr size_t smem = elem_smem<NP, OP>();
-  static_assert(smem <= 227 * 1024, "element tile does not fit in shared memory");
+  static_assert(elem_smem<NP, OP>(max_stage<OP>()) <= 227 * 1024, "element tiles do not fit in shared memory");
+  const size_t smem = elem_smem<NP, OP>(a.nstage);
   if (smem > 48 * 1024)
     SX_CUDA(cudaFuncSetAttribute(k_elem<NP, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   DMat<NP> D;
@@ -419,8 +470,8 @@ extern "C" int sx_field_gradient(sx_mesh mesh, double *d_data, int nz, int plane
     return SX_OK;
   }
   ElemArgs a{};
-  a.f0 = d_data;
-  a.f1 = d_data;
+  a.stage[0] = d_data;
+  a.nstage = 1;
   a.out = d_data;
   a.r0 = dir == 0 ? mesh->ddrdx.p : mesh->ddrdy.p;
   a.s0 = dir == 0 ? mesh->ddsdx.p : mesh->ddsdy.p;
@@ -446,9 +497,13 @@ extern "C" int sx_dns_pressure_forcing(sx_mesh mesh, const double *const *d_us, 
     return SX_ERR_ARG;
   }
   ElemArgs a{};
-  a.f0 = d_us[0];
-  a.f1 = d_us[1];
-  a.fz = ndim == 3 ? d_us[2] : nullptr;
+  a.stage[0] = d_us[0];
+  a.stage[1] = d_us[1];
+  if (ndim == 3) {
+    a.stage[2] = d_us[2];  // read at each plane's partner: the other half of its mode
+    a.partner[2] = 1;
+  }
+  a.nstage = ndim;
   a.out = d_out;
   a.r0 = mesh->ddrdx.p;
   a.s0 = mesh->ddsdx.p;
@@ -481,11 +536,16 @@ extern "C" int sx_dns_project(sx_mesh mesh, const double *const *d_us, const dou
     return SX_ERR_ARG;
   }
   ElemArgs a{};
-  a.f0 = d_p;
-  a.f1 = d_p;
-  a.fz = d_p;
+  a.stage[0] = d_p;
+  a.nstage = 1;
+  if (ndim == 3) {  // P at each plane's partner, for d/dz
+    a.stage[1] = d_p;
+    a.partner[1] = 1;
+    a.nstage = 2;
+  }
+  a.ubase = a.nstage;
   for (int i = 0; i < nadv; i++) {
-    a.us[i] = d_us[i];
+    a.stage[a.nstage++] = d_us[i];
     a.uf[i] = d_uf[i];
   }
   a.r0 = mesh->ddrdx.p;

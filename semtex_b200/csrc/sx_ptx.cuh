@@ -98,8 +98,11 @@ __device__ __forceinline__ void cp_async8_ca(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Wait until every cp.async group of the calling thread has landed.
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-// Wait until at most one (the most recent) cp.async group is still in flight.
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// Wait until at most N (the most recent) cp.async groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_ring() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // 1-D TMA bulk copy this CTA's shared memory -> global, in the calling
 // thread's bulk group.  dst/src 16-B aligned, bytes a multiple of 16.  The
