@@ -1077,7 +1077,7 @@ def main():
     ap.add_argument("--serve-precision", choices=["mixed", "fp64"], default="mixed",
                     help="serving loop: mixed (per mode FP32 CG or FP64 band) or fp64 (band for every mode)")
     ap.add_argument("--serve-slots", type=int, default=4, help="serving loop: requests on the device at once")
-    ap.add_argument("--serve-requests", type=int, default=32,
+    ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")

@@ -314,9 +314,9 @@ __global__ void k_dz_inplace(double *__restrict__ w, int nmodes, int npts, long 
 // writes the value back into those slots.  The CSR g2e lists each node's
 // slots in element order, so the sum here is the reference's sum, rounding
 // for rounding, and each slot is read and written by one thread only.
-constexpr int SMOOTH_CACHE = 8;
+constexpr int SMOOTH_CACHE = 4;  // holders kept in registers; more are walked in the CSR
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_smooth(double *__restrict__ u, const int *__restrict__ ptr, const int *__restrict__ idx,
              const int *__restrict__ emap, const double *__restrict__ Q4, const double *__restrict__ imass,
              int nglobal, int next, int npnp, int nz, int zgroup, long long stride) {
@@ -337,18 +337,19 @@ __global__ void __launch_bounds__(256)
     }
   }
   const double im = imass[g];
-  for (int z = z0; z < z1; z++) {
-    double *p = u + (size_t)z * stride;
+  auto dssum = [&](const double *p) {
     double s = 0.0;
 #pragma unroll
     for (int c = 0; c < SMOOTH_CACHE; c++)
       if (c < n) s = __dadd_rn(s, __dmul_rn(wq[c], p[off[c]]));
-    for (int c = SMOOTH_CACHE; c < n; c++) {  // vertices shared by more than 8 elements
+    for (int c = SMOOTH_CACHE; c < n; c++) {  // vertices shared by more elements
       const int slot = idx[b + c], e = slot / next;
       const int o = e * npnp + emap[slot - e * next];
       s = __dadd_rn(s, __dmul_rn(Q4[o], p[o]));
     }
-    s = __dmul_rn(s, im);
+    return __dmul_rn(s, im);
+  };
+  auto insert = [&](double *p, double s) {
 #pragma unroll
     for (int c = 0; c < SMOOTH_CACHE; c++)
       if (c < n) p[off[c]] = s;
@@ -356,6 +357,19 @@ __global__ void __launch_bounds__(256)
       const int slot = idx[b + c], e = slot / next;
       p[e * npnp + emap[slot - e * next]] = s;
     }
+  };
+  // two planes at a time: both sums' loads are in flight before either
+  // plane is written
+  int z = z0;
+  for (; z + 1 < z1; z += 2) {
+    double *p0 = u + (size_t)z * stride, *p1 = p0 + stride;
+    const double s0 = dssum(p0), s1 = dssum(p1);
+    insert(p0, s0);
+    insert(p1, s1);
+  }
+  if (z < z1) {
+    double *p0 = u + (size_t)z * stride;
+    insert(p0, dssum(p0));
   }
 }
 
