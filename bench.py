@@ -19,7 +19,9 @@ the plain FP64 mode-by-mode form and the batched FP64 form are reported
 beside it, and the lowest-, median- and highest-lambda2 modes are checked
 against the oracle.  Config 2 (32 x 32, N = 8, nz = 64, lambda2 = 1e6 + k^2),
 the multi-mesh batch, the z-transform, the DNS elliptic-phase field
-operations (config 5's field shape) and the serving loop are extra keys.
+operations (config 5's field shape), one DNS elliptic step of config 5 at
+full size (one rank's 16-mode block of an 8-GPU split) and the serving loop
+are extra keys.
 
 Multi-GPU (torchrun): Fourier modes are independent, so the modes of a
 64 N-mode problem are split in contiguous blocks of 64 (the reference's mode
@@ -528,6 +530,7 @@ def run_ours(args, rank, world):
         line["multi_mesh"] = run_multi()
         line["transform_z"] = run_transform()
         line["dns_elliptic_phase"] = run_dns()
+        line["config5_full"] = run_config5(ranks=(0,))
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = run_serving(args.serve_requests, check_oracle=not args.no_cpu,
                                       precision=args.serve_precision, slots=args.serve_slots)
@@ -857,6 +860,138 @@ def run_dns(reps=5, nz=256, check=True):
     return out
 
 
+def run_config5(ranks=(0,), pressure_checks=None, viscous_checks=None, reps=3):
+    """One DNS elliptic step of config 5 at full size (128 x 64 quads, N = 10,
+    nz = 256: 128 modes) as the ranks of an 8-GPU node take it, one rank's
+    block of 16 modes at a time on this GPU (modes are independent: the step
+    time of the node is the slowest rank's).  Per rank the step is, all on
+    the device: the wave step (order 2) of the velocity levels, the pressure
+    forcing, the pressure solve (natural walls, every mode's band factor
+    resident: 16 x 6.1 GB; k = 0 singular, pinned), project, and the three
+    viscous solves (lambda2 = 1/(nu dt) = 4e6 + k^2) in the mixed form.
+    Inputs: seeded random velocity levels and nonlinear terms, made
+    continuous by Field::smooth.  Checked against the oracle: the pressure
+    solve of `pressure_checks` modes (LAPACK dpbtrf factor), the viscous
+    solve of `viscous_checks` modes (oracle Jacobi PCG to 1e-14), and the
+    forcing operations on those modes' planes."""
+    import torch
+    import semtex_b200 as sx
+    from oracle import dns
+    from oracle.oracle import DIRECT as O_DIRECT
+    from oracle.oracle import JACPCG as O_JACPCG
+    from oracle.oracle import OracleMesh, OracleSystem
+    from semtex_b200.workloads import config5_block
+    torch.cuda.set_device(0)
+    sptr = torch.cuda.current_stream().cuda_stream
+    pressure_checks = [1] if pressure_checks is None else list(pressure_checks)
+    viscous_checks = [1] if viscous_checks is None else list(viscous_checks)
+    out = {"workload": None, "ranks": {}}
+    ptr = lambda ts: [t.data_ptr() for t in ts]  # noqa: E731
+    for rank in ranks:
+        b = config5_block(rank=rank)
+        out["workload"] = b.name
+        mv, mp = b.mesh_v, b.mesh_p
+        nz, n = b.nz, mv.nplane
+        t0 = time.perf_counter()
+        mesh_v, mesh_p = sx.Mesh(mv), sx.Mesh(mp)
+        Sp = sx.ModalMatrixSys(mesh_p, base_mode=b.base_mode, num_modes=b.num_modes, method=sx.DIRECT,
+                               lambda2_modes=b.lambda2_p, betak2_modes=b.betak2)
+        Sv = sx.ModalMatrixSys(mesh_v, base_mode=b.base_mode, num_modes=b.num_modes, method=sx.JACPCG,
+                               lambda2_modes=b.lambda2_v, betak2_modes=b.betak2)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        order = 2
+        us = [_dns_fields(nz, n, 3, 500 + 10 * rank + q) for q in range(order)]
+        uf = [_dns_fields(nz, n, 3, 600 + 10 * rank + q) for q in range(order)]
+        for lev in us + uf:
+            for x in lev:
+                sx.field_smooth(mesh_v, x.data_ptr(), nz, n, stream=sptr)
+        h = [torch.empty_like(us[0][0]) for _ in range(3)]
+        fp, p = torch.empty_like(h[0]), torch.zeros_like(h[0])
+        uo = [torch.zeros_like(h[0]) for _ in range(3)]
+        stats = {}
+
+        def step(keep=None):
+            sx.wave_prop([ptr(x) for x in us], [ptr(x) for x in uf], ptr(h), nz * n, b.dt, stream=sptr)
+            sx.pressure_forcing(mesh_v, ptr(h), fp.data_ptr(), nz, n, b.dt, b.beta, b.base_mode, stream=sptr)
+            if keep is not None:
+                keep["h"] = [x.clone() for x in h]
+                keep["fp"] = fp.clone()
+            stats["p"] = Sp.solve_batched(p.data_ptr(), fp.data_ptr(), 0, nz, n, sx.FP64, stream=sptr)
+            sx.project(mesh_v, ptr(h), p.data_ptr(), ptr(h), nz, n, b.dt, b.nu, ndim=3, beta=b.beta,
+                       base_mode=b.base_mode, stream=sptr)
+            if keep is not None:
+                keep["fv"] = [x.clone() for x in h]
+            for c in range(3):
+                stats[f"v{c}"] = Sv.solve_batched(uo[c].data_ptr(), h[c].data_ptr(), 0, nz, n, sx.MIXED_FP32,
+                                                  tol_rel=1e-12, max_refine=20, stream=sptr)
+
+        step()  # warm-up: graphs captured, iteration counts settled
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        ms = float(np.median(ts))
+        dof = (3 * mv.n_unique + mp.n_unique) * b.planes_solved
+        res = {"modes": [b.base_mode, b.base_mode + b.num_modes - 1], "setup_s": setup_s, "ms_per_step": ms,
+               "dof_solves_per_s": dof / (ms * 1e-3), "dof_solves_per_step": dof,
+               "pressure_band_gb": Sp.device_bytes / 1e9,
+               "viscous_iterations": [stats[f"v{c}"]["iterations_total"] for c in range(3)],
+               "viscous_refinements": [stats[f"v{c}"]["refinements"] for c in range(3)],
+               "viscous_final_rel_residual": max(stats[f"v{c}"]["final_rel_residual"] for c in range(3)),
+               "nband_p": mp.nband, "nband_v": mv.nband}
+        keep = {}
+        step(keep)
+        torch.cuda.synchronize()
+        errs = {}
+        mine_p = [k for k in pressure_checks if b.base_mode <= k < b.base_mode + b.num_modes]
+        mine_v = [k for k in viscous_checks if b.base_mode <= k < b.base_mode + b.num_modes]
+        if mine_p or mine_v:
+            geo = dns.Geometry(mv)
+        for k in sorted(set(mine_p + mine_v)):
+            lo = 2 * (k - b.base_mode)
+            sl = slice(lo, lo + 2)
+            hh = [x[sl].cpu().numpy() for x in keep["h"]]
+            pp = p[sl].cpu().numpy()
+            e = {}
+            want_f = dns.pressure_forcing(geo, hh, b.dt, b.beta, base_mode=k)
+            got_f = keep["fp"][sl].cpu().numpy()
+            e["pressure_forcing"] = float(np.abs(got_f - want_f).max() / np.abs(want_f).max())
+            want_v = dns.project(geo, hh, pp, b.dt, b.nu, ndim=3, beta=b.beta, base_mode=k)
+            got_v = [x[sl].cpu().numpy() for x in keep["fv"]]
+            e["project"] = float(max(np.abs(g - w).max() / np.abs(w).max() for g, w in zip(got_v, want_v)))
+            planes = [0] if k == 0 else [0, 1]
+            if k in mine_p:
+                t1 = time.perf_counter()
+                osys = OracleSystem(OracleMesh(mp), 0.0, float(k * k), O_DIRECT, factor="lapack")
+                uo_p = np.array([osys.solve_plane(got_f[q], None)[0] for q in planes])
+                del osys
+                e["pressure_solve"] = rel_err(pp[planes], uo_p)
+                e["oracle_pressure_s"] = time.perf_counter() - t1
+            if k in mine_v:
+                osys = OracleSystem(OracleMesh(mv), float(b.lambda2_v[0]), float(k * k), O_JACPCG)
+                uo_v = np.array([osys.solve_plane(got_v[0][q], None, tol_rel=1e-14, step_max=20000)[0]
+                                 for q in planes])
+                del osys
+                e["viscous_solve"] = rel_err(uo[0][sl].cpu().numpy()[planes], uo_v)
+            errs[str(k)] = e
+        res["rel_err_vs_oracle"] = errs
+        out["ranks"][str(rank)] = res
+        del Sp, Sv, mesh_v, mesh_p, us, uf, h, fp, p, uo, keep
+        torch.cuda.empty_cache()
+    worst = [v for r in out["ranks"].values() for e in r["rel_err_vs_oracle"].values()
+             for key, v in e.items() if key.endswith("solve")]
+    out["worst_solve_err"] = max(max(x) for x in worst) if worst else None
+    out["node_ms_per_step"] = max(r["ms_per_step"] for r in out["ranks"].values())
+    out["note"] = ("ranks of an 8-GPU node (16 modes each), run one after another on this GPU; the node's step "
+                   "time is its slowest rank's (no collective in the elliptic phase)")
+    return out
+
+
 def _build_request(args):
     """Build one planned serving request (a spawned worker process)."""
     spec, seed = args
@@ -1079,6 +1214,10 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=4, help="serving loop: requests on the device at once")
     ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the mixed-size serving trace to run (0 skips it)")
+    ap.add_argument("--config5-ranks", default=None, metavar="R,R,...",
+                    help="run only the config-5 elliptic step for these ranks of the 8-GPU split, checking "
+                         "pressure modes 0, 1, 2, 31, 127 and viscous modes 1, 127 where they fall, and print "
+                         "its JSON (not a bench line)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
     ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform", "dns"], default=None,
@@ -1093,6 +1232,11 @@ def main():
         print(json.dumps({"serving_only": run_serving(args.serve_only, check_oracle=False,
                                                       precision=args.serve_precision, slots=args.serve_slots)}),
               flush=True)
+        return
+    if args.config5_ranks:
+        ranks = tuple(int(r) for r in args.config5_ranks.split(","))
+        print(json.dumps({"config5_full": run_config5(ranks, pressure_checks=(0, 1, 2, 31, 127),
+                                                      viscous_checks=(1, 127))}), flush=True)
         return
     if args.profile:
         run_profile(args)

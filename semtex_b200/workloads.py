@@ -205,6 +205,52 @@ def config5(nx=128, ny=64, np_=11, nz=256, seed=5, nu=5e-4, dt=5e-4):
 
 
 @dataclass
+class DnsBlock:
+    """One rank's share of a DNS elliptic step: its block of Fourier modes
+    of the velocity (Dirichlet walls) and pressure (natural walls) meshes of
+    one geometry, with the viscous and pressure Helmholtz constants of the
+    block's modes."""
+    name: str
+    mesh_v: QuadMesh
+    mesh_p: QuadMesh
+    base_mode: int
+    num_modes: int
+    beta: float
+    nu: float
+    dt: float
+    lambda2_v: np.ndarray        # per local mode: 1/(nu dt)
+    lambda2_p: np.ndarray        # per local mode: 0
+    betak2: np.ndarray           # per local mode: (beta k)^2
+    info: dict = field(default_factory=dict)
+
+    @property
+    def nz(self):
+        return 2 * self.num_modes
+
+    @property
+    def planes_solved(self):
+        return self.nz - 1 if self.base_mode == 0 else self.nz
+
+
+def config5_block(world=8, rank=0, nx=128, ny=64, np_=11, modes_per_rank=16, seed=5, nu=5e-4, dt=5e-4):
+    """Rank `rank`'s block of config 5 (128 x 64 quads jittered +-15 %,
+    N = 10, [0, 2pi] x [0, 1], periodic in x) split over `world` ranks as
+    the reference splits modes (partition.mode_block): with the default
+    8 x 16 modes, nz = 256 planes in all.  All 128 pressure factors (about
+    5.9 GB each) exceed one GPU; a block of 16 holds about 94 GB."""
+    from .partition import mode_block
+    nm = modes_per_rank * world
+    base, count = mode_block(nm, world, rank)
+    mv = _jittered_channel(nx, ny, np_, 0.15, seed)
+    mp = rect_mesh(nx, ny, np_, 0.0, 2 * np.pi, 0.0, 1.0, jitter=0.15, seed=seed, periodic_x=True,
+                   bc={"bottom": "N", "top": "N"})
+    k = np.arange(base, base + count, dtype=np.float64)
+    return DnsBlock(f"cfg5_channel_{nx}x{ny}_N{np_ - 1}_nz{2 * nm}", mv, mp, base, count, 1.0, nu, dt,
+                    np.full(count, 1.0 / (nu * dt)), np.zeros(count), k ** 2,
+                    info={"modes_total": nm, "rank": rank, "world": world, "jitter": 0.15})
+
+
+@dataclass
 class ServeRequest:
     t_arrival: float             # seconds after the first arrival
     mesh: QuadMesh
