@@ -23,6 +23,7 @@
 
 #include "sx_internal.h"
 #include "sx_kernels.cuh"
+#include "sx_ptx.cuh"
 
 namespace sx {
 
@@ -275,71 +276,125 @@ __global__ void __launch_bounds__(256) k_potrf(const SysDesc *__restrict__ sys, 
   if (tid == 0 && bad) atomicOr(S.status, 1 << SX_ERR_NOT_SPD);
 }
 
-// C (+)= alpha * A^T B on NB x NB smem tiles; thread (ty, tx) of a 16x16
-// layout owns rows ty + 16a, cols tx + 16b.
-__device__ __forceinline__ void tile_gemm_tn(double *C, const double *A, const double *B,
-                                             double alpha, bool accumulate) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-  for (int l = 0; l < NB; l++) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int a = 0; a < 4; a++) av[a] = A[l * LDT + ty + 16 * a];
-#pragma unroll
-    for (int b = 0; b < 4; b++) bv[b] = B[l * LDT + tx + 16 * b];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+// Tile products on the FP64 tensor cores (mma.sync m8n8k4, f64).  The two
+// factor tiles of a product are staged into shared memory with rows padded
+// to LDM = 68 doubles (68 = 4 mod 16: the 4 x 8 slab a fragment reads, rows
+// t = 0..3 and columns g = 0..7, falls on 16 distinct bank pairs in each
+// half-warp).  Warp w owns rows 16 (w / 2) .. +16 and columns 32 (w % 2) ..
+// +32 of the 64 x 64 result: 2 x 4 blocks of 8 x 8, two accumulators a
+// thread each, held in registers from the first product to the store.
+constexpr int LDM = NB + 4;
+
+__device__ __forceinline__ void tile_stage_mma(double *dst, const double *__restrict__ src) {
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx >> 6, c = idx & (NB - 1);
+    cp_async8_ca(dst + r * LDM + c, src + r * LDT + c);
   }
+}
+
+struct MmaAcc {
+  double v[2][4][2];
+};
+
+// This thread's result elements: (row r0 + 8m + g, column c0 + 8n + 2t + q).
+__device__ __forceinline__ void mma_coords(int &r0, int &c0, int &g, int &t) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  g = lane >> 2;
+  t = lane & 3;
+  r0 = (w >> 1) * 16;
+  c0 = (w & 1) * 32;
+}
+
+__device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// acc += (neg ? -1 : 1) * A^T B over the NB rows of the staged tiles:
+// entry (r, c) gains sum_l A[l][r] B[l][c].
+__device__ __forceinline__ void mma_tn(MmaAcc &acc, const double *As, const double *Bs, bool neg) {
+  int r0, c0, g, t;
+  mma_coords(r0, c0, g, t);
+#pragma unroll 4
+  for (int l0 = 0; l0 < NB; l0 += 4) {
+    const double *Ar = As + (l0 + t) * LDM + r0 + g, *Br = Bs + (l0 + t) * LDM + c0 + g;
+    double a[2], b[4];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+    for (int m = 0; m < 2; m++) a[m] = neg ? -Ar[8 * m] : Ar[8 * m];
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
-      double *c = &C[(ty + 16 * a) * LDT + tx + 16 * b];
-      *c = accumulate ? (*c + alpha * acc[a][b]) : alpha * acc[a][b];
-    }
+    for (int n = 0; n < 4; n++) b[n] = Br[8 * n];
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+      for (int n = 0; n < 4; n++) mma_f64(acc.v[m][n][0], acc.v[m][n][1], a[m], b[n]);
+  }
+}
+
+// Load (or zero) and store this thread's result elements of a band tile.
+__device__ __forceinline__ void mma_load(MmaAcc &acc, const double *__restrict__ T) {
+  int r0, c0, g, t;
+  mma_coords(r0, c0, g, t);
+#pragma unroll
+  for (int m = 0; m < 2; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+      for (int q = 0; q < 2; q++) acc.v[m][n][q] = T ? T[(r0 + 8 * m + g) * LDT + c0 + 8 * n + 2 * t + q] : 0.0;
+}
+
+__device__ __forceinline__ void mma_store(double *T, const MmaAcc &acc) {
+  int r0, c0, g, t;
+  mma_coords(r0, c0, g, t);
+#pragma unroll
+  for (int m = 0; m < 2; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+      for (int q = 0; q < 2; q++) T[(r0 + 8 * m + g) * LDT + c0 + 8 * n + 2 * t + q] = acc.v[m][n][q];
 }
 
 // Off-diagonal tiles of block row k: U(k, k+i) = U_kk^-T A(k, k+i).
-__global__ void __launch_bounds__(256) k_trsm(const SysDesc *__restrict__ sys, int k) {
+__global__ void __launch_bounds__(256, 3) k_trsm(const SysDesc *__restrict__ sys, int k) {
   const SysDesc S = sys[blockIdx.y];
   const int i = blockIdx.x + 1;
   if (k >= S.nblk || i > S.J || k + i >= S.nblk) return;
   extern __shared__ __align__(16) double smt[];
-  double *X = smt, *B = X + TSZ, *C = B + TSZ;
+  double *X = smt, *B = X + NB * LDM;
   double *T = S.tiles + ((size_t)(k + i) * (S.J + 1) + i) * TSZ;
-  tile_load(X, S.dinv + (size_t)k * TSZ);
-  tile_load(B, T);
+  tile_stage_mma(X, S.dinv + (size_t)k * TSZ);
+  tile_stage_mma(B, T);
+  cp_async_commit();
+  MmaAcc acc;
+  mma_load(acc, nullptr);
+  cp_async_wait_all();
   __syncthreads();
-  tile_gemm_tn(C, X, B, 1.0, false);
-  __syncthreads();
-  tile_store(T, C);
+  mma_tn(acc, X, B, false);
+  mma_store(T, acc);
 }
 
 // Trailing update inside the band: A(k+i, k+j) -= U(k,k+i)^T U(k,k+j),
-// 1 <= i <= j <= J.
-__global__ void __launch_bounds__(256) k_update(const SysDesc *__restrict__ sys, int k,
-                                                const int2 *__restrict__ pairs) {
+// 1 <= i <= j <= J.  The target tile goes from global memory to the
+// accumulators and back; the products are added negated.
+__global__ void __launch_bounds__(256, 3) k_update(const SysDesc *__restrict__ sys, int k,
+                                                   const int2 *__restrict__ pairs) {
   const SysDesc S = sys[blockIdx.y];
   const int2 pr = pairs[blockIdx.x];
   const int i = pr.x, j = pr.y;
   if (k >= S.nblk || j > S.J || k + j >= S.nblk) return;
   extern __shared__ __align__(16) double smt[];
-  double *A = smt, *B = A + TSZ, *C = B + TSZ;
+  double *A = smt, *B = A + NB * LDM;
   const size_t J1 = S.J + 1;
   double *Ct = S.tiles + ((size_t)(k + j) * J1 + (j - i)) * TSZ;
-  tile_load(A, S.tiles + ((size_t)(k + i) * J1 + i) * TSZ);
-  tile_load(B, S.tiles + ((size_t)(k + j) * J1 + j) * TSZ);
-  tile_load(C, Ct);
+  tile_stage_mma(A, S.tiles + ((size_t)(k + i) * J1 + i) * TSZ);
+  tile_stage_mma(B, S.tiles + ((size_t)(k + j) * J1 + j) * TSZ);
+  cp_async_commit();
+  MmaAcc acc;
+  mma_load(acc, Ct);
+  cp_async_wait_all();
   __syncthreads();
-  tile_gemm_tn(C, A, B, -1.0, true);
-  __syncthreads();
-  tile_store(Ct, C);
+  mma_tn(acc, A, B, true);
+  mma_store(Ct, acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -434,16 +489,16 @@ int factor_batch(std::vector<System *> &systems, cudaStream_t st, bool sync) {
     for (int i = 1; i <= j; i++) pairs.push_back(make_int2(i, j));
   DBuf<int2> dpairs;
   if (!pairs.empty()) SX_TRY(dpairs.upload_on(pairs.data(), pairs.size(), st));
-  const size_t sm3 = 3 * TSZ * sizeof(double), sm2 = 2 * TSZ * sizeof(double);
+  const size_t smm = 2 * NB * LDM * sizeof(double), sm2 = 2 * TSZ * sizeof(double);
   SX_CUDA(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-  SX_CUDA(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
-  SX_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  SX_CUDA(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm));
+  SX_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm));
   const int ns = (int)systems.size();
   for (int k = 0; k < maxblk; k++) {
     k_potrf<<<ns, 256, sm2, st>>>(dd.p, k);
     if (maxJ > 0) {
-      k_trsm<<<dim3(maxJ, ns), 256, sm3, st>>>(dd.p, k);
-      k_update<<<dim3((unsigned)pairs.size(), ns), 256, sm3, st>>>(dd.p, k, dpairs.p);
+      k_trsm<<<dim3(maxJ, ns), 256, smm, st>>>(dd.p, k);
+      k_update<<<dim3((unsigned)pairs.size(), ns), 256, smm, st>>>(dd.p, k, dpairs.p);
     }
   }
   SX_CUDA(cudaGetLastError());
