@@ -1211,7 +1211,7 @@ def main():
                          "and print its JSON (not a bench line)")
     ap.add_argument("--serve-precision", choices=["mixed", "fp64"], default="mixed",
                     help="serving loop: mixed (per mode FP32 CG or FP64 band) or fp64 (band for every mode)")
-    ap.add_argument("--serve-slots", type=int, default=4, help="serving loop: requests on the device at once")
+    ap.add_argument("--serve-slots", type=int, default=8, help="serving loop: requests on the device at once")
     ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the mixed-size serving trace to run (0 skips it)")
     ap.add_argument("--config5-ranks", default=None, metavar="R,R,...",

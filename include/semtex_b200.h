@@ -432,7 +432,7 @@ typedef struct sx_server_s *sx_server;
 
 typedef struct {
   unsigned long long hbm_budget; /* device bytes for caches + in-flight work; 0 = 70% of free */
-  int slots;                     /* requests on the device at once; 0 = 4                      */
+  int slots;                     /* requests on the device at once; 0 = 8                      */
   int precision;                 /* SX_MIXED_FP32 (PCG) or SX_FP64 (DIRECT, cached factors)     */
   double tol_rel;                /* mixed: FP64 relative residual target; 0 = 1e-12            */
   int max_refine;                /* mixed: refinement rounds cap; 0 = 30                        */

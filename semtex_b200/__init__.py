@@ -573,7 +573,7 @@ class Server:
     batch; geometry and systems stay resident across requests.
     """
 
-    def __init__(self, slots=4, precision=MIXED_FP32, hbm_budget=0, tol_rel=1e-12,
+    def __init__(self, slots=8, precision=MIXED_FP32, hbm_budget=0, tol_rel=1e-12,
                  max_refine=30, inner_iters=12, max_batch=8):
         cfg = ServerConfig(int(hbm_budget), slots, precision, tol_rel, max_refine, inner_iters, max_batch)
         h = C.c_void_p()

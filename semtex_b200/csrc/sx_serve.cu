@@ -743,7 +743,7 @@ extern "C" int sx_server_create(const sx_server_config *cfg, sx_server *out) {
   if (cfg) S->cfg = *cfg;
   sx_server_config &c = S->cfg;
   if (c.precision != SX_FP64) c.precision = SX_MIXED_FP32;
-  if (c.slots <= 0) c.slots = 4;
+  if (c.slots <= 0) c.slots = 8;
   if (c.slots > 64) return SX_ERR_ARG;
   if (c.tol_rel <= 0.0) c.tol_rel = 1e-12;
   if (c.max_refine <= 0) c.max_refine = 30;
