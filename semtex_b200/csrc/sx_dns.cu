@@ -75,27 +75,32 @@ constexpr int stage_words() {
   return (tile_words<NP>() + 1) & ~1;
 }
 // fields staged per plane, at most: GRAD u; PFORCE u, v and w's partner
-// plane; PROJECT P, P's partner plane and up to four u^ components
+// plane; PROJECT P and P's partner plane (its u^ components go straight to
+// registers: only the epilogue reads them)
 template <int OP>
 constexpr int max_stage() {
-  return OP == OP_GRAD ? 1 : OP == OP_PFORCE ? 3 : 6;
+  return OP == OP_GRAD ? 1 : OP == OP_PFORCE ? 3 : 2;
 }
 template <int OP>
 constexpr int n_jobs() {
   return OP == OP_GRAD ? 1 : 2;  // derivatives formed per plane
 }
-// planes in the copy ring: two in flight while a third is worked on; one
-// for project, whose five or six staged fields would otherwise leave room
-// for two CTAs an SM
+// planes in the copy ring: two in flight while a third is worked on
 template <int OP>
 constexpr int el_ring() {
-  return OP == OP_PROJECT ? 2 : 3;
+  return 3;
 }
-// tiles [ring slots][staged fields], then A [jobs], C [jobs]
+// product arrays a line thread writes: project keeps its x and y
+// derivatives apart; pressure forcing needs only their sum
+template <int OP>
+constexpr int n_prod() {
+  return OP == OP_PROJECT ? 2 : 1;
+}
+// tiles [ring slots][staged fields], then A [products], C [products]
 template <int NP, int OP>
 constexpr size_t elem_smem(int nstage) {
   return sizeof(double) *
-         ((size_t)el_ring<OP>() * nstage * stage_words<NP>() + 2 * n_jobs<OP>() * tile_words<NP>());
+         ((size_t)el_ring<OP>() * nstage * stage_words<NP>() + 2 * n_prod<OP>() * tile_words<NP>());
 }
 // a row group and a column group; with two jobs a thread forms both, each
 // D entry it reads serving two multiply-adds
@@ -113,7 +118,8 @@ struct ElemArgs {
   // read at plane z ^ 1 (the other half of plane z's Fourier mode)
   const double *stage[6];
   int partner[6];
-  int nstage, ubase;      // PROJECT: the first u^ component's stage
+  int nstage;
+  const double *us[4];    // PROJECT: u^ components
   double *out;            // GRAD: the field itself (in place); PFORCE: the forcing
   double *uf[4];          // PROJECT: results
   // partials of job 0 (r, s) and job 1 (r, s)
@@ -142,8 +148,9 @@ __device__ __forceinline__ void deriv_line(const double *__restrict__ T, double 
   }
 }
 
-// Both jobs of a line: two fields with a partial each (TWO_FIELDS) or one
-// field with two partials (the x and y derivatives of the same P).
+// Both jobs of a line: two fields with a partial each (TWO_FIELDS: u's
+// x-product plus v's y-product, summed into d0) or one field with two
+// partials (the x and y derivatives of the same P, into d0 and d1).
 template <int NP, int LP, bool TWO_FIELDS>
 __device__ __forceinline__ void deriv_pair(const double *__restrict__ T0, const double *__restrict__ T1,
                                            double *__restrict__ d0, double *__restrict__ d1, bool rowt, int t,
@@ -166,8 +173,12 @@ __device__ __forceinline__ void deriv_pair(const double *__restrict__ T0, const 
       x = fma(u[k], dk, x);
       if (TWO_FIELDS) y = fma(v[k], dk, y);
     }
-    d0[b + j * step] = __dmul_rn(x, p0[j]);
-    d1[b + j * step] = __dmul_rn(TWO_FIELDS ? y : x, p1[j]);
+    if (TWO_FIELDS) {
+      d0[b + j * step] = __dadd_rn(__dmul_rn(x, p0[j]), __dmul_rn(y, p1[j]));
+    } else {
+      d0[b + j * step] = __dmul_rn(x, p0[j]);
+      d1[b + j * step] = __dmul_rn(x, p1[j]);
+    }
   }
 }
 
@@ -181,8 +192,8 @@ __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
   extern __shared__ __align__(16) double sm[];
   const int ns = a.nstage;
   double *tiles = sm;                  // [EL_RING buffers][ns][SW]
-  double *A = sm + EL_RING * ns * SW;  // [NJ][TW] row products
-  double *Cs = A + NJ * TW;          // [NJ][TW] column products
+  double *A = sm + EL_RING * ns * SW;  // [n_prod][TW] row products
+  double *Cs = A + n_prod<OP>() * TW;  // [n_prod][TW] column products
   const int tid = threadIdx.x;
   const int e0 = blockIdx.x * TE;
   const int ne = min(TE, a.nel - e0);
@@ -237,6 +248,19 @@ __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
     cp_async_wait_ring<EL_RING - 1>();
     __syncthreads();
     auto S = [&](int f) { return tiles + (buf * ns + f) * SW; };
+    // project's u^ values at this thread's epilogue points, loaded now so
+    // that they arrive while the derivatives are formed
+    constexpr int NI = OP == OP_PROJECT ? (TE * NP * NP + NT - 1) / NT : 1;
+    double ur[NI][4];
+    if (OP == OP_PROJECT) {
+      const size_t pz = (size_t)z * a.stride + (size_t)e0 * NP * NP;
+#pragma unroll
+      for (int q = 0; q < NI; q++) {
+        const int i = tid + q * NT;
+#pragma unroll
+        for (int c = 0; c < 4; c++) ur[q][c] = (i < nwords && c < a.nadv) ? a.us[c][pz + i] : 0.0;
+      }
+    }
     if (active) {
       if (OP == OP_GRAD)
         deriv_line<NP, LP>(S(0), prod, rowt, t, r, D, p0);
@@ -251,18 +275,21 @@ __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
     // epilogue, coalesced over the tile's doubles of plane z
     const size_t pb = (size_t)z * a.stride + (size_t)e0 * NP * NP;
     const double *sz = OP == OP_PFORCE ? S(ns == 3 ? 2 : 0) : S(a.ndim == 3 ? 1 : 0);  // the z partner
-    const double *su[4];
 #pragma unroll
-    for (int c = 0; c < 4; c++) su[c] = (OP == OP_PROJECT && c < a.nadv) ? S(a.ubase + c) : sz;
-    for (int i = tid; i < nwords; i += NT) {
+    for (int q = 0; q < (OP == OP_PROJECT ? NI : (TE * NP * NP + NT - 1) / NT); q++) {
+      const int i = tid + q * NT;
+      if (i >= nwords) break;
       const int si = FLAT ? i : (i / NP) * LP + (i - (i / NP) * NP);
       const size_t gi = pb + i;
       const double g0 = __dadd_rn(Cs[si], A[si]);
       if (OP == OP_GRAD) {
         a.out[gi] = g0;
       } else if (OP == OP_PFORCE) {
-        // ((d/dx u + d/dy v) + d/dz w) / dt  (dns/integrate.cpp:272-276)
-        double s = __dadd_rn(g0, __dadd_rn(Cs[TW + si], A[TW + si]));
+        // ((d/dx u + d/dy v) + d/dz w) / dt  (dns/integrate.cpp:272-276); the
+        // four derivative products are summed as (s terms) + (r terms), each
+        // pair added where it is formed, so each takes one trip through
+        // shared memory
+        double s = g0;
         if (ns == 3) s = __dadd_rn(s, __dmul_rn(bz, sz[si]));
         a.out[gi] = __dmul_rn(s, a.dtinv);
       } else {
@@ -272,7 +299,7 @@ __global__ void __launch_bounds__(elem_threads<OP>(), elem_min_blocks<OP>())
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           if (c >= a.nadv) break;
-          double v = __dmul_rn(a.alpha, su[c][si]);
+          double v = __dmul_rn(a.alpha, ur[OP == OP_PROJECT ? q : 0][c]);
           if (c == a.ncom) v = __dmul_rn(v, a.prandtl);
           if (c < a.ndim) {
             const double g = c == 0 ? g0 : c == 1 ? g1 : __dmul_rn(bz, sz[si]);
@@ -557,9 +584,8 @@ extern "C" int sx_dns_project(sx_mesh mesh, const double *const *d_us, const dou
     a.partner[1] = 1;
     a.nstage = 2;
   }
-  a.ubase = a.nstage;
   for (int i = 0; i < nadv; i++) {
-    a.stage[a.nstage++] = d_us[i];
+    a.us[i] = d_us[i];
     a.uf[i] = d_uf[i];
   }
   a.r0 = mesh->ddrdx.p;
