@@ -100,3 +100,42 @@ def test_mesh_create_rejects_band_too_narrow():
     widest = max(int(g.max() - g.min()) + 1 for g in
                  (m.btog[e][m.bmask[e] == 0] for e in range(m.nel)) if len(g))
     assert widest == m.nband
+
+
+def test_elliptic_phase_entry_points_refuse_bad_arguments():
+    """The DNS elliptic-phase entry points check their arguments before
+    touching the device: a missing mesh or pointer, a wave step of order
+    outside 1-3 or more than four fields is SX_ERR_ARG; an empty wave step
+    is a no-op."""
+    import semtex_b200 as sx
+    L = sx.lib
+    ARG = 1
+    null = C.c_void_p()
+    ptrs = sx._ptrs([1, 2, 3])  # never dereferenced: the checks fail first
+    assert L.sx_field_gradient(null, 8, 4, 100, 0, 1.0, 0, null) == ARG
+    assert L.sx_field_smooth(null, 8, 4, 100, null) == ARG
+    assert L.sx_dns_pressure_forcing(null, ptrs, 3, 8, 4, 100, 0.1, 1.0, 0, null) == ARG
+    assert L.sx_dns_project(null, ptrs, 8, ptrs, 3, 3, 3, 4, 100, 0.1, 0.01, 1.0, 1.0, 0, null) == ARG
+    assert L.sx_mesh_partials(null, 0, None, None, None, None, None) == ARG
+    one = sx._ptrs([8])
+    assert L.sx_dns_wave_prop(one, one, one, 1, 0, 10, 0.1, null) == ARG    # order 0
+    assert L.sx_dns_wave_prop(one, one, one, 1, 4, 10, 0.1, null) == ARG    # order 4
+    assert L.sx_dns_wave_prop(one, one, one, 5, 1, 10, 0.1, null) == ARG    # five fields
+    assert L.sx_dns_wave_prop(one, one, one, 1, 1, -1, 0.1, null) == ARG    # negative length
+    assert L.sx_dns_wave_prop(one, one, one, 1, 1, 0, 0.1, null) == 0       # nothing to do
+
+
+def test_config5_block_split():
+    """config5_block: the 8 x 16 mode split of config 5, as the reference
+    splits modes across processes; betak2 = k^2 of the block's modes."""
+    from semtex_b200.partition import mode_block
+    from semtex_b200.workloads import config5_block
+    b = config5_block(world=8, rank=7, nx=8, ny=4, np_=5)
+    assert (b.base_mode, b.num_modes) == mode_block(128, 8, 7) == (112, 16)
+    assert b.nz == 32 and b.planes_solved == 32
+    assert np.array_equal(b.betak2, np.arange(112, 128, dtype=float) ** 2)
+    assert np.all(b.lambda2_v == 1.0 / (b.nu * b.dt)) and np.all(b.lambda2_p == 0.0)
+    b0 = config5_block(world=8, rank=0, nx=8, ny=4, np_=5)
+    assert b0.base_mode == 0 and b0.planes_solved == 31
+    # velocity: Dirichlet walls (essential nodes numbered last); pressure: none
+    assert b0.mesh_v.nsolve < b0.mesh_v.nglobal and b0.mesh_p.nsolve == b0.mesh_p.nglobal
