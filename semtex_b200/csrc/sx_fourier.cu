@@ -228,62 +228,103 @@ __global__ void __launch_bounds__(128) k_z_inv(double *__restrict__ data, int np
 }
 
 // Lengths 128, 256, 512: a block of four warps takes 32 points (lane =
-// point); the half-length complex sequence of each point lies in shared
-// memory, Zr/Zi[m][32], and the warps share each radix-2 stage's
-// butterflies, a barrier between stages.  Same steps as the register
-// kernels; loads and stores of a plane are 32 consecutive doubles.
+// point); the half-length complex sequence z (length M = N/2) of each point
+// lies in shared memory, Zr/Zi[m][32], in natural order.  The complex FFT
+// of length M = M1 M2 runs in four steps with m = M2 m1 + m2 and
+// k = k1 + M1 k2: (1) the M2 FFTs of length M1 over m1, each a warp's, in
+// registers; (2) the twiddles W_M^(m2 k1); (3) the M1 FFTs of length M2
+// over m2, in registers.  Two round trips through shared memory and two
+// barriers, against one per radix-2 stage (log2 M).  Z_k ends at row
+// M2 (k mod M1) + k / M1.  The real-to-complex steps around it are the
+// register kernels'; loads and stores of a plane are 32 consecutive doubles.
 constexpr size_t zsmem(int nz) { return (size_t)nz * 32 * sizeof(double); }
 
-template <int N>
-__device__ __forceinline__ void smem_stages(double *Zr, double *Zi, bool inv) {
-  constexpr int M = N / 2;
+template <int M>
+struct FourStep {
+  static constexpr int M1 = M >= 128 ? 16 : 8, M2 = M / M1;
+  static __device__ __forceinline__ int row(int k) { return M2 * (k % M1) + k / M1; }
+};
+
+// W_M^e = exp(-2 pi i e / M) from the half-turn table (conjugated for the
+// inverse).
+template <int M>
+__device__ __forceinline__ void twiddle(int e, bool inv, double &wr, double &wi) {
+  e &= M - 1;
+  const bool neg = e >= M / 2;
+  const int t = (neg ? e - M / 2 : e) * (TWN / M);
+  wr = neg ? -c_twr[t] : c_twr[t];
+  wi = neg ? -c_twi[t] : c_twi[t];
+  if (inv) wi = -wi;
+}
+
+template <int M, bool INV>
+__device__ __forceinline__ void four_step(double *Zr, double *Zi) {
+  using F = FourStep<M>;
+  constexpr int M1 = F::M1, M2 = F::M2, L1 = ilog2c(M1), L2 = ilog2c(M2);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll 1
-  for (int len = 2; len <= M; len <<= 1) {
-    const int h = len >> 1;
-    for (int b = w; b < M / 2; b += 4) {
-      const int j = b & (h - 1), a = (b - j) * 2 + j, c = a + h;
-      const int t = j * (TWN / len);
-      const double wr = c_twr[t], wi = inv ? -c_twi[t] : c_twi[t];
-      const double br = Zr[c * 32 + lane], bi = Zi[c * 32 + lane];
-      const double vr = br * wr - bi * wi, vi = br * wi + bi * wr;
-      const double ar = Zr[a * 32 + lane], ai = Zi[a * 32 + lane];
-      Zr[c * 32 + lane] = ar - vr;
-      Zi[c * 32 + lane] = ai - vi;
-      Zr[a * 32 + lane] = ar + vr;
-      Zi[a * 32 + lane] = ai + vi;
+  for (int m2 = w; m2 < M2; m2 += 4) {
+    double re[M1], im[M1];
+#pragma unroll
+    for (int m1 = 0; m1 < M1; m1++) {
+      re[bitrev(m1, L1)] = Zr[(M2 * m1 + m2) * 32 + lane];
+      im[bitrev(m1, L1)] = Zi[(M2 * m1 + m2) * 32 + lane];
     }
-    __syncthreads();
+    cfft_reg<M1, INV>(re, im);
+#pragma unroll
+    for (int k1 = 0; k1 < M1; k1++) {
+      double wr, wi;
+      twiddle<M>(m2 * k1, INV, wr, wi);
+      const double xr = re[k1] * wr - im[k1] * wi, xi = re[k1] * wi + im[k1] * wr;
+      Zr[(M2 * k1 + m2) * 32 + lane] = xr;
+      Zi[(M2 * k1 + m2) * 32 + lane] = xi;
+    }
   }
+  __syncthreads();
+  for (int k1 = w; k1 < M1; k1 += 4) {
+    double re[M2], im[M2];
+#pragma unroll
+    for (int m2 = 0; m2 < M2; m2++) {
+      re[bitrev(m2, L2)] = Zr[(M2 * k1 + m2) * 32 + lane];
+      im[bitrev(m2, L2)] = Zi[(M2 * k1 + m2) * 32 + lane];
+    }
+    cfft_reg<M2, INV>(re, im);
+#pragma unroll
+    for (int k2 = 0; k2 < M2; k2++) {
+      Zr[(M2 * k1 + k2) * 32 + lane] = re[k2];
+      Zi[(M2 * k1 + k2) * 32 + lane] = im[k2];
+    }
+  }
+  __syncthreads();
 }
 
 template <int N>
 __global__ void __launch_bounds__(128) k_z_fwd_s(double *__restrict__ data, int npts, long long stride,
                                                   double scale) {
-  constexpr int M = N / 2, LB = ilog2c(M);
+  constexpr int M = N / 2;
+  using F = FourStep<M>;
   extern __shared__ __align__(16) double zs[];
   double *Zr = zs, *Zi = zs + M * 32;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * 32 + lane;
   const bool ok = p < npts;
   for (int m = w; m < M; m += 4) {
-    const int r = (int)(__brev((unsigned)m) >> (32 - LB));
-    Zr[r * 32 + lane] = ok ? data[(2 * m) * stride + p] : 0.0;
-    Zi[r * 32 + lane] = ok ? data[(2 * m + 1) * stride + p] : 0.0;
+    Zr[m * 32 + lane] = ok ? data[(2 * m) * stride + p] : 0.0;
+    Zi[m * 32 + lane] = ok ? data[(2 * m + 1) * stride + p] : 0.0;
   }
   __syncthreads();
-  smem_stages<N>(Zr, Zi, false);
+  four_step<M, false>(Zr, Zi);
   if (!ok) return;  // no barrier follows
   for (int k = w; k <= M / 2; k += 4) {
     if (k == 0) {
-      data[p] = (Zr[lane] + Zi[lane]) * scale;
-      data[stride + p] = (Zr[lane] - Zi[lane]) * scale;
+      const int r0 = F::row(0);
+      data[p] = (Zr[r0 * 32 + lane] + Zi[r0 * 32 + lane]) * scale;
+      data[stride + p] = (Zr[r0 * 32 + lane] - Zi[r0 * 32 + lane]) * scale;
       continue;
     }
     // X_k from Z_k and conj Z_{M-k}; and X_{M-k} from the same pair
-    const int kk = M - k;
-    const double zr = Zr[k * 32 + lane], zi = Zi[k * 32 + lane];
-    const double qr = Zr[kk * 32 + lane], qi = Zi[kk * 32 + lane];
+    const int kk = M - k, rk = F::row(k), rkk = F::row(kk);
+    const double zr = Zr[rk * 32 + lane], zi = Zi[rk * 32 + lane];
+    const double qr = Zr[rkk * 32 + lane], qi = Zi[rkk * 32 + lane];
     for (int side = 0; side < (k == kk ? 1 : 2); side++) {
       const int q = side ? kk : k;
       const double ar = side ? qr : zr, ai = side ? qi : zi;   // Z_q
@@ -300,13 +341,13 @@ __global__ void __launch_bounds__(128) k_z_fwd_s(double *__restrict__ data, int 
 
 template <int N>
 __global__ void __launch_bounds__(128) k_z_inv_s(double *__restrict__ data, int npts, long long stride) {
-  constexpr int M = N / 2, LB = ilog2c(M);
+  constexpr int M = N / 2;
+  using F = FourStep<M>;
   extern __shared__ __align__(16) double zs[];
   double *Zr = zs, *Zi = zs + M * 32;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = blockIdx.x * 32 + lane;
   const bool ok = p < npts;
-  auto rev = [](int v) { return (int)(__brev((unsigned)v) >> (32 - LB)); };
   for (int k = w; k <= M / 2; k += 4) {
     if (k == 0) {
       const double x0 = ok ? data[p] : 0.0, xm = ok ? data[stride + p] : 0.0;
@@ -326,16 +367,17 @@ __global__ void __launch_bounds__(128) k_z_inv_s(double *__restrict__ data, int 
       const int t = q * (TWN / N);
       const double wr = c_twr[t], wi = -c_twi[t];
       const double orr = dr * wr - di * wi, oi = dr * wi + di * wr;
-      Zr[rev(q) * 32 + lane] = er - oi;
-      Zi[rev(q) * 32 + lane] = ei + orr;
+      Zr[q * 32 + lane] = er - oi;
+      Zi[q * 32 + lane] = ei + orr;
     }
   }
   __syncthreads();
-  smem_stages<N>(Zr, Zi, true);
+  four_step<M, true>(Zr, Zi);
   if (!ok) return;
   for (int m = w; m < M; m += 4) {
-    data[(2 * m) * stride + p] = 2.0 * Zr[m * 32 + lane];
-    data[(2 * m + 1) * stride + p] = 2.0 * Zi[m * 32 + lane];
+    const int r = F::row(m);
+    data[(2 * m) * stride + p] = 2.0 * Zr[r * 32 + lane];
+    data[(2 * m + 1) * stride + p] = 2.0 * Zi[r * 32 + lane];
   }
 }
 
