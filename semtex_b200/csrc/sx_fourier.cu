@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(128) k_z_inv(double *__restrict__ data, int np
   }
 }
 
-// Lengths 128, 256, 512: a block of four warps takes 32 points (lane =
+// Lengths 128, 256, 512: a block of eight warps takes 32 points (lane =
 // point); the half-length complex sequence z (length M = N/2) of each point
 // lies in shared memory, Zr/Zi[m][32], in natural order.  The complex FFT
 // of length M = M1 M2 runs in four steps with m = M2 m1 + m2 and
@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(128) k_z_inv(double *__restrict__ data, int np
 // M2 (k mod M1) + k / M1.  The real-to-complex steps around it are the
 // register kernels'; loads and stores of a plane are 32 consecutive doubles.
 constexpr size_t zsmem(int nz) { return (size_t)nz * 32 * sizeof(double); }
+constexpr int ZW = 8;  // warps a block: every sub-FFT of a pass at once
 
 template <int M>
 struct FourStep {
@@ -261,8 +262,8 @@ template <int M, bool INV>
 __device__ __forceinline__ void four_step(double *Zr, double *Zi) {
   using F = FourStep<M>;
   constexpr int M1 = F::M1, M2 = F::M2, L1 = ilog2c(M1), L2 = ilog2c(M2);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int m2 = w; m2 < M2; m2 += 4) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;  // ZW warps
+  for (int m2 = w; m2 < M2; m2 += ZW) {
     double re[M1], im[M1];
 #pragma unroll
     for (int m1 = 0; m1 < M1; m1++) {
@@ -280,7 +281,7 @@ __device__ __forceinline__ void four_step(double *Zr, double *Zi) {
     }
   }
   __syncthreads();
-  for (int k1 = w; k1 < M1; k1 += 4) {
+  for (int k1 = w; k1 < M1; k1 += ZW) {
     double re[M2], im[M2];
 #pragma unroll
     for (int m2 = 0; m2 < M2; m2++) {
@@ -298,23 +299,25 @@ __device__ __forceinline__ void four_step(double *Zr, double *Zi) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) k_z_fwd_s(double *__restrict__ data, int npts, long long stride,
+__global__ void __launch_bounds__(ZW * 32, 3) k_z_fwd_s(double *__restrict__ data, int npts, long long stride,
                                                   double scale) {
   constexpr int M = N / 2;
   using F = FourStep<M>;
   extern __shared__ __align__(16) double zs[];
   double *Zr = zs, *Zi = zs + M * 32;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;  // ZW warps
   const int p = blockIdx.x * 32 + lane;
   const bool ok = p < npts;
-  for (int m = w; m < M; m += 4) {
+#pragma unroll 4
+  for (int m = w; m < M; m += ZW) {
     Zr[m * 32 + lane] = ok ? data[(2 * m) * stride + p] : 0.0;
     Zi[m * 32 + lane] = ok ? data[(2 * m + 1) * stride + p] : 0.0;
   }
   __syncthreads();
   four_step<M, false>(Zr, Zi);
   if (!ok) return;  // no barrier follows
-  for (int k = w; k <= M / 2; k += 4) {
+#pragma unroll 2
+  for (int k = w; k <= M / 2; k += ZW) {
     if (k == 0) {
       const int r0 = F::row(0);
       data[p] = (Zr[r0 * 32 + lane] + Zi[r0 * 32 + lane]) * scale;
@@ -340,15 +343,16 @@ __global__ void __launch_bounds__(128) k_z_fwd_s(double *__restrict__ data, int 
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) k_z_inv_s(double *__restrict__ data, int npts, long long stride) {
+__global__ void __launch_bounds__(ZW * 32, 3) k_z_inv_s(double *__restrict__ data, int npts, long long stride) {
   constexpr int M = N / 2;
   using F = FourStep<M>;
   extern __shared__ __align__(16) double zs[];
   double *Zr = zs, *Zi = zs + M * 32;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;  // ZW warps
   const int p = blockIdx.x * 32 + lane;
   const bool ok = p < npts;
-  for (int k = w; k <= M / 2; k += 4) {
+#pragma unroll 2
+  for (int k = w; k <= M / 2; k += ZW) {
     if (k == 0) {
       const double x0 = ok ? data[p] : 0.0, xm = ok ? data[stride + p] : 0.0;
       Zr[0 * 32 + lane] = 0.5 * (x0 + xm);
@@ -374,7 +378,8 @@ __global__ void __launch_bounds__(128) k_z_inv_s(double *__restrict__ data, int 
   __syncthreads();
   four_step<M, true>(Zr, Zi);
   if (!ok) return;
-  for (int m = w; m < M; m += 4) {
+#pragma unroll 4
+  for (int m = w; m < M; m += ZW) {
     const int r = F::row(m);
     data[(2 * m) * stride + p] = 2.0 * Zr[r * 32 + lane];
     data[(2 * m + 1) * stride + p] = 2.0 * Zi[r * 32 + lane];
@@ -393,9 +398,9 @@ static int launch_smem(double *d, int npts, long long stride, int sign, cudaStre
   SX_CUDA(attr);
   const int grid = (npts + 31) / 32;
   if (sign == 1)
-    k_z_fwd_s<N><<<grid, 128, zsmem(N), st>>>(d, npts, stride, 1.0 / N);
+    k_z_fwd_s<N><<<grid, ZW * 32, zsmem(N), st>>>(d, npts, stride, 1.0 / N);
   else
-    k_z_inv_s<N><<<grid, 128, zsmem(N), st>>>(d, npts, stride);
+    k_z_inv_s<N><<<grid, ZW * 32, zsmem(N), st>>>(d, npts, stride);
   return SX_OK;
 }
 
