@@ -1131,6 +1131,8 @@ def run_profile(args):
     transform: the z-direction transform of the config-2 field (nz = 64,
            82,944 points, 42 MB), forward and inverse, `steps` times each,
            a 256 MB write between calls
+    transform256: the transform at config 5's length (nz = 256) on 99,840
+           points (205 MB), forward and inverse, `steps` times each
     dns:   the DNS elliptic-phase operations on config 5's plane shape with
            nz = 32 (254 MB a field), `steps` + 1 launches of each
     """
@@ -1149,6 +1151,19 @@ def run_profile(args):
                 sx.transform_z(d.data_ptr(), w.nz, w.mesh.nplane, w.mesh.nplane, sign, sptr)
         torch.cuda.synchronize()
         print(json.dumps({"profile": "transform", "nz": w.nz, "points": w.mesh.nplane}), flush=True)
+        return
+    if args.profile == "transform256":
+        # config 5's transform length on 99,840 points (205 MB, above L2)
+        x = torch.randn((256, 99840), dtype=torch.float64, device="cuda",
+                        generator=torch.Generator(device="cuda").manual_seed(5))
+        l2 = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+        sptr = torch.cuda.current_stream().cuda_stream
+        for _ in range(max(1, args.steps)):
+            for sign in (+1, -1):
+                l2.zero_()
+                sx.transform_z(x.data_ptr(), 256, 99840, 99840, sign, sptr)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "transform256", "nz": 256, "points": 99840}), flush=True)
         return
     if args.profile == "dns":
         print(json.dumps({"profile": "dns", "run": run_dns(reps=max(1, args.steps), nz=32, check=False)}),
@@ -1220,7 +1235,8 @@ def main():
                          "its JSON (not a bench line)")
     ap.add_argument("--tol", type=float, default=1e-12,
                     help="FP64 relative residual at which the mixed form stops")
-    ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform", "dns"], default=None,
+    ap.add_argument("--profile", choices=["band", "band3", "solve3", "mixed", "transform", "transform256", "dns"],
+                    default=None,
                     help="bounded run of one kernel family for ncu (no bench line)")
     ap.add_argument("--band-cluster", type=int, default=0, help="--profile band*: CTAs per cluster (0: default)")
     ap.add_argument("--band-stages", type=int, default=0, help="--profile band*: ring depth (0: default)")
