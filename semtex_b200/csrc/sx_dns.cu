@@ -31,20 +31,22 @@ namespace {
 // ---------------------------------------------------------------------------
 //
 // A CTA holds a tile of TE consecutive elements of one plane in shared
-// memory and walks a group of planes, copying the next plane's tile in
-// (cp.async) while it works on this one.  Each derivative the operation
-// forms (a "job": d/dx of u, d/dy of v, ...) has two groups of 64 threads.
-// A "row" thread (t, r) forms row r of element t's r-derivative,
+// memory and walks a group of planes, copying the next planes' tiles in
+// (a cp.async ring) while it works on this one.  It has a group of 64 "row"
+// threads and a group of 64 "column" threads.  Row thread (t, r) forms row r
+// of element t's r-derivative,
 //     dr[r][j] = sum_k u[r][k] D[j][k]        (u D^T, src/element.cpp:569)
-// times that row of dr/dx (or dr/dy) into A; a "column" thread (t, c) forms
+// times that row of dr/dx (or dr/dy) into A; column thread (t, c) forms
 // column c of the s-derivative,
 //     ds[i][c] = sum_k D[i][k] u[k][c]        (D u, src/element.cpp:570)
-// times ds/dx (or ds/dy) into C.  The epilogue adds C + A -- the rounding
-// sequence of vmul + vvtvp (src/element.cpp:571-572) -- and applies the
-// operation's own arithmetic on the way out.  D is a kernel parameter: every
-// thread of a warp reads the same entry at the same time, so it is a
-// constant-bank operand of the FMA; each thread keeps its row (column) of
-// its job's partial in registers for the whole plane group.
+// times ds/dx (or ds/dy) into C.  Where an operation forms two derivatives
+// (a "job" each: pressure forcing's d/dx u and d/dy v, project's d/dx P and
+// d/dy P), a thread forms both for its line.  The epilogue adds C + A --
+// the rounding sequence of vmul + vvtvp (src/element.cpp:571-572) -- and
+// applies the operation's own arithmetic on the way out.  D is a kernel
+// parameter: every thread of a warp reads the same entry at the same time,
+// so it is a constant-bank operand of the FMA; each thread keeps its row
+// (column) of each job's partial in registers for the whole plane group.
 
 constexpr int EL_GROUP = 64;
 
