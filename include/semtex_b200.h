@@ -133,6 +133,15 @@ SX_API int sx_mesh_geometry(sx_mesh mesh, int e, double *q1, double *q2, double 
  * mass (nglobal doubles, src/bcmgr.cpp:805-821).  Any pointer may be NULL. */
 SX_API int sx_mesh_partials(sx_mesh mesh, int e, double *drdx, double *drdy, double *dsdx, double *dsdy,
                             double *imass);
+/* The band factor's envelope in tiles of 64 x 64: *nblk block columns of
+ * nsolve; when env is not NULL it receives 2 * nblk ints, env[k] the tiles
+ * above the diagonal of block column k that can be non-zero and
+ * env[nblk + k] those right of the diagonal in block row k.  Every other tile
+ * of the band (nband wide, as LAPACK's dpbtrf stores it, src/matrix.cpp:
+ * 236-262) is an exact zero of the factor; the factorisation and the sweeps
+ * skip them.  No counterpart in the reference, which stores and sweeps the
+ * whole band. */
+SX_API int sx_mesh_envelope(sx_mesh mesh, int *nblk, int *env);
 
 /* ---- modal system: replaces ModalMatrixSys::ModalMatrixSys ---------------
  * src/matrix.cpp:33-110, MatrixSys::MatrixSys src/matrix.cpp:139-317.

@@ -147,6 +147,7 @@ def _load():
     L.sx_modal_autotune.argtypes = [vp, vp, vp, vp, ip, ip, ip, dp, ip, vp, P(TuneResult)]
     L.sx_transform_z.argtypes = [vp, ip, ip, ip, ip, vp]
     L.sx_mesh_partials.argtypes = [vp, ip] + [P(dp)] * 5
+    L.sx_mesh_envelope.argtypes = [vp, P(ip), P(ip)]
     L.sx_field_gradient.argtypes = [vp, vp, ip, ip, ip, dp, ip, vp]
     L.sx_dns_pressure_forcing.argtypes = [vp, P(vp), ip, vp, ip, ip, dp, dp, ip, vp]
     L.sx_dns_project.argtypes = [vp, P(vp), vp, P(vp), ip, ip, ip, ip, ip, dp, dp, dp, dp, ip, vp]
@@ -248,6 +249,17 @@ class Mesh:
         out = [np.zeros(self.qm.npnp) for _ in range(4)] + [np.zeros(self.qm.nglobal)]
         _check(lib.sx_mesh_partials(self.h, e, *[_dptr(a) for a in out]), "sx_mesh_partials")
         return out
+
+    def envelope(self):
+        """The band factor's envelope by 64 x 64 tiles: (above, right), the
+        tiles above the diagonal of each block column and right of it in
+        each block row that the factorisation and the sweeps visit."""
+        nb = C.c_int()
+        _check(lib.sx_mesh_envelope(self.h, C.byref(nb), None), "sx_mesh_envelope")
+        env = np.zeros(2 * max(nb.value, 1), dtype=np.int32)
+        _check(lib.sx_mesh_envelope(self.h, C.byref(nb), env.ctypes.data_as(C.POINTER(C.c_int))),
+               "sx_mesh_envelope")
+        return env[:nb.value].copy(), env[nb.value:2 * nb.value].copy()
 
     def geometry(self, e):
         out = [np.zeros(self.qm.npnp) for _ in range(5)]

@@ -347,6 +347,8 @@ static Job make_job(sx_modal_s &M, const Group &g, int slot, double *u, double *
   j.dinv = S.dinv.p;
   j.nblk = S.nblk;
   j.J = S.J;
+  j.jf = S.mesh->denv.p;
+  j.jb = S.mesh->denv.p + S.mesh->env_nblk;
   j.npad = std::max(S.nblk, 1) * NB;
   j.rhs_stride = (long long)M.npad_max;
   j.rhs = M.rhs.p + (size_t)slot * M.npad_max;

@@ -69,40 +69,56 @@ struct SweepGeom {
   // the j = 1 tile and before D_k.
   int Q;
   FastDiv dC1, dQ, dQ1;  // divisions by C - 1, Q and Q - 1 (1 when unused)
-  // tiles owned by `rank` at sequence step t (t < nblk: forward block t,
-  // else backward block 2 nblk - 1 - t); D_k is always last, on rank 0.
+  // Envelope of the factor (null: the whole band): jf[k] tiles above the
+  // diagonal are non-zero in block column k, jb[k] right of it in block row
+  // k; every tile beyond them is an exact zero and is skipped.
+  const int *jf, *jb;
+  // off-diagonal tiles of step t (t < nblk: forward block t, else backward
+  // block 2 nblk - 1 - t)
   __device__ __forceinline__ int jmax(int t) const {
     if (t >= 2 * nblk) return 0;
-    return t < nblk ? min(J, t) : min(J, nblk - 1 - (2 * nblk - 1 - t));
+    if (t < nblk) {
+      const int b = min(J, t);
+      return jf ? max(0, min(b, __ldg(jf + t))) : b;
+    }
+    const int k = 2 * nblk - 1 - t, b = min(J, nblk - 1 - k);
+    return jb ? max(0, min(b, __ldg(jb + k))) : b;
   }
+  // what a step's tile list depends on: its own tile count and the next
+  // step's (the leader's share of it); read once per step
+  struct Step {
+    int jm, jm1;
+  };
+  __device__ __forceinline__ Step step(int t) const { return Step{jmax(t), jmax(t + 1)}; }
   // the leader's tiles of step t + 1, listed at step t
-  __device__ __forceinline__ int ahead_count(int t) const { return dQ.div(max(jmax(t + 1) - 1, 0)); }
+  __device__ __forceinline__ int ahead_count(const Step &s) const { return dQ.div(max(s.jm1 - 1, 0)); }
   // tiles j >= 2 of step t that are not the leader's
-  __device__ __forceinline__ int rank_positions(int t) const {
-    const int npos = max(jmax(t) - 1, 0);
+  __device__ __forceinline__ int rank_positions(const Step &s) const {
+    const int npos = max(s.jm - 1, 0);
     return Q == 0 ? npos : npos - dQ.div(npos);
   }
-  __device__ __forceinline__ int count(int t) const {
-    const int jm = jmax(t);
+  // tiles owned by `rank` at a step; D_k is always last, on rank 0
+  __device__ __forceinline__ int count(const Step &s) const {
+    const int jm = s.jm;
     if (C == 1) return jm + 1;
-    if (rank == 0) return (jm >= 1 ? 1 : 0) + (Q == 0 ? 0 : ahead_count(t)) + 1;
-    const int N = rank_positions(t);
+    if (rank == 0) return (jm >= 1 ? 1 : 0) + (Q == 0 ? 0 : ahead_count(s)) + 1;
+    const int N = rank_positions(s);
     return N > rank - 1 ? dC1.div(N - rank) + 1 : 0;
   }
   // j of the idx-th owned tile, in processing order: a rank's tiles j >= 2
   // from the oldest block down; the leader's j = 1 tile, its tiles of step
   // t + 1 from the oldest block down, then D_k (j = 0)
-  __device__ __forceinline__ int jat(int t, int idx) const {
-    const int jm = jmax(t);
+  __device__ __forceinline__ int jat(const Step &s, int idx) const {
+    const int jm = s.jm;
     if (C == 1) return idx < jm ? jm - idx : 0;
     if (rank == 0) {
       const int a = jm >= 1 ? 1 : 0;
       if (idx < a) return 1;
       if (Q == 0) return 0;
-      const int F1 = ahead_count(t), e = idx - a;
+      const int F1 = ahead_count(s), e = idx - a;
       return e < F1 ? (F1 - 1 - e) * Q + (Q - 1) + 2 : 0;
     }
-    const int N = rank_positions(t);
+    const int N = rank_positions(s);
     const int n = N > rank - 1 ? dC1.div(N - rank) + 1 : 0;
     const int i = (rank - 1) + (n - 1 - idx) * (C - 1);
     return (Q == 0 ? i : i + dQ1.div(i)) + 2;
@@ -142,8 +158,16 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   __shared__ int abort_flag;
 
   const int tid = threadIdx.x, c = tid & (NB - 1), q = tid >> 6;
-  const SweepGeom G{nblk, Jb.J, C, rank, Q, FastDiv((unsigned)max(C - 1, 1)), FastDiv((unsigned)max(Q, 1)),
-                    FastDiv((unsigned)max(Q - 1, 1))};
+  const SweepGeom G{nblk,
+                    Jb.J,
+                    C,
+                    rank,
+                    Q,
+                    FastDiv((unsigned)max(C - 1, 1)),
+                    FastDiv((unsigned)max(Q, 1)),
+                    FastDiv((unsigned)max(Q - 1, 1)),
+                    Jb.jf,
+                    Jb.jb};
   const FastDiv dW((unsigned)W);
   const long long lim = g_sweep_wait;
   if (tid == 0) {
@@ -160,6 +184,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   const int T = 2 * nblk;
   // producer state (thread 0): next tile (tp, ip); counters are uniform.
   int tp = 0, ip = 0, pslot = 0;
+  SweepGeom::Step ps = G.step(0);  // the producer's step tp
   long long nissued = 0, ncons = 0;
   int cslot = 0;
   uint32_t cphase = 0;  // slot and phase parity of tile ncons
@@ -172,12 +197,13 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   };
   auto produce = [&](long long limit) {
     while (nissued < limit) {
-      while (tp < T && ip >= G.count(tp)) {
+      while (tp < T && ip >= G.count(ps)) {
         tp++;
         ip = 0;
+        ps = SweepGeom::Step{ps.jm1, G.jmax(tp + 1)};
       }
       if (tp >= T) return;
-      const int j = G.jat(tp, ip);
+      const int j = G.jat(ps, ip);
       double *dst = ring + (size_t)pslot * TSZ;
       uint64_t *bar = &full[pslot];
       if (++pslot == S) pslot = 0;
@@ -242,7 +268,8 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
   for (int t = 0; t < T; t++) {
     const bool fwd = t < nblk;
     const int k = fwd ? t : 2 * nblk - 1 - t;
-    const int n = G.count(t);
+    const SweepGeom::Step cs = G.step(t);
+    const int n = G.count(cs);
     double s[PMAX];
 #pragma unroll
     for (int p = 0; p < PMAX; p++) {
@@ -252,7 +279,7 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
     bool bad = false;
     // the step's first tile's block; each later one is fetched under the
     // work of the tile before it (j = 1 uses the leader's own yk, D_k none)
-    int jn = n > 0 ? G.jat(t, 0) : 0;
+    int jn = n > 0 ? G.jat(cs, 0) : 0;
     if (jn >= 2 && !pre && !fetch_y(t, jn, (int)(ytile & 1))) bad = true;
     pre = false;
     for (int idx = 0; idx < n; idx++) {
@@ -266,13 +293,14 @@ __global__ void __launch_bounds__(256, PMAX <= 2 ? 2 : 1)
       if (abort_flag) break;
       const double *yv = yk;
       if (j >= 2) yv = ysl + (size_t)(ytile++ & 1) * PMAX * NB;
-      jn = idx + 1 < n ? G.jat(t, idx + 1) : 0;
+      jn = idx + 1 < n ? G.jat(cs, idx + 1) : 0;
       // ysl[ytile & 1] was last read two fetched tiles ago, before the
       // barrier that ended it; a failed wait is seen after this tile's barrier
       if (jn >= 2) {
         if (!fetch_y(t, jn, (int)(ytile & 1))) abort_flag = 1;
       } else if (t + 1 < T) {
-        const int n1 = G.count(t + 1), j1 = n1 > 0 ? G.jat(t + 1, 0) : 0;
+        const SweepGeom::Step ns = SweepGeom::Step{cs.jm1, G.jmax(t + 2)};
+        const int n1 = G.count(ns), j1 = n1 > 0 ? G.jat(ns, 0) : 0;
         const int src = (G.ahead(j1) ? t + 2 : t + 1) - j1;
         // the leader copies without a release; block t itself is solved
         // only at the end of this step

@@ -371,11 +371,12 @@ __device__ __forceinline__ void mma_store(double *T, const MmaAcc &acc) {
       for (int q = 0; q < 2; q++) T[(r0 + 8 * m + g) * LDT + c0 + 8 * n + 2 * t + q] = acc.v[m][n][q];
 }
 
-// Off-diagonal tiles of block row k: U(k, k+i) = U_kk^-T A(k, k+i).
+// Off-diagonal tiles of block row k: U(k, k+i) = U_kk^-T A(k, k+i), for the
+// tiles inside the envelope (i <= jb[k]); the others stay zero.
 __global__ void __launch_bounds__(256, 3) k_trsm(const SysDesc *__restrict__ sys, int k) {
   const SysDesc S = sys[blockIdx.y];
   const int i = blockIdx.x + 1;
-  if (k >= S.nblk || i > S.J || k + i >= S.nblk) return;
+  if (k >= S.nblk || i > S.J || k + i >= S.nblk || (S.jb && i > S.jb[k])) return;
   extern __shared__ __align__(16) double smt[];
   double *X = smt, *B = X + NB * LDM;
   double *T = S.tiles + ((size_t)(k + i) * (S.J + 1) + i) * TSZ;
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(256, 3) k_trsm(const SysDesc *__restrict__ sys
 }
 
 // Trailing update inside the band: A(k+i, k+j) -= U(k,k+i)^T U(k,k+j),
-// 1 <= i <= j <= J.  The product is formed in the accumulators from zero and
+// 1 <= i <= j <= jb[k] (every other product has a zero factor).  The product is formed in the accumulators from zero and
 // subtracted from the target tile once: accumulating into the target
 // instead moved an ill-conditioned mode's solution 170 times further from
 // LAPACK's (1.3e-12 -> 2.2e-10 relative, config 5's pressure mode 1).
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(256, 3) k_update(const SysDesc *__restrict__ s
   const SysDesc S = sys[blockIdx.y];
   const int2 pr = pairs[blockIdx.x];
   const int i = pr.x, j = pr.y;
-  if (k >= S.nblk || j > S.J || k + j >= S.nblk) return;
+  if (k >= S.nblk || j > S.J || k + j >= S.nblk || (S.jb && j > S.jb[k])) return;
   extern __shared__ __align__(16) double smt[];
   double *A = smt, *B = A + NB * LDM;
   const size_t J1 = S.J + 1;
@@ -497,9 +498,17 @@ int factor_batch(std::vector<System *> &systems, cudaStream_t st, bool sync) {
   int maxblk = 0, maxJ = 0;
   for (size_t s = 0; s < systems.size(); s++) {
     System &S = *systems[s];
-    hd[s] = SysDesc{S.tiles.p, S.dinv.p, S.nblk, S.J, S.status.p};
+    const sx_mesh_s &Mh = *S.mesh;
+    hd[s] = SysDesc{S.tiles.p, S.dinv.p, S.nblk, S.J, S.status.p, Mh.denv.p + Mh.env_nblk};
     maxblk = std::max(maxblk, S.nblk);
     maxJ = std::max(maxJ, S.J);
+  }
+  // tiles of block row k over the systems (the launches' extent)
+  std::vector<int> rowmax(std::max(maxblk, 1), 0);
+  for (System *Sp : systems) {
+    const sx_mesh_s &Mh = *Sp->mesh;
+    for (int k = 0; k < Sp->nblk; k++)
+      rowmax[k] = std::max(rowmax[k], std::min(std::min(Sp->J, Mh.env[Mh.env_nblk + k]), Sp->nblk - 1 - k));
   }
   DBuf<SysDesc> dd;
   SX_TRY(dd.upload_on(hd.data(), hd.size(), st));
@@ -515,9 +524,11 @@ int factor_batch(std::vector<System *> &systems, cudaStream_t st, bool sync) {
   const int ns = (int)systems.size();
   for (int k = 0; k < maxblk; k++) {
     k_potrf<<<ns, 256, sm2, st>>>(dd.p, k);
-    if (maxJ > 0) {
-      k_trsm<<<dim3(maxJ, ns), 256, smm, st>>>(dd.p, k);
-      k_update<<<dim3((unsigned)pairs.size(), ns), 256, smm, st>>>(dd.p, k, dpairs.p);
+    const int m = rowmax[k];
+    if (m > 0) {
+      // pairs are listed by j, so those with j <= m come first
+      k_trsm<<<dim3(m, ns), 256, smm, st>>>(dd.p, k);
+      k_update<<<dim3((unsigned)(m * (m + 1) / 2), ns), 256, smm, st>>>(dd.p, k, dpairs.p);
     }
   }
   SX_CUDA(cudaGetLastError());

@@ -205,6 +205,13 @@ struct sx_mesh_s {
   // mass diagonal: the Jacobi-scaled operator's condition number is about
   // 1 + kratio / hCon
   double kratio = 0.0;
+  // Envelope of the band factor in tiles of NB: for the env_nblk block
+  // columns of nsolve, env[k] = off-diagonal tiles of block column k that
+  // can be non-zero (above the diagonal), env[env_nblk + k] = those of block
+  // row k (right of it).  Every other tile of the band is an exact zero.
+  int env_nblk = 0;
+  std::vector<int> env;
+  sx::DBuf<int> denv;
   sx::DBuf<unsigned long long> downer;
   sx::MeshView view() const;
 };

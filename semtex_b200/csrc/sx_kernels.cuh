@@ -11,6 +11,7 @@ struct SysDesc {
   double *dinv;   // nblk*TSZ
   int nblk, J;
   int *status;
+  const int *jb;  // tiles right of the diagonal in each block row (null: J)
 };
 
 // Address of U(m, n), m <= n, n - m <= kd, inside the tile array.

@@ -286,6 +286,45 @@ int mesh_kratio(const sx_mesh_desc *d, double *out) {
 
 }  // namespace sx
 
+// Envelope of the condensed matrix and of its Cholesky factor, by tiles.
+// Node c (< nsolve) is coupled to every solve node of the elements that hold
+// it, so row c of the matrix starts at first(c) = the lowest solve node of
+// those elements.  Cholesky fill stays inside this envelope (George & Liu,
+// Computer Solution of Large Sparse Positive Definite Systems, 1981, ch. 4):
+// U(r, c) = 0 exactly for r < first(c), in floating point too, because every
+// product that forms such an entry has a zero factor.  By block columns of NB,
+// column block k can be non-zero only from row block fb(k) = min first(c) / NB
+// over its columns.  The tables use the suffix minimum fm(k) = min over k' >= k
+// of fb(k'), a monotone hull of that staircase, so that the non-zero tiles of
+// every block row are contiguous too: block column k holds jf(k) = k - fm(k)
+// tiles above its diagonal, block row k the jb(k) = max{ j : fm(k + j) <= k }
+// right of it.  The pressure pin (nsolve - 1) only removes a row and column,
+// so the tables of nsolve hold for it as well.
+static int band_envelope(sx_mesh_s &M) {
+  const int ns = M.nsolve, nblk = (ns + NB - 1) / NB, J = (M.nband - 1 + NB - 1) / NB;
+  std::vector<int> fm(nblk);
+  for (int k = 0; k < nblk; k++) fm[k] = k;
+  for (int e = 0; e < M.nel; e++) {
+    const int *g = &M.btog[(size_t)e * M.next];
+    int lo = ns;
+    for (int i = 0; i < M.next; i++)
+      if (g[i] < ns) lo = std::min(lo, g[i]);
+    for (int i = 0; i < M.next; i++)
+      if (g[i] < ns) fm[g[i] / NB] = std::min(fm[g[i] / NB], lo / NB);
+  }
+  for (int k = nblk - 2; k >= 0; k--) fm[k] = std::min(fm[k], fm[k + 1]);
+  M.env_nblk = nblk;
+  M.env.assign((size_t)2 * std::max(nblk, 1), 0);
+  int c = 0;  // the last block column whose hull reaches row block k
+  for (int k = 0; k < nblk; k++) {
+    M.env[k] = std::min(J, k - fm[k]);
+    c = std::max(c, k);
+    while (c + 1 < nblk && fm[c + 1] <= k) c++;
+    M.env[nblk + k] = std::min(J, c - k);
+  }
+  return SX_OK;
+}
+
 extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   if (!d || !out) return SX_ERR_ARG;
   *out = nullptr;
@@ -338,6 +377,7 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       return SX_ERR_BAND;
     }
   }
+  SX_TRY(band_envelope(*M));
   M->emask.assign(nel, 0);
   for (int e = 0; e < nel; e++)
     for (int i = 0; i < next; i++) M->emask[e] |= M->bmask[(size_t)e * next + i] != 0;
@@ -468,6 +508,7 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
   SX_TRY(M->dDf.upload(df.data(), df.size()));
   SX_TRY(M->dhasQ3.upload(M->hasQ3.data(), nel));
   SX_TRY(M->dbtog.upload(M->btog.data(), tb));
+  SX_TRY(M->denv.upload(M->env.data(), M->env.size()));
   SX_TRY(M->dbmask.upload(M->bmask.data(), tb));
   SX_TRY(M->demask.upload(M->emask.data(), nel));
   SX_TRY(M->dg2e_ptr.upload(ptr.data(), ptr.size()));
@@ -531,6 +572,13 @@ extern "C" int sx_mesh_geometry(sx_mesh m, int e, double *q1, double *q2, double
   if (q3) std::memcpy(q3, &m->Q3[o], n * 8);
   if (q4) std::memcpy(q4, &m->Q4[o], n * 8);
   if (q8) std::memcpy(q8, &m->Q8[o], n * 8);
+  return SX_OK;
+}
+
+extern "C" int sx_mesh_envelope(sx_mesh m, int *nblk, int *env) {
+  if (!m || !nblk) return SX_ERR_ARG;
+  *nblk = m->env_nblk;
+  if (env) std::memcpy(env, m->env.data(), sizeof(int) * 2 * (size_t)m->env_nblk);
   return SX_OK;
 }
 

@@ -20,6 +20,7 @@ struct Job {
   const double *hbi, *hii;
   const double *tiles, *dinv;
   int nblk, J, npad;
+  const int *jf, *jb;   // factor envelope by block column / row (null: whole band)
   double *rhs;          // P * rhs_stride
   long long rhs_stride;
   double *Fb;           // P * nel * next

@@ -145,6 +145,8 @@ extern "C" int sx_field_solve_device_static(sx_modal s, double *d_u, double *d_f
     j.dinv = S.dinv.p;
     j.nblk = S.nblk;
     j.J = S.J;
+    j.jf = S.mesh->denv.p;
+    j.jb = S.mesh->denv.p + S.mesh->env_nblk;
     j.npad = std::max(S.nblk, 1) * NB;
     j.rhs_stride = j.npad;
     size_t off = align256(sizeof(Job));
