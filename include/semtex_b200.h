@@ -247,13 +247,22 @@ SX_API int sx_field_solve_batched_host(sx_modal modal, double *u, const double *
  *                         while it waits for the other CTAs' partial sums);
  *                         1 = none (it keeps only the tile next to the
  *                         diagonal and the diagonal block's inverse);
- *                         <= 0 = the default                               */
+ *                         <= 0 = the default
+ *   SX_TUNE_HOST_CHUNK    Fourier modes per chunk of the host-buffer
+ *                         pipeline of sx_field_solve_batched_host (each
+ *                         chunk is copied up, solved and copied back on
+ *                         its own streams, overlapping the others); auto:
+ *                         eight chunks of at least 8 modes when every mode
+ *                         goes to the band Cholesky and there are 32 or
+ *                         more, else half the modes rounded up to a
+ *                         multiple of 16                                   */
 enum {
   SX_TUNE_INNER_ITERS = 1,
   SX_TUNE_BAND_CLUSTER = 2,
   SX_TUNE_MIXED_ROUTE = 3,
   SX_TUNE_BAND_STAGES = 4,
-  SX_TUNE_BAND_LEAD = 5
+  SX_TUNE_BAND_LEAD = 5,
+  SX_TUNE_HOST_CHUNK = 6
 };
 SX_API int sx_modal_tune(sx_modal modal, int knob, int value);
 

@@ -33,6 +33,7 @@ DIRECT, JACPCG, MIXED_SOLVER, AUTO = 0, 1, 2, 3
 FP64, MIXED_FP32 = 0, 1
 OK, WARN_STEP_LIMIT = 0, 8
 TUNE_INNER_ITERS, TUNE_BAND_CLUSTER, TUNE_MIXED_ROUTE, TUNE_BAND_STAGES, TUNE_BAND_LEAD = 1, 2, 3, 4, 5
+TUNE_HOST_CHUNK = 6
 ROUTE_AUTO, ROUTE_CG, ROUTE_BAND = 0, 1, 2
 STATIC_SCRATCH_BYTES = 4 << 20  # SX_STATIC_SCRATCH_BYTES
 
@@ -373,12 +374,16 @@ class ModalMatrixSys:
         self.last_stats = st.as_dict()
         return u
 
-    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None, band_stages=None, band_lead=None):
+    def tune(self, inner_iters=None, band_cluster=None, mixed_route=None, band_stages=None, band_lead=None,
+             host_chunk=None):
         """Schedule knobs of the batched forms (None leaves a knob alone, 0
         restores its default).  mixed_route: ROUTE_AUTO (by cost), ROUTE_CG
         (FP32 CG for every mode), ROUTE_BAND (band Cholesky for every
         factored mode).  band_lead: K >= 2, the cluster leader taking the last
-        of every K band tiles off the critical path (1: none)."""
+        of every K band tiles off the critical path (1: none).  host_chunk:
+        modes per chunk of solve_batched_host's copy/solve pipeline."""
+        if host_chunk is not None:
+            _check(lib.sx_modal_tune(self.h, TUNE_HOST_CHUNK, int(host_chunk)), "sx_modal_tune")
         if band_lead is not None:
             _check(lib.sx_modal_tune(self.h, TUNE_BAND_LEAD, int(band_lead)), "sx_modal_tune")
         if inner_iters is not None:

@@ -263,6 +263,10 @@ extern "C" int sx_modal_tune(sx_modal s, int knob, int value) {
       s->fp64.reset();
       s->hyb.reset();
       return SX_OK;
+    case SX_TUNE_HOST_CHUNK:
+      if (value > 1 << 20) return SX_ERR_ARG;
+      s->host_chunk = value > 0 ? value : 0;
+      return SX_OK;
     case SX_TUNE_BAND_LEAD:
       if (value > 64) return SX_ERR_ARG;
       s->forced_lead = value <= 0 ? -1 : (value == 1 ? 0 : value);
@@ -783,16 +787,18 @@ sx_modal_s::HostPipe::~HostPipe() {
   if (d2h) cudaStreamDestroy(d2h);
 }
 
-// Modes per chunk of the pipelined host entry: half the modes, rounded up to
-// a multiple of 16 (32 planes, one full lane chunk of the mixed form's
-// kernels), at least 16.  Two chunks let the second chunk's copy in and the
-// first chunk's copy out overlap the solves; more, smaller chunks would
-// shorten the overlap's ends but run each chunk's band sweeps with fewer
-// systems per launch, where every system's block-column chain, not HBM,
-// sets the time (config 3: four 16-mode chunks 81.6 ms end to end against a
-// 41.9 ms solve).
+// Modes per chunk of the pipelined host entry.  When every mode is solved
+// by the band Cholesky and there are 32 modes or more: eight chunks of at
+// least 8 modes.  The chunks are solved side by side on their own streams,
+// so their band sweeps share the GPU as one launch would, and small chunks
+// shorten the ends of the pipeline: the last chunk's copy in and the copy
+// out after it (config 3's 64 modes end to end: 38.0 ms with 8-mode chunks,
+// 39.9 with 16, 43.2 with 32, 48.8 unpipelined, for a 31 ms solve).
+// Otherwise half the modes, rounded up to a multiple of 16 (32 planes, one
+// full lane chunk of the mixed form's FP32 kernels), at least 16.
 constexpr int HOST_CHUNK_MIN = 16;
-static int host_chunk_modes(int nmodes) {
+static int host_chunk_modes(int nmodes, bool all_band) {
+  if (all_band && nmodes >= 32) return std::max(8, ((nmodes + 7) / 8 + 7) / 8 * 8);
   const int half = (nmodes + 1) / 2;
   return std::max(HOST_CHUNK_MIN, (half + HOST_CHUNK_MIN - 1) / HOST_CHUNK_MIN * HOST_CHUNK_MIN);
 }
@@ -811,7 +817,13 @@ extern "C" int sx_field_solve_batched_host(sx_modal s, double *u, const double *
   if (!s->own) SX_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamDefault));
   cudaStream_t st = s->own;
   const int nmodes = nz == 1 ? 1 : nz / 2;
-  const int chunk = host_chunk_modes(nmodes);
+  bool all_band = true;
+  for (int l = 0; l < std::min(nmodes, s->num_modes) && all_band; l++) {
+    const System &S = *s->sys[l];
+    all_band = S.method == SX_DIRECT && S.tiles.p &&
+               (precision == SX_FP64 || route_direct(*s, S, tol_rel, max_refine));
+  }
+  const int chunk = s->host_chunk > 0 ? s->host_chunk : host_chunk_modes(nmodes, all_band);
   const int nchunks = (nmodes + chunk - 1) / chunk;
   if (nchunks < 2 || nz % 2 || nmodes > s->num_modes) {
     SX_CUDA(cudaMemcpyAsync(s->hf.p, f, n * 8, cudaMemcpyHostToDevice, st));

@@ -131,6 +131,14 @@ struct DBuf {
     os = free_on_s ? s : nullptr;
     return SX_OK;
   }
+  // From `pool` (alloc_in), copied on stream s and complete on return (the
+  // wait is for s alone, not the device)
+  int upload_in(const T *h, size_t count, cudaMemPool_t pool, cudaStream_t s) {
+    SX_TRY(alloc_in(count, pool, s));
+    SX_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    SX_CUDA(cudaStreamSynchronize(s));
+    return SX_OK;
+  }
   int upload(const T *h, size_t count) {
     SX_TRY(alloc(count));
     SX_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));

@@ -9,6 +9,8 @@
 #include <cstdarg>
 #include <cstring>
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <numeric>
 
 #include "sx_internal.h"
@@ -286,6 +288,49 @@ int mesh_kratio(const sx_mesh_desc *d, double *out) {
 
 }  // namespace sx
 
+// Device memory of meshes comes from a stream-ordered pool of their own
+// (one per device), so that dropping a mesh frees its memory without the
+// device-wide synchronisation of cudaFree (a server drops one per request
+// while other requests run), and creating one waits for nothing but its own
+// copies.  Up to MESH_POOL_KEEP bytes of freed mesh memory stay mapped for
+// the next mesh.
+constexpr uint64_t MESH_POOL_KEEP = uint64_t(4) << 30;
+
+static int mesh_pool(int device, cudaMemPool_t *out) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = pools.find(device);
+  if (it == pools.end()) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    SX_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = MESH_POOL_KEEP;
+    SX_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    it = pools.emplace(device, pool).first;
+  }
+  *out = it->second;
+  return SX_OK;
+}
+
+// The pool and a private stream for one mesh's uploads.
+struct MeshUpload {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t s = nullptr;
+  int begin(int device) {
+    SX_TRY(mesh_pool(device, &pool));
+    SX_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return SX_OK;
+  }
+  ~MeshUpload() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
 // Envelope of the condensed matrix and of its Cholesky factor, by tiles.
 // Node c (< nsolve) is coupled to every solve node of the elements that hold
 // it, so row c of the matrix starts at first(c) = the lowest solve node of
@@ -481,39 +526,41 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
     f1[i] = (float)M->Q1[i]; f2[i] = (float)M->Q2[i];
     f3[i] = (float)M->Q3[i]; f4[i] = (float)M->Q4[i];
   }
-  SX_TRY(M->dD.upload(M->D.data(), nn));
-  SX_TRY(M->demap.upload(M->emap.data(), nn));
-  SX_TRY(M->dQ1.upload(M->Q1.data(), tot));
-  SX_TRY(M->dQ2.upload(M->Q2.data(), tot));
-  SX_TRY(M->dQ3.upload(M->Q3.data(), tot));
-  SX_TRY(M->dQ4.upload(M->Q4.data(), tot));
-  SX_TRY(M->dQ8.upload(M->Q8.data(), tot));
-  SX_TRY(M->ddrdx.upload(M->drdx.data(), tot));
-  SX_TRY(M->ddrdy.upload(M->drdy.data(), tot));
-  SX_TRY(M->ddsdx.upload(M->dsdx.data(), tot));
-  SX_TRY(M->ddsdy.upload(M->dsdy.data(), tot));
-  SX_TRY(M->dimass.upload(M->imass.data(), M->imass.size()));
-  SX_TRY(M->dQ1f.upload(f1.data(), tot));
-  SX_TRY(M->dQ2f.upload(f2.data(), tot));
-  SX_TRY(M->dQ3f.upload(f3.data(), tot));
-  SX_TRY(M->dQ4f.upload(f4.data(), tot));
+  MeshUpload up;
+  SX_TRY(up.begin(M->device));
+  SX_TRY(M->dD.upload_in(M->D.data(), nn, up.pool, up.s));
+  SX_TRY(M->demap.upload_in(M->emap.data(), nn, up.pool, up.s));
+  SX_TRY(M->dQ1.upload_in(M->Q1.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ2.upload_in(M->Q2.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ3.upload_in(M->Q3.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ4.upload_in(M->Q4.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ8.upload_in(M->Q8.data(), tot, up.pool, up.s));
+  SX_TRY(M->ddrdx.upload_in(M->drdx.data(), tot, up.pool, up.s));
+  SX_TRY(M->ddrdy.upload_in(M->drdy.data(), tot, up.pool, up.s));
+  SX_TRY(M->ddsdx.upload_in(M->dsdx.data(), tot, up.pool, up.s));
+  SX_TRY(M->ddsdy.upload_in(M->dsdy.data(), tot, up.pool, up.s));
+  SX_TRY(M->dimass.upload_in(M->imass.data(), M->imass.size(), up.pool, up.s));
+  SX_TRY(M->dQ1f.upload_in(f1.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ2f.upload_in(f2.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ3f.upload_in(f3.data(), tot, up.pool, up.s));
+  SX_TRY(M->dQ4f.upload_in(f4.data(), tot, up.pool, up.s));
   {
     std::vector<float4> gf(tot);
     for (size_t i = 0; i < tot; i++) gf[i] = make_float4(f1[i], f2[i], f3[i], f4[i]);
-    SX_TRY(M->dGf.upload(gf.data(), tot));
+    SX_TRY(M->dGf.upload_in(gf.data(), tot, up.pool, up.s));
   }
-  SX_TRY(M->dpmap.upload(M->pmap.data(), nn));
+  SX_TRY(M->dpmap.upload_in(M->pmap.data(), nn, up.pool, up.s));
   M->kratio = stiffness_mass_ratio(*M);
   std::vector<float> df(M->D.begin(), M->D.end());
-  SX_TRY(M->dDf.upload(df.data(), df.size()));
-  SX_TRY(M->dhasQ3.upload(M->hasQ3.data(), nel));
-  SX_TRY(M->dbtog.upload(M->btog.data(), tb));
-  SX_TRY(M->denv.upload(M->env.data(), M->env.size()));
-  SX_TRY(M->dbmask.upload(M->bmask.data(), tb));
-  SX_TRY(M->demask.upload(M->emask.data(), nel));
-  SX_TRY(M->dg2e_ptr.upload(ptr.data(), ptr.size()));
-  SX_TRY(M->dg2e_idx.upload(idx.data(), idx.size()));
-  SX_TRY(M->dg2e_last.upload(last.data(), last.size()));
+  SX_TRY(M->dDf.upload_in(df.data(), df.size(), up.pool, up.s));
+  SX_TRY(M->dhasQ3.upload_in(M->hasQ3.data(), nel, up.pool, up.s));
+  SX_TRY(M->dbtog.upload_in(M->btog.data(), tb, up.pool, up.s));
+  SX_TRY(M->denv.upload_in(M->env.data(), M->env.size(), up.pool, up.s));
+  SX_TRY(M->dbmask.upload_in(M->bmask.data(), tb, up.pool, up.s));
+  SX_TRY(M->demask.upload_in(M->emask.data(), nel, up.pool, up.s));
+  SX_TRY(M->dg2e_ptr.upload_in(ptr.data(), ptr.size(), up.pool, up.s));
+  SX_TRY(M->dg2e_idx.upload_in(idx.data(), idx.size(), up.pool, up.s));
+  SX_TRY(M->dg2e_last.upload_in(last.data(), last.size(), up.pool, up.s));
   {
     std::vector<int4> g4(d->nglobal);
     for (int g = 0; g < d->nglobal; g++) {
@@ -523,7 +570,7 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       if (n > 4) v[3] = -2;  // more than 4 contributions: walk the CSR
       g4[g] = make_int4(v[0], v[1], v[2], v[3]);
     }
-    SX_TRY(M->dg2e4.upload(g4.data(), g4.size()));
+    SX_TRY(M->dg2e4.upload_in(g4.data(), g4.size(), up.pool, up.s));
     // per element slot: the holders of its node as (element << 8 | tensor
     // node), the element-layout address of their A u (nel < 2^23, np^2 < 256)
     if (nel >= (1 << 23)) {
@@ -536,29 +583,38 @@ extern "C" int sx_mesh_create(const sx_mesh_desc *d, sx_mesh *out) {
       const int4 q = g4[M->btog[k]];
       e4[k] = make_int4(pack(q.x), pack(q.y), pack(q.z), q.w == -2 ? -2 : pack(q.w));
     }
-    SX_TRY(M->de2w4.upload(e4.data(), e4.size()));
+    SX_TRY(M->de2w4.upload_in(e4.data(), e4.size(), up.pool, up.s));
     std::vector<unsigned long long> own(nel, 0ull);
     for (int e = 0; e < nel; e++)
       for (int a = 0; a < next; a++)
         if (last[M->btog[(size_t)e * next + a]] == e * next + a) own[e] |= 1ull << a;
-    SX_TRY(M->downer.upload(own.data(), own.size()));
+    SX_TRY(M->downer.upload_in(own.data(), own.size(), up.pool, up.s));
   }
   std::vector<int> be(M->b_elmt), bs(M->b_side), bk(M->b_kind);
   if (nb == 0) { be.push_back(0); bs.push_back(0); bk.push_back(0); M->b_K.push_back(0); M->b_C.push_back(0); }
-  SX_TRY(M->dbe.upload(be.data(), be.size()));
-  SX_TRY(M->dbs.upload(bs.data(), bs.size()));
-  SX_TRY(M->dbk.upload(bk.data(), bk.size()));
-  SX_TRY(M->dK.upload(M->b_K.data(), M->b_K.size()));
-  SX_TRY(M->dC.upload(M->b_C.data(), M->b_C.size()));
-  SX_TRY(M->darea.upload(M->b_area.data(), M->b_area.size()));
-  SX_TRY(M->dnat_ptr.upload(nptr.data(), nptr.size()));
-  SX_TRY(M->dnat_idx.upload(nidx.data(), nidx.size()));
-  SX_TRY(M->dcolour_elmt.upload(M->colour_elmt.data(), M->colour_elmt.size()));
+  SX_TRY(M->dbe.upload_in(be.data(), be.size(), up.pool, up.s));
+  SX_TRY(M->dbs.upload_in(bs.data(), bs.size(), up.pool, up.s));
+  SX_TRY(M->dbk.upload_in(bk.data(), bk.size(), up.pool, up.s));
+  SX_TRY(M->dK.upload_in(M->b_K.data(), M->b_K.size(), up.pool, up.s));
+  SX_TRY(M->dC.upload_in(M->b_C.data(), M->b_C.size(), up.pool, up.s));
+  SX_TRY(M->darea.upload_in(M->b_area.data(), M->b_area.size(), up.pool, up.s));
+  SX_TRY(M->dnat_ptr.upload_in(nptr.data(), nptr.size(), up.pool, up.s));
+  SX_TRY(M->dnat_idx.upload_in(nidx.data(), nidx.size(), up.pool, up.s));
+  SX_TRY(M->dcolour_elmt.upload_in(M->colour_elmt.data(), M->colour_elmt.size(), up.pool, up.s));
   *out = M.release();
   return SX_OK;
 }
 
 extern "C" int sx_mesh_destroy(sx_mesh m) {
+  // the mesh's memory is freed stream-ordered: work the caller enqueued with
+  // it (on any stream) must finish first
+  if (m) {
+    int dev = -1;
+    cudaGetDevice(&dev);
+    cudaSetDevice(m->device);
+    cudaDeviceSynchronize();
+    cudaSetDevice(dev);
+  }
   delete m;
   return SX_OK;
 }

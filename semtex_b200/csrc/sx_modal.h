@@ -70,6 +70,7 @@ struct sx_modal_s {
   cudaMemPool_t pool = nullptr;      // when set, workspaces are allocated from it
   std::map<int, sx::BandSched> sched_for;  // systems per launch -> band-sweep schedule (default or tuned)
   int forced_cluster = 0, forced_stages = 0, forced_lead = -1;
+  int host_chunk = 0;                // modes per host-pipeline chunk (0: auto)
   // Band-sweep schedule for nj systems per launch: the knobs where set, else
   // the autotuner's choice for nj, else the largest cluster whose CTAs are
   // all resident (and the default leader share).
