@@ -2,6 +2,8 @@
 
 * GLL points/weights/derivatives vs the reference's femlib/polylib.c
   (tests/golden/gll_ref.npz, made by tests/golden/make_gll_fixture.py).
+* Edge maps vs the reference's femlib/mapping.c
+  (tests/golden/edgemap_ref.npz, made by tests/golden/make_edgemap_fixture.py).
 * Whole DIRECT solves vs regress/*.ok (helmholtz1, poisson1, laplace1,
   laplace4, mixed1, laplace3).
 * JACPCG converges to the DIRECT answer on the same systems.
@@ -35,6 +37,27 @@ def test_edge_maps():
     # CCW exterior from node 0, then interior row-major (femlib/mapping.c:100-113)
     assert emap.tolist() == [0, 1, 2, 3, 7, 11, 15, 14, 13, 12, 8, 4, 5, 6, 9, 10]
     assert (emap[pmap] == np.arange(16)).all()
+
+
+@pytest.mark.parametrize("n", range(3, 17))
+def test_edge_maps_match_reference_mapping(n):
+    """The front-end's and both oracles' edge maps equal the ones the
+    reference's own femlib/mapping.c builds (tests/golden/edgemap_ref.npz,
+    made by tests/golden/make_edgemap_fixture.py): the element-boundary slot
+    order that btog, the static condensation and every gather depend on."""
+    import ctypes as C
+    from oracle.dns import edge_map
+    from oracle.oracle import lib
+    ref = np.load(os.path.join(HERE, "golden", "edgemap_ref.npz"))
+    emap, pmap = edge_maps(n)
+    np.testing.assert_array_equal(emap, ref[f"emap2_{n}"])
+    np.testing.assert_array_equal(pmap, ref[f"pmap2_{n}"])
+    np.testing.assert_array_equal(edge_map(n), ref[f"emap2_{n}"])
+    ce, cp = np.zeros(n * n, dtype=np.int32), np.zeros(n * n, dtype=np.int32)
+    ip = C.POINTER(C.c_int)
+    lib().orc_edgemaps(C.c_int(n), ce.ctypes.data_as(ip), cp.ctypes.data_as(ip))
+    np.testing.assert_array_equal(ce, ref[f"emap2_{n}"])
+    np.testing.assert_array_equal(cp, ref[f"pmap2_{n}"])
 
 
 @pytest.mark.parametrize("name", list(PROBLEMS_2D))
