@@ -504,7 +504,8 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": int(fh.nbytes), "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_s * 1e3, "rel_err_vs_device_call": e2e_err,
                 "call": "sx_field_solve_batched_host (pinned host buffers; copies and solve in the timed "
-                        "region, chunks of 16 modes overlapped)"},
+                        "region; the modes in chunks whose copies and solves overlap, 8 modes a chunk "
+                        "when every mode goes to the band solve)"},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
