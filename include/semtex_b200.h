@@ -142,6 +142,10 @@ SX_API int sx_mesh_partials(sx_mesh mesh, int e, double *drdx, double *drdy, dou
  * skip them.  No counterpart in the reference, which stores and sweeps the
  * whole band. */
 SX_API int sx_mesh_envelope(sx_mesh mesh, int *nblk, int *env);
+/* The same tables from a mesh description, on the host alone (no device is
+ * touched): to size the factor's storage before a mesh is created.  Reads
+ * np, nel, btog, nglobal, nsolve and nband of desc. */
+SX_API int sx_mesh_desc_envelope(const sx_mesh_desc *desc, int *nblk, int *env);
 
 /* ---- modal system: replaces ModalMatrixSys::ModalMatrixSys ---------------
  * src/matrix.cpp:33-110, MatrixSys::MatrixSys src/matrix.cpp:139-317.

@@ -149,6 +149,7 @@ def _load():
     L.sx_transform_z.argtypes = [vp, ip, ip, ip, ip, vp]
     L.sx_mesh_partials.argtypes = [vp, ip] + [P(dp)] * 5
     L.sx_mesh_envelope.argtypes = [vp, P(ip), P(ip)]
+    L.sx_mesh_desc_envelope.argtypes = [P(MeshDesc), P(ip), P(ip)]
     L.sx_field_gradient.argtypes = [vp, vp, ip, ip, ip, dp, ip, vp]
     L.sx_dns_pressure_forcing.argtypes = [vp, P(vp), ip, vp, ip, ip, dp, dp, ip, vp]
     L.sx_dns_project.argtypes = [vp, P(vp), vp, P(vp), ip, ip, ip, ip, ip, dp, dp, dp, dp, ip, vp]
@@ -232,6 +233,21 @@ def mesh_desc(qm: QuadMesh):
                  _iptr(k["bmask"]), qm.nglobal, qm.nsolve, qm.nband, nb,
                  _iptr(k["be"]), _iptr(k["bs"]), _iptr(k["bk"]), _dptr(k["bK"]), _dptr(k["bC"]))
     return d, k
+
+
+def band_envelope(qm: QuadMesh):
+    """The band factor's envelope of a mesh by 64 x 64 tiles, computed on the
+    host from its numbering alone (no device): (above, right), the tiles
+    above the diagonal of each block column and right of it in each block
+    row that the factorisation and the sweeps visit."""
+    d, keep = mesh_desc(qm)
+    nb = C.c_int()
+    _check(lib.sx_mesh_desc_envelope(C.byref(d), C.byref(nb), None), "sx_mesh_desc_envelope")
+    env = np.zeros(2 * max(nb.value, 1), dtype=np.int32)
+    _check(lib.sx_mesh_desc_envelope(C.byref(d), C.byref(nb), env.ctypes.data_as(C.POINTER(C.c_int))),
+           "sx_mesh_desc_envelope")
+    del keep
+    return env[:nb.value].copy(), env[nb.value:2 * nb.value].copy()
 
 
 class Mesh:

@@ -345,28 +345,55 @@ struct MeshUpload {
 // tiles above its diagonal, block row k the jb(k) = max{ j : fm(k + j) <= k }
 // right of it.  The pressure pin (nsolve - 1) only removes a row and column,
 // so the tables of nsolve hold for it as well.
-static int band_envelope(sx_mesh_s &M) {
-  const int ns = M.nsolve, nblk = (ns + NB - 1) / NB, J = (M.nband - 1 + NB - 1) / NB;
+// btog entries must lie in [0, nglobal) (the callers check).
+static void envelope_tables(const int *btog, int nel, int next, int ns, int nband, int &nblk,
+                            std::vector<int> &env) {
+  const int J = (nband - 1 + NB - 1) / NB;
+  nblk = (ns + NB - 1) / NB;
   std::vector<int> fm(nblk);
   for (int k = 0; k < nblk; k++) fm[k] = k;
-  for (int e = 0; e < M.nel; e++) {
-    const int *g = &M.btog[(size_t)e * M.next];
+  for (int e = 0; e < nel; e++) {
+    const int *g = &btog[(size_t)e * next];
     int lo = ns;
-    for (int i = 0; i < M.next; i++)
+    for (int i = 0; i < next; i++)
       if (g[i] < ns) lo = std::min(lo, g[i]);
-    for (int i = 0; i < M.next; i++)
+    for (int i = 0; i < next; i++)
       if (g[i] < ns) fm[g[i] / NB] = std::min(fm[g[i] / NB], lo / NB);
   }
   for (int k = nblk - 2; k >= 0; k--) fm[k] = std::min(fm[k], fm[k + 1]);
-  M.env_nblk = nblk;
-  M.env.assign((size_t)2 * std::max(nblk, 1), 0);
+  env.assign((size_t)2 * std::max(nblk, 1), 0);
   int c = 0;  // the last block column whose hull reaches row block k
   for (int k = 0; k < nblk; k++) {
-    M.env[k] = std::min(J, k - fm[k]);
+    env[k] = std::min(J, k - fm[k]);
     c = std::max(c, k);
     while (c + 1 < nblk && fm[c + 1] <= k) c++;
-    M.env[nblk + k] = std::min(J, c - k);
+    env[nblk + k] = std::min(J, c - k);
   }
+}
+
+static int band_envelope(sx_mesh_s &M) {
+  envelope_tables(M.btog.data(), M.nel, M.next, M.nsolve, M.nband, M.env_nblk, M.env);
+  return SX_OK;
+}
+
+extern "C" int sx_mesh_desc_envelope(const sx_mesh_desc *d, int *nblk, int *env) {
+  if (!d || !nblk || d->np < 2 || d->nel <= 0 || !d->btog || d->nglobal <= 0 || d->nsolve < 0 ||
+      d->nsolve > d->nglobal || d->nband <= 0) {
+    set_error("invalid mesh description");
+    return SX_ERR_ARG;
+  }
+  const int next = 4 * (d->np - 1);
+  const size_t tb = (size_t)d->nel * next;
+  for (size_t i = 0; i < tb; i++)
+    if (d->btog[i] < 0 || d->btog[i] >= d->nglobal) {
+      set_error("btog[%zu] = %d outside [0, nglobal)", i, d->btog[i]);
+      return SX_ERR_ARG;
+    }
+  std::vector<int> tab;
+  int nb = 0;
+  envelope_tables(d->btog, d->nel, next, d->nsolve, d->nband, nb, tab);
+  *nblk = nb;
+  if (env) std::memcpy(env, tab.data(), sizeof(int) * 2 * (size_t)nb);
   return SX_OK;
 }
 
