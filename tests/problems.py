@@ -52,8 +52,38 @@ PROBLEMS_2D = {
 }
 
 
+def _sin_exp(x, y):
+    return np.sin(x) * np.exp(-y)
+
+
+# Two more of the reference's 2 x 2, N_P = 11 Laplace problems on the unit
+# square, exact solution sin(x) exp(-y), goldens "noise-level"; pinned on the
+# oracle (CPU tests) in addition to the five above.
+PROBLEMS_2D_MORE = {
+    # mesh/laplace5, regress/laplace5.ok: the exact solution as essential BC
+    # on every side
+    "laplace5": dict(
+        np=11, lambda2=0.0,
+        forcing=lambda x, y: 0.0 * x,
+        exact=_sin_exp,
+        bc=None, bcval={s: _sin_exp for s in ("bottom", "right", "top", "left")}, periodic=False,
+        golden=None),
+    # mesh/laplace7, regress/laplace7.ok: essential on top, natural (the
+    # outward normal derivative) on the other three sides
+    "laplace7": dict(
+        np=11, lambda2=0.0,
+        forcing=lambda x, y: 0.0 * x,
+        exact=_sin_exp,
+        bc={"bottom": "N", "right": "N", "left": "N"},
+        bcval={"top": _sin_exp, "bottom": _sin_exp,
+               "right": lambda x, y: np.cos(x) * np.exp(-y),
+               "left": lambda x, y: -np.cos(x) * np.exp(-y)},
+        periodic=False, golden=None),
+}
+
+
 def build_2d(name):
-    p = PROBLEMS_2D[name]
+    p = PROBLEMS_2D[name] if name in PROBLEMS_2D else PROBLEMS_2D_MORE[name]
     m = rect_mesh(2, 2, p["np"], bc=p["bc"], periodic_x=p["periodic"])
     f = m.eval_nodes(p["forcing"])[None]
     bc = m.bc_line(p["bcval"])[None]

@@ -5,7 +5,7 @@
 * Edge maps vs the reference's femlib/mapping.c
   (tests/golden/edgemap_ref.npz, made by tests/golden/make_edgemap_fixture.py).
 * Whole DIRECT solves vs regress/*.ok (helmholtz1, poisson1, laplace1,
-  laplace4, mixed1, laplace3).
+  laplace4, laplace5, laplace7, mixed1, laplace3).
 * JACPCG converges to the DIRECT answer on the same systems.
 * Banded Cholesky restatement vs a dense factorisation.
 """
@@ -16,7 +16,7 @@ import pytest
 
 from oracle.oracle import DIRECT, JACPCG, OracleMesh, OracleSystem, gll, solve_planes
 from semtex_b200.mesh import edge_maps, gll_points, rect_mesh
-from tests.problems import (LAPLACE3, PROBLEMS_2D, build_2d, build_laplace3, golden_ok,
+from tests.problems import (LAPLACE3, PROBLEMS_2D, PROBLEMS_2D_MORE, build_2d, build_laplace3, golden_ok,
                             to_physical)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -60,7 +60,7 @@ def test_edge_maps_match_reference_mapping(n):
     np.testing.assert_array_equal(cp, ref[f"pmap2_{n}"])
 
 
-@pytest.mark.parametrize("name", list(PROBLEMS_2D))
+@pytest.mark.parametrize("name", list(PROBLEMS_2D) + list(PROBLEMS_2D_MORE))
 def test_direct_matches_regress_golden(name):
     m, p, f, bc, exact = build_2d(name)
     u, _ = solve_planes(OracleMesh(m), p["lambda2"], 0.0, f, bc, method=DIRECT)
@@ -68,7 +68,7 @@ def test_direct_matches_regress_golden(name):
     assert golden_ok(err, p["golden"]), (name, err)
 
 
-@pytest.mark.parametrize("name", list(PROBLEMS_2D))
+@pytest.mark.parametrize("name", list(PROBLEMS_2D) + list(PROBLEMS_2D_MORE))
 def test_jacpcg_converges_to_direct(name):
     m, p, f, bc, exact = build_2d(name)
     om = OracleMesh(m)
